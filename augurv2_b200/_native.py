@@ -1,0 +1,96 @@
+"""ctypes binding of the CUDA library (include/augur_b200.h).
+
+The library is the only compute path: if libaugur_b200.so is missing or a
+call fails, an AugurError is raised; there is no CPU fallback.
+"""
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libaugur_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "augur_b200.h")
+
+
+class AugurError(RuntimeError):
+    pass
+
+
+_lib = None
+
+i32, u32, u64, f64, f32 = C.c_int, C.c_uint32, C.c_uint64, C.c_double, C.c_float
+vp, sz = C.c_void_p, C.c_size_t
+
+
+def header_symbols(path=HEADER):
+    """Names of every function declared in the public header."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ab_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib():
+    """Loads libaugur_b200.so (building it first if the sources are newer is
+    the job of augurv2_b200.build; this only loads)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AugurError(
+                "CUDA library %s is missing: run `python -m augurv2_b200.build` "
+                "(there is no CPU fallback)" % LIB_PATH)
+        _lib = C.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+def last_error():
+    return lib().ab_last_error().decode()
+
+
+def check(rc, what=""):
+    if rc != 0:
+        raise AugurError("%s failed (status %d): %s" % (what, rc, last_error()))
+    return rc
+
+
+class LdaDesc(C.Structure):
+    _fields_ = [("D", i32), ("K", i32), ("V", i32),
+                ("doc_off", vp), ("w", vp), ("alpha", vp), ("beta", vp),
+                ("z", vp), ("theta", vp), ("phiT", vp), ("cnt_dk", vp), ("cnt_kw", vp),
+                ("scratch", vp), ("seed", u64)]
+
+
+_SIGS = {
+    "ab_last_error": (C.c_char_p, []),
+    "ab_version": (C.c_char_p, []),
+    # LDA
+    "ab_lda_phi_stride": (i32, [i32]),
+    "ab_lda_count": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp]),
+    "ab_lda_conj_theta": (i32, [i32, i32, vp, vp, vp, u64, u32, vp]),
+    "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp]),
+    "ab_lda_disc_z": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
+    "ab_lda_scratch_bytes": (sz, []),
+    "ab_lda_create": (i32, [C.POINTER(LdaDesc), C.POINTER(vp)]),
+    "ab_lda_init_state": (i32, [vp, u32, vp]),
+    "ab_lda_run": (i32, [vp, i32, i32, vp]),
+    "ab_lda_destroy": (i32, [vp]),
+}
+
+
+def _declare(L):
+    for name, (res, args) in _SIGS.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def stream_ptr(stream=None):
+    """cudaStream_t of a torch stream (current stream by default)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    return None if t is None else C.c_void_p(t.data_ptr())

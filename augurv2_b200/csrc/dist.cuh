@@ -1,0 +1,42 @@
+// Device samplers shared by the Gibbs and HMC kernels.  Each follows the
+// reference distribution library (cbits/augur_dist.c) operation for
+// operation in binary64, drawing from a Philox substream (philox.cuh).
+#pragma once
+#include "philox.cuh"
+
+namespace ab {
+
+// Marsaglia & Tsang (2000) for shape >= 1 (cbits/augur_dist.c:287-300).
+// The binary64 mul/add steps are spelled with _rn intrinsics so that no
+// multiply-add is contracted, as in the reference's libcpu build.
+__device__ __forceinline__ double gamma_ge1(Stream& s, double alpha) {
+  const double d = __dadd_rn(alpha, -1.0 / 3.0);
+  const double c = 1.0 / sqrt(__dmul_rn(9.0, d));
+  const double neg_inv_c = -1.0 / c;
+  for (int tries = 0; tries < 1000000; ++tries) {
+    double z = s.normal();
+    double u = s.uniform();
+    double t = __dadd_rn(1.0, __dmul_rn(c, z));
+    double V = __dmul_rn(__dmul_rn(t, t), t);
+    if (z > neg_inv_c) {
+      double rhs = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(0.5, z), z), d),
+                                       -__dmul_rn(d, V)),
+                             __dmul_rn(d, log(V)));
+      if (log(u) < rhs) return __dmul_rn(d, V);
+    }
+  }
+  return __dmul_rn(d, 1.0);  // unreachable in practice (acceptance > 95%)
+}
+
+// cbits/augur_dist.c:302-312: boost shape < 1 through Gamma(shape + 1).
+__device__ __forceinline__ double gamma_draw(Stream& s, double shape, double rate) {
+  const double scale = 1.0 / rate;
+  if (shape < 1.0) {
+    double x = gamma_ge1(s, __dadd_rn(shape, 1.0));
+    double u = s.uniform();
+    return __dmul_rn(__dmul_rn(x, pow(u, 1.0 / shape)), scale);
+  }
+  return __dmul_rn(gamma_ge1(s, shape), scale);
+}
+
+}  // namespace ab

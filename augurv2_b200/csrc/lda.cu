@@ -1,0 +1,425 @@
+// LDA collapsed-free Gibbs sweep for the reference schedule
+//   ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z]
+// over the model of compiler/augur/test/lda.rv.
+//
+// Layout in HBM (all row-major):
+//   w        int32 [T]      token ids, documents contiguous
+//   doc_off  int32 [D+1]    CSR offsets of documents into w / z
+//   z        int32 [T]      topic assignments
+//   theta    f64   [D][K]   document-topic proportions
+//   phiT     f64   [V][Kp]  topic-word proportions stored word-major, each
+//                           row padded to Kp = round_up(K, 4) doubles so
+//                           that a token's K values are one aligned segment
+//   cnt_dk   int32 [D][K]   document-topic counts
+//   cnt_kw   int32 [K][V]   topic-word counts
+//
+// One sweep is three kernels:
+//   lda_theta_kernel  theta[d] ~ Dir(alpha + cnt_dk[d])      (reads cnt_dk)
+//   lda_phi_kernel    phi[k]   ~ Dir(beta + cnt_kw[k])       (reads, then
+//                     clears cnt_kw); one thread-block cluster per topic
+//   lda_z_kernel      z ~ p(z | theta, phi), and the counts of the new z
+//                     (cnt_dk rows written whole, cnt_kw incremented)
+// The count statistics of the reference (conj_stat_*, rebuilt from zero each
+// step, CgKern.hs:103-107) are a function of z alone, so they are produced
+// by the z kernel of the previous sweep instead of by a separate pass.
+//
+// Bit-exactness: the z draw follows cbits/augur_dist.c:798-813 and
+// CgDisc.hs:132-139 operation for operation in binary64 with no contraction
+// (_rn intrinsics; this file is also compiled with -fmad=false), so given the
+// same theta, phi and Philox uniforms the assignments and counts equal the
+// reference's CPU sampler's bit for bit.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "dist.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace ab {
+
+constexpr int LDA_PHI_CLUSTER = 4;     // CTAs per topic row in the phi kernel
+constexpr int LDA_THREADS = 256;
+constexpr int LDA_MAX_K = 1024;
+
+__device__ __forceinline__ uint32_t read_iter(const uint32_t* iter_dev, uint32_t iter_fixed) {
+  return iter_dev ? *(volatile const uint32_t*)iter_dev : iter_fixed;
+}
+
+// ---------------------------------------------------------------------------
+// theta[d][k] = g[d][k] / sum_k g[d][k],  g ~ Gamma(alpha_k + cnt[d][k], 1)
+// (augur_dirichlet_categorical_conj, cbits/augur_dist.c:526-538).  The row
+// sum is taken sequentially over k by one thread, as the reference does, so
+// theta is bit-identical to the reference given identical gamma draws.
+// Block: R = 256 / K rows (or one row looped when K > 256).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
+                 const int* __restrict__ cnt_dk, double* __restrict__ theta,
+                 uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+  extern __shared__ double sg[];  // [rows_per_block][K] gamma draws, then [rows] sums
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  const int rows = K <= LDA_THREADS ? LDA_THREADS / K : 1;
+  const int row0 = blockIdx.x * rows;
+  double* sums = sg + rows * K;
+  for (int e = threadIdx.x; e < rows * K; e += blockDim.x) {
+    const int r = e / K, k = e - r * K;
+    const int d = row0 + r;
+    if (d < D) {
+      const size_t idx = (size_t)d * K + k;
+      Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_THETA);
+      sg[e] = gamma_draw(s, __dadd_rn(alpha[k], (double)cnt_dk[idx]), 1.0);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < rows && row0 + (int)threadIdx.x < D) {
+    double acc = 0.0;
+    const double* g = sg + threadIdx.x * K;
+    for (int k = 0; k < K; ++k) acc = __dadd_rn(acc, g[k]);
+    sums[threadIdx.x] = acc;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < rows * K; e += blockDim.x) {
+    const int r = e / K;
+    const int d = row0 + r;
+    if (d < D) theta[(size_t)row0 * K + e] = __ddiv_rn(sg[e], sums[r]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phi[k][v] = g[k][v] / sum_v g[k][v], g ~ Gamma(beta_v + cnt[k][v], 1),
+// stored word-major into phiT[v][k].  One cluster of LDA_PHI_CLUSTER CTAs per
+// topic: each CTA draws its slice of V into phiT (and clears the counts it
+// read), reduces its partial sum in a fixed order, publishes it in shared
+// memory, and after a cluster barrier every CTA adds the partials of all
+// CTAs of the cluster (distributed shared memory) in rank order and
+// normalises its slice.  The sum is deterministic but not in the reference's
+// sequential order, so phi matches the reference to rounding, not bitwise.
+// ---------------------------------------------------------------------------
+__global__ void __cluster_dims__(LDA_PHI_CLUSTER, 1, 1) __launch_bounds__(LDA_THREADS)
+lda_phi_kernel(int K, int V, int Kp, const double* __restrict__ beta,
+               int* __restrict__ cnt_kw, double* __restrict__ phiT, int clear_counts,
+               uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+  __shared__ double red[33];
+  __shared__ double partial;
+  cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  const int k = blockIdx.x / LDA_PHI_CLUSTER;
+  const int rank = (int)cluster.block_rank();
+  const int per = (V + LDA_PHI_CLUSTER - 1) / LDA_PHI_CLUSTER;
+  const int v0 = rank * per;
+  const int v1 = min(V, v0 + per);
+  double local = 0.0;
+  if (k < K) {
+    for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+      const size_t idx = (size_t)k * V + v;
+      const int c = cnt_kw[idx];
+      if (clear_counts) cnt_kw[idx] = 0;
+      Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
+      const double g = gamma_draw(s, __dadd_rn(beta[v], (double)c), 1.0);
+      phiT[(size_t)v * Kp + k] = g;
+      local = __dadd_rn(local, g);
+    }
+  }
+  const double bsum = block_sum_f64(local, red);
+  if (threadIdx.x == 0) partial = bsum;
+  cluster.sync();
+  double norm = 0.0;
+  for (int r = 0; r < LDA_PHI_CLUSTER; ++r) {
+    const double* p = cluster.map_shared_rank(&partial, r);
+    norm = __dadd_rn(norm, *p);
+  }
+  if (k < K) {
+    for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
+      const size_t o = (size_t)v * Kp + k;
+      phiT[o] = __ddiv_rn(phiT[o], norm);
+    }
+  }
+  cluster.sync();  // keep `partial` alive until every CTA has read it
+}
+
+// ---------------------------------------------------------------------------
+// z[t] for every token of document d (one CTA per document):
+//   pmf_k  = (1 * theta[d][k]) * phi[k][w]                (CgDisc.hs:132-139)
+//   norm   = sum_k pmf_k  (sequential)                    (augur_dist.c:800-803)
+//   z      = first i with u < sum_{j<=i} pmf_j / norm      (:805-812)
+// The products are recomputed in the second pass instead of stored; they are
+// the same binary64 values.  Counts of the new z: the document's row of
+// cnt_dk is accumulated in shared memory and stored whole; cnt_kw receives
+// warp-aggregated atomic increments (lanes with the same (z, w) key elect
+// one leader that adds the group size).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
+             const int* __restrict__ w, const double* __restrict__ theta,
+             const double* __restrict__ phiT, int* __restrict__ z,
+             int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
+             uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
+  extern __shared__ double smem[];
+  double* th = smem;                                   // [K]
+  int* hist = reinterpret_cast<int*>(smem + K);        // [K]
+  const int d = blockIdx.x;
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  for (int k = threadIdx.x; k < K; k += blockDim.x) {
+    th[k] = theta[(size_t)d * K + k];
+    hist[k] = 0;
+  }
+  __syncthreads();
+  const int t0 = doc_off[d], t1 = doc_off[d + 1];
+  for (int tb = t0; tb < t1; tb += blockDim.x) {
+    const int t = tb + threadIdx.x;
+    const bool active = t < t1;
+    int zk = 0, wt = 0;
+    if (active) {
+      wt = w[t];
+      const double* row = phiT + (size_t)wt * Kp;
+      double norm = 0.0;
+      for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], __ldg(row + k)));
+      Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+      const double u = s.uniform();
+      double acc = __ddiv_rn(__dmul_rn(th[0], __ldg(row)), norm);
+      zk = K - 1;
+      for (int i = 1; i < K; ++i) {
+        if (u < acc) { zk = i - 1; break; }
+        acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], __ldg(row + i)), norm));
+      }
+      z[t] = zk;
+      atomicAdd(&hist[zk], 1);
+    }
+    if (cnt_kw != nullptr) {
+      const unsigned mask = __ballot_sync(0xffffffffu, active);
+      if (active) {
+        const long long key = (long long)zk * V + wt;
+        const unsigned peers = __match_any_sync(mask, key);
+        const int leader = __ffs(peers) - 1;
+        if ((int)(threadIdx.x & 31) == leader) atomicAdd(cnt_kw + key, __popc(peers));
+      }
+    }
+  }
+  __syncthreads();
+  if (cnt_dk != nullptr)
+    for (int k = threadIdx.x; k < K; k += blockDim.x) cnt_dk[(size_t)d * K + k] = hist[k];
+  // The last CTA to finish advances the device iteration counter, so a
+  // captured sweep can be replayed without host updates.
+  if (iter_dev != nullptr && done_ctr != nullptr) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(done_ctr, 1u);
+      if (prev == (unsigned)(D - 1)) {
+        *done_ctr = 0u;
+        *iter_dev = iter + 1u;
+        __threadfence();
+      }
+    }
+  }
+}
+
+// Count statistics of a given z (conj_stat_theta / conj_stat_phi of
+// CgConj.hs:171-177): one CTA per document; cnt_kw must be zero on entry.
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_count_kernel(int K, int V, const int* __restrict__ doc_off,
+                 const int* __restrict__ w, const int* __restrict__ z,
+                 int* __restrict__ cnt_dk, int* __restrict__ cnt_kw) {
+  extern __shared__ int hist_s[];
+  const int d = blockIdx.x;
+  for (int k = threadIdx.x; k < K; k += blockDim.x) hist_s[k] = 0;
+  __syncthreads();
+  for (int t = doc_off[d] + threadIdx.x; t < doc_off[d + 1]; t += blockDim.x) {
+    const int zk = z[t];
+    atomicAdd(&hist_s[zk], 1);
+    atomicAdd(cnt_kw + (size_t)zk * V + w[t], 1);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < K; k += blockDim.x) cnt_dk[(size_t)d * K + k] = hist_s[k];
+}
+
+// ------------------------------- launchers ---------------------------------
+
+static int check_lda_dims(int D, int K, int V) {
+  AB_REQUIRE(D > 0 && K > 0 && V > 0, AB_ERR_ARG, "LDA sizes must be positive (D=%d K=%d V=%d)", D, K, V);
+  AB_REQUIRE(K <= LDA_MAX_K, AB_ERR_ARG, "LDA supports K <= %d topics (got %d)", LDA_MAX_K, K);
+  AB_REQUIRE((size_t)K * (size_t)V < (1ull << 32), AB_ERR_ARG, "K*V must be < 2^32");
+  return AB_OK;
+}
+
+int launch_lda_theta(int D, int K, const double* alpha, const int* cnt_dk, double* theta,
+                     uint64_t seed, const uint32_t* iter_dev, uint32_t iter, cudaStream_t st) {
+  const int rows = K <= LDA_THREADS ? LDA_THREADS / K : 1;
+  const size_t smem = sizeof(double) * ((size_t)rows * K + rows);
+  lda_theta_kernel<<<ceil_div(D, rows), LDA_THREADS, smem, st>>>(D, K, alpha, cnt_dk, theta, seed,
+                                                                 iter_dev, iter);
+  AB_LAUNCH_CHECK("lda_theta_kernel");
+  return AB_OK;
+}
+
+int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double* phiT, int clear,
+                   uint64_t seed, const uint32_t* iter_dev, uint32_t iter, cudaStream_t st) {
+  lda_phi_kernel<<<K * LDA_PHI_CLUSTER, LDA_THREADS, 0, st>>>(K, V, Kp, beta, cnt_kw, phiT, clear,
+                                                              seed, iter_dev, iter);
+  AB_LAUNCH_CHECK("lda_phi_kernel");
+  return AB_OK;
+}
+
+int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
+                 const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                 uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
+  const size_t smem = sizeof(double) * K + sizeof(int) * K;
+  lda_z_kernel<<<D, 128, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed,
+                                      iter_dev, iter, done_ctr);
+  AB_LAUNCH_CHECK("lda_z_kernel");
+  return AB_OK;
+}
+
+int launch_lda_count(int D, int K, int V, const int* doc_off, const int* w, const int* z,
+                     int* cnt_dk, int* cnt_kw, cudaStream_t st) {
+  AB_CUDA(cudaMemsetAsync(cnt_kw, 0, sizeof(int) * (size_t)K * V, st));
+  lda_count_kernel<<<D, LDA_THREADS, sizeof(int) * K, st>>>(K, V, doc_off, w, z, cnt_dk, cnt_kw);
+  AB_LAUNCH_CHECK("lda_count_kernel");
+  return AB_OK;
+}
+
+static inline int lda_kp(int K) { return (K + 3) & ~3; }
+
+}  // namespace ab
+
+using namespace ab;
+
+// ------------------------------- C ABI -------------------------------------
+
+extern "C" int ab_lda_phi_stride(int K) { return lda_kp(K); }
+
+extern "C" int ab_lda_count(int D, int K, int V, const int* doc_off, const int* w, const int* z,
+                            int* cnt_dk, int* cnt_kw, void* stream) {
+  int rc = check_lda_dims(D, K, V);
+  if (rc) return rc;
+  AB_REQUIRE(doc_off && w && z && cnt_dk && cnt_kw, AB_ERR_ARG, "ab_lda_count: null pointer");
+  return launch_lda_count(D, K, V, doc_off, w, z, cnt_dk, cnt_kw, as_stream(stream));
+}
+
+extern "C" int ab_lda_conj_theta(int D, int K, const double* alpha, const int* cnt_dk, double* theta,
+                                 uint64_t seed, uint32_t iter, void* stream) {
+  AB_REQUIRE(D > 0 && K > 0 && K <= LDA_MAX_K, AB_ERR_ARG, "ab_lda_conj_theta: bad sizes D=%d K=%d", D, K);
+  AB_REQUIRE(alpha && cnt_dk && theta, AB_ERR_ARG, "ab_lda_conj_theta: null pointer");
+  return launch_lda_theta(D, K, alpha, cnt_dk, theta, seed, nullptr, iter, as_stream(stream));
+}
+
+extern "C" int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
+                               int clear_counts, uint64_t seed, uint32_t iter, void* stream) {
+  int rc = check_lda_dims(1, K, V);
+  if (rc) return rc;
+  AB_REQUIRE(beta && cnt_kw && phiT, AB_ERR_ARG, "ab_lda_conj_phi: null pointer");
+  return launch_lda_phi(K, V, lda_kp(K), beta, cnt_kw, phiT, clear_counts, seed, nullptr, iter,
+                        as_stream(stream));
+}
+
+extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int* w,
+                             const double* theta, const double* phiT, int* z, int* cnt_dk,
+                             int* cnt_kw, uint64_t seed, uint32_t iter, void* stream) {
+  int rc = check_lda_dims(D, K, V);
+  if (rc) return rc;
+  AB_REQUIRE(doc_off && w && theta && phiT && z, AB_ERR_ARG, "ab_lda_disc_z: null pointer");
+  AB_REQUIRE((cnt_dk == nullptr) == (cnt_kw == nullptr), AB_ERR_ARG,
+             "ab_lda_disc_z: pass both count tables or neither");
+  return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, nullptr,
+                      iter, nullptr, as_stream(stream));
+}
+
+// ---- sweep runner with a captured CUDA graph -------------------------------
+
+struct ab_lda {
+  ab_lda_desc d;
+  int Kp;
+  cudaGraphExec_t exec = nullptr;
+  int graph_sweeps = 0;
+  cudaStream_t s_main = nullptr, s_side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
+  const ab_lda_desc& d = h->d;
+  uint32_t* iter_dev = reinterpret_cast<uint32_t*>(d.scratch);
+  uint32_t* done = iter_dev + 1;
+  AB_CUDA(cudaEventRecord(h->fork, main));
+  AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
+  int rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, main);
+  if (rc) return rc;
+  rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.seed, iter_dev, 0, side);
+  if (rc) return rc;
+  AB_CUDA(cudaEventRecord(h->join, side));
+  AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
+  return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, d.z, d.cnt_dk, d.cnt_kw,
+                      d.seed, iter_dev, 0, done, main);
+}
+
+extern "C" size_t ab_lda_scratch_bytes(void) { return 256; }
+
+extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
+  AB_REQUIRE(desc && out, AB_ERR_ARG, "ab_lda_create: null argument");
+  int rc = check_lda_dims(desc->D, desc->K, desc->V);
+  if (rc) return rc;
+  AB_REQUIRE(desc->doc_off && desc->w && desc->z && desc->theta && desc->phiT && desc->alpha &&
+                 desc->beta && desc->cnt_dk && desc->cnt_kw && desc->scratch,
+             AB_ERR_ARG, "ab_lda_create: every device pointer of the descriptor is required");
+  ab_lda* h = new ab_lda();
+  h->d = *desc;
+  h->Kp = lda_kp(desc->K);
+  cudaError_t e = cudaStreamCreateWithFlags(&h->s_main, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->s_side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    ab_lda_destroy(h);
+    return cuda_status(e, "ab_lda_create");
+  }
+  *out = h;
+  return AB_OK;
+}
+
+extern "C" int ab_lda_init_state(ab_lda* h, uint32_t iter, void* stream) {
+  AB_REQUIRE(h, AB_ERR_ARG, "ab_lda_init_state: null handle");
+  const ab_lda_desc& d = h->d;
+  cudaStream_t st = as_stream(stream);
+  uint32_t hdr[2] = {iter, 0u};
+  AB_CUDA(cudaMemcpyAsync(d.scratch, hdr, sizeof(hdr), cudaMemcpyHostToDevice, st));
+  return launch_lda_count(d.D, d.K, d.V, d.doc_off, d.w, d.z, d.cnt_dk, d.cnt_kw, st);
+}
+
+extern "C" int ab_lda_run(ab_lda* h, int n_sweeps, int use_graph, void* stream) {
+  AB_REQUIRE(h, AB_ERR_ARG, "ab_lda_run: null handle");
+  AB_REQUIRE(n_sweeps >= 0, AB_ERR_ARG, "ab_lda_run: n_sweeps < 0");
+  cudaStream_t st = as_stream(stream);
+  if (!use_graph) {
+    for (int s = 0; s < n_sweeps; ++s) {
+      int rc = lda_enqueue_sweep(h, st, h->s_side);
+      if (rc) return rc;
+    }
+    return AB_OK;
+  }
+  if (h->exec == nullptr) {
+    cudaGraph_t g = nullptr;
+    AB_CUDA(cudaStreamBeginCapture(h->s_main, cudaStreamCaptureModeThreadLocal));
+    int rc = lda_enqueue_sweep(h, h->s_main, h->s_side);
+    cudaError_t e = cudaStreamEndCapture(h->s_main, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    AB_CUDA(e);
+    e = cudaGraphInstantiate(&h->exec, g, 0);
+    cudaGraphDestroy(g);
+    AB_CUDA(e);
+  }
+  for (int s = 0; s < n_sweeps; ++s) AB_CUDA(cudaGraphLaunch(h->exec, st));
+  return AB_OK;
+}
+
+extern "C" int ab_lda_destroy(ab_lda* h) {
+  if (!h) return AB_OK;
+  if (h->exec) cudaGraphExecDestroy(h->exec);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
+  if (h->s_main) cudaStreamDestroy(h->s_main);
+  if (h->s_side) cudaStreamDestroy(h->s_side);
+  delete h;
+  return AB_OK;
+}

@@ -1,0 +1,134 @@
+"""LDA Gibbs sampler on the GPU: host side of the ab_lda_* entry points.
+
+Model (compiler/augur/test/lda.rv, examples/lda.py:12-22):
+    theta[d] ~ Dirichlet(alpha)            for d < D
+    phi[k]   ~ Dirichlet(beta)             for k < K
+    z[d, n]  ~ Categorical(theta[d])       for n < N[d]
+    w[d, n]  ~ Categorical(phi[z[d, n]])
+Schedule: ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z].
+
+Device state lives in torch tensors owned by this object; every sweep runs
+as a replay of a captured CUDA graph of three kernels (lda.cu).
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+def flatten_docs(w):
+    """Ragged documents (sequence of int arrays, or a 2-D array) -> CSR
+    (doc_off int32[D+1], w int32[T]), the flattening of
+    cbits/augur_vecop.c:842-941 without per-row headers."""
+    docs = [np.asarray(x, dtype=np.int32).ravel() for x in w]
+    lens = np.array([len(x) for x in docs], dtype=np.int64)
+    off = np.zeros(len(docs) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    if off[-1] >= 2**31:
+        raise ValueError("more than 2^31 tokens")
+    flat = np.concatenate(docs) if docs else np.zeros(0, np.int32)
+    return off.astype(np.int32), flat.astype(np.int32)
+
+
+class LdaGibbs:
+    def __init__(self, K, V, doc_off, w, alpha, beta, seed=0, theta=None, phi=None, z=None,
+                 iter0=0, device="cuda"):
+        self.dev = torch.device(device)
+        self.K, self.V = int(K), int(V)
+        doc_off = np.ascontiguousarray(doc_off, dtype=np.int32)
+        w = np.ascontiguousarray(w, dtype=np.int32)
+        self.D = len(doc_off) - 1
+        self.T = int(doc_off[-1])
+        if w.shape[0] != self.T:
+            raise ValueError("w has %d tokens, doc_off says %d" % (w.shape[0], self.T))
+        if self.T and (w.min() < 0 or w.max() >= self.V):
+            raise ValueError("token ids must lie in [0, V)")
+        L = N.lib()
+        self.Kp = L.ab_lda_phi_stride(self.K)
+        self.seed = int(seed)
+        t = lambda a, dt: torch.as_tensor(a, dtype=dt).to(self.dev)
+        self.doc_off = t(doc_off, torch.int32)
+        self.w = t(w, torch.int32)
+        self.alpha = t(np.broadcast_to(np.asarray(alpha, np.float64), (self.K,)).copy(), torch.float64)
+        self.beta = t(np.broadcast_to(np.asarray(beta, np.float64), (self.V,)).copy(), torch.float64)
+        self.theta = torch.empty((self.D, self.K), dtype=torch.float64, device=self.dev)
+        self.phiT = torch.zeros((self.V, self.Kp), dtype=torch.float64, device=self.dev)
+        self.z = torch.zeros(self.T, dtype=torch.int32, device=self.dev)
+        self.cnt_dk = torch.zeros((self.D, self.K), dtype=torch.int32, device=self.dev)
+        self.cnt_kw = torch.zeros((self.K, self.V), dtype=torch.int32, device=self.dev)
+        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes()), dtype=torch.uint8, device=self.dev)
+        self.set_state(theta=theta if theta is not None else np.full((self.D, self.K), 1.0 / self.K),
+                       phi=phi if phi is not None else np.full((self.K, self.V), 1.0 / self.V),
+                       z=z if z is not None else np.zeros(self.T, np.int32), iteration=iter0)
+        desc = N.LdaDesc(self.D, self.K, self.V, self.doc_off.data_ptr(), self.w.data_ptr(),
+                         self.alpha.data_ptr(), self.beta.data_ptr(), self.z.data_ptr(),
+                         self.theta.data_ptr(), self.phiT.data_ptr(), self.cnt_dk.data_ptr(),
+                         self.cnt_kw.data_ptr(), self.scratch.data_ptr(), self.seed)
+        h = C.c_void_p()
+        N.check(L.ab_lda_create(C.byref(desc), C.byref(h)), "ab_lda_create")
+        self._h = h
+        self._desc = desc
+        N.check(L.ab_lda_init_state(self._h, self.iteration, N.stream_ptr()), "ab_lda_init_state")
+
+    # ---- state -------------------------------------------------------------
+    def set_state(self, theta=None, phi=None, z=None, iteration=None):
+        if theta is not None:
+            self.theta.copy_(torch.as_tensor(np.asarray(theta, np.float64).reshape(self.D, self.K)))
+        if phi is not None:
+            ph = torch.as_tensor(np.asarray(phi, np.float64).reshape(self.K, self.V))
+            self.phiT[:, :self.K].copy_(ph.t())
+        if z is not None:
+            self.z.copy_(torch.as_tensor(np.asarray(z, np.int32).ravel()))
+        if iteration is not None:
+            self.iteration = int(iteration)
+        if getattr(self, "_h", None) is not None:
+            N.check(N.lib().ab_lda_init_state(self._h, self.iteration, N.stream_ptr()),
+                    "ab_lda_init_state")
+
+    def state(self):
+        """(theta [D,K], phi [K,V], z [T]) as host numpy arrays."""
+        return (self.theta.cpu().numpy(), self.phiT[:, :self.K].t().contiguous().cpu().numpy(),
+                self.z.cpu().numpy())
+
+    # ---- sampling ----------------------------------------------------------
+    def sweep(self, n=1, graph=True, stream=None):
+        N.check(N.lib().ab_lda_run(self._h, int(n), int(bool(graph)), N.stream_ptr(stream)),
+                "ab_lda_run")
+        self.iteration += int(n)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            N.lib().ab_lda_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def synthetic_corpus(K, V, D, mean_len, alpha, beta, seed):
+    """Documents from the LDA generative process (numpy, seeded): lengths
+    ~ Poisson(mean_len) (at least 1), theta ~ Dir(alpha), phi ~ Dir(beta)."""
+    rng = np.random.default_rng(seed)
+    lens = np.maximum(1, rng.poisson(mean_len, size=D)).astype(np.int64)
+    theta = rng.dirichlet(np.full(K, alpha), size=D)
+    phi = rng.dirichlet(np.full(V, beta), size=K)
+    off = np.zeros(D + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    T = int(off[-1])
+    doc_of = np.repeat(np.arange(D), lens)
+    # z per token by inverse CDF on theta rows, then w by inverse CDF on phi rows
+    u1, u2 = rng.random(T), rng.random(T)
+    ct = np.cumsum(theta, axis=1)
+    z = np.minimum((ct[doc_of] < u1[:, None]).sum(1), K - 1)
+    cp = np.cumsum(phi, axis=1)
+    w = np.empty(T, np.int64)
+    for k in range(K):
+        m = z == k
+        if m.any():
+            w[m] = np.minimum(np.searchsorted(cp[k], u2[m]), V - 1)
+    return off.astype(np.int32), w.astype(np.int32)

@@ -1,0 +1,120 @@
+/*
+ * augur_b200.h - C ABI of the B200 (sm_100a) backend for the MCMC samplers
+ * that AugurV2 compiles.
+ *
+ * In the reference, the Python front end (pyaugur/pyaugur/augurlib.py:
+ * 445-519) loads a per-model library generated by the Haskell compiler and
+ * calls augur_iface_init / augur_step / augur_cpy / augur_set_pt /
+ * augur_get_curr_ll through ctypes (compiler/augur/src/CudaC/CgStInit.hs:
+ * 474-602, CgKern.hs:232-238).  Those functions run the kernels of
+ * cbits/augur_mcmclib.h over generated log-density, gradient and Gibbs
+ * functions.  This library replaces that generated code and the cbits
+ * runtime with hand-written CUDA: each entry point below names the reference
+ * function or generated function it stands in for.
+ *
+ * Conventions (all entry points):
+ *  - plain C types only; arrays are DEVICE pointers owned by the caller;
+ *  - every call is enqueued on the caller's CUDA stream (`stream`, a
+ *    cudaStream_t passed as void*; NULL is the legacy default stream);
+ *  - the return value is a status (AB_OK == 0); on failure
+ *    ab_last_error() describes it.  Nothing calls exit();
+ *  - random draws come from Philox4x32-10 substreams addressed by
+ *    (draw, element, iteration, tag) under the 64-bit seed, so results are
+ *    reproducible and independent of launch shapes.
+ */
+#ifndef AUGUR_B200_H
+#define AUGUR_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status ------------------------------------------------------------ */
+enum {
+  AB_OK = 0,
+  AB_ERR_ARG = 1,      /* invalid argument (sizes, null pointers)          */
+  AB_ERR_CUDA = 2,     /* a CUDA runtime call or launch failed              */
+  AB_ERR_TIMEOUT = 3,  /* a bounded device-side wait gave up                */
+  AB_ERR_NUMERIC = 4,  /* non-finite value detected where one is forbidden  */
+  AB_ERR_STATE = 5     /* call not valid in the object's current state      */
+};
+
+/* Message of the calling thread's last failed call ("" if none).
+ * Replaces the reference's exit()-on-error (cbits/augur_util.c:30-36). */
+const char* ab_last_error(void);
+/* Library version string. */
+const char* ab_version(void);
+
+/* ======================================================================= *
+ * LDA Gibbs (model compiler/augur/test/lda.rv, schedule
+ *   ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z])
+ * Layouts: w, z int32[T] (documents contiguous); doc_off int32[D+1];
+ * theta f64[D][K]; phiT f64[V][Kp] word-major with Kp = ab_lda_phi_stride(K);
+ * cnt_dk int32[D][K]; cnt_kw int32[K][V].
+ * ======================================================================= */
+
+/* Row stride (in doubles) of phiT for K topics. */
+int ab_lda_phi_stride(int K);
+
+/* Count statistics of z: replaces the generated conj_stat_theta and
+ * conj_stat_phi (CgConj.hs:171-177) with the reset of CgKern.hs:103-107.
+ * Overwrites both tables. */
+int ab_lda_count(int D, int K, int V, const int* doc_off, const int* w, const int* z,
+                 int* cnt_dk, int* cnt_kw, void* stream);
+
+/* theta[d] ~ Dirichlet(alpha + cnt_dk[d]) for every d: replaces the generated
+ * conj_samp_theta (CgConj.hs:278-299) over augur_dirichlet_categorical_conj
+ * (cbits/augur_dist.c:526-538).  Element (d,k) draws from substream
+ * (d*K+k, iter, 2). */
+int ab_lda_conj_theta(int D, int K, const double* alpha, const int* cnt_dk, double* theta,
+                      uint64_t seed, uint32_t iter, void* stream);
+
+/* phi[k] ~ Dirichlet(beta + cnt_kw[k]) stored as phiT: replaces conj_samp_phi.
+ * Element (k,v) draws from substream (k*V+v, iter, 3).  clear_counts != 0
+ * zeroes cnt_kw after reading it. */
+int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
+                    int clear_counts, uint64_t seed, uint32_t iter, void* stream);
+
+/* z[t] ~ p(z | theta, phi) for every token: replaces the generated disc_z
+ * (CgDisc.hs:122-156) over augur_unnorm_disc_samp (cbits/augur_dist.c:
+ * 798-813); token t draws one uniform from substream (t, iter, 1).  If the
+ * count tables are given, cnt_dk is overwritten with the counts of the new z
+ * and the counts of the new z are ADDED to cnt_kw (pass it zeroed). */
+int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                  const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                  uint32_t iter, void* stream);
+
+/* Sweep runner: the whole augur_step of the LDA schedule (CgKern.hs:232-238)
+ * as a captured CUDA graph of three kernels. */
+typedef struct ab_lda_desc {
+  int D, K, V;
+  const int* doc_off;   /* [D+1] */
+  const int* w;         /* [T]   */
+  const double* alpha;  /* [K]   */
+  const double* beta;   /* [V]   */
+  int* z;               /* [T]   */
+  double* theta;        /* [D][K] */
+  double* phiT;         /* [V][Kp] */
+  int* cnt_dk;          /* [D][K] */
+  int* cnt_kw;          /* [K][V] */
+  void* scratch;        /* ab_lda_scratch_bytes() bytes of device memory */
+  uint64_t seed;
+} ab_lda_desc;
+
+typedef struct ab_lda ab_lda;
+size_t ab_lda_scratch_bytes(void);
+/* Replaces augur_iface_init for the LDA model (CgStInit.hs:474-510); the
+ * caller owns every buffer named by the descriptor. */
+int ab_lda_create(const ab_lda_desc* desc, ab_lda** out);
+/* Sets the iteration counter and rebuilds the counts from the current z. */
+int ab_lda_init_state(ab_lda* h, uint32_t iter, void* stream);
+/* n_sweeps augur_step calls; use_graph selects graph replay. */
+int ab_lda_run(ab_lda* h, int n_sweeps, int use_graph, void* stream);
+int ab_lda_destroy(ab_lda* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AUGUR_B200_H */

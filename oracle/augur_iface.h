@@ -1,0 +1,27 @@
+/*
+ * ORACLE (test infrastructure only).  Stand-in for the per-model header that
+ * the reference compiler generates (written by pyaugur/pyaugur/augurlib.py:
+ * 318-332, included by cbits/augur_mcmclib.h:26).  It declares the model
+ * state records that the restated generated functions in ref_models.c pass
+ * to the reference's MCMC kernels.
+ */
+#ifndef AUGUR_IFACE_H
+#define AUGUR_IFACE_H
+#include <augur_vecop.h>
+#include <augur_dist.h>
+
+typedef struct AugurMod {
+  /* HLR block state */
+  AugurVec_t* theta;   /* Vec Real [K] */
+  double* b;           /* Real */
+  double* v;           /* Real */
+  /* GMM means (ESlice / MWG) */
+  AugurVec_t* mu;      /* Vec (Vec Real) [K][d] flattened per component */
+} AugurMod_t;
+
+typedef struct AugurAux {
+  augur_rng* rng;
+  void* model;         /* model-specific data record (ref_models.c) */
+} AugurAux_t;
+
+#endif

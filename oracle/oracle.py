@@ -1,0 +1,143 @@
+"""ORACLE (test infrastructure only).
+
+ctypes front end of the two CPU checkers:
+
+* ``Oracle("oracle")`` - the standalone C restatement (oracle/augur_oracle.c,
+  built into oracle/_build/liboracle.so);
+* ``Oracle("ref")`` - the reference's own cbits runtime compiled in place with
+  the GSL shim and the restated generated code (oracle/_ref/libaugur_ref.so).
+
+Both export the same functions under the prefixes ``orc_`` and ``ref_``; this
+module hides the prefix so a test can run the same call on both and compare.
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBS = {
+    "oracle": os.path.join(HERE, "_build", "liboracle.so"),
+    "ref": os.path.join(HERE, "_ref", "libaugur_ref.so"),
+}
+PREFIX = {"oracle": "orc_", "ref": "ref_"}
+
+TAG_Z, TAG_THETA, TAG_PHI, TAG_MOM, TAG_HMC, TAG_NUTS = 1, 2, 3, 4, 5, 6
+TAG_PI, TAG_MU, TAG_COV, TAG_ESLICE, TAG_MWG, TAG_INIT, TAG_DATA = 7, 8, 9, 10, 11, 12, 13
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u32p = C.POINTER(C.c_uint32)
+
+
+def build_oracle():
+    """Compile the standalone oracle (and the reference build when the
+    reference sources are present) with oracle/Makefile."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
+    if os.path.isdir(os.environ.get("REF_SRC", "/root/reference/cbits")):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+
+
+def available(kind):
+    return os.path.exists(LIBS[kind])
+
+
+def dptr(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_ip)
+
+
+class Oracle:
+    def __init__(self, kind="oracle"):
+        path = LIBS[kind]
+        if not os.path.exists(path):
+            if kind == "oracle":
+                build_oracle()
+            else:
+                raise FileNotFoundError(path)
+        self.kind = kind
+        self.lib = C.CDLL(path)
+        self.p = PREFIX[kind]
+
+    def fn(self, name, restype=None):
+        f = getattr(self.lib, self.p + name)
+        f.restype = restype
+        return f
+
+    # ---- scalar samplers --------------------------------------------------
+    def gamma_sample(self, shape, rate, seed, elem, it, tag):
+        f = self.fn("gamma_sample", C.c_double)
+        f.argtypes = [C.c_double, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        return f(shape, rate, seed, elem, it, tag)
+
+    def unnorm_disc_samp(self, pmf, seed, elem, it, tag):
+        pmf = np.ascontiguousarray(pmf, dtype=np.float64)
+        f = self.fn("unnorm_disc_samp", C.c_int)
+        f.argtypes = [_dp, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        return f(dptr(pmf), len(pmf), seed, elem, it, tag)
+
+    def philox_block(self, ctr, key):
+        ctr = np.asarray(ctr, dtype=np.uint32)
+        out = np.zeros(4, dtype=np.uint32)
+        f = self.fn("philox_block")
+        f(ctr.ctypes.data_as(_u32p), C.c_uint32(key[0]), C.c_uint32(key[1]), out.ctypes.data_as(_u32p))
+        return out
+
+    def draws(self, seed, elem, it, tag, n, normal=False):
+        out = np.zeros(n, dtype=np.float64)
+        f = self.fn("draws")
+        f.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, _dp]
+        f(seed, elem, it, tag, n, int(normal), dptr(out))
+        return out
+
+    # ---- LDA ----------------------------------------------------------------
+    def lda_disc_z(self, doc_off, w, theta, phi, z, seed, it):
+        D, K = theta.shape
+        V = phi.shape[1]
+        f = self.fn("lda_disc_z")
+        f.argtypes = [C.c_int] * 3 + [_ip, _ip, _dp, _dp, _ip, C.c_uint64, C.c_uint32]
+        f(D, K, V, iptr(doc_off), iptr(w), dptr(theta), dptr(phi), iptr(z), seed, it)
+        return z
+
+    def lda_conj_stat(self, doc_off, w, z, D, K, V):
+        cnt_dk = np.zeros((D, K), np.int32)
+        cnt_kw = np.zeros((K, V), np.int32)
+        f = self.fn("lda_conj_stat")
+        f.argtypes = [C.c_int] * 3 + [_ip, _ip, _ip, _ip, _ip]
+        f(D, K, V, iptr(doc_off), iptr(w), iptr(z), iptr(cnt_dk), iptr(cnt_kw))
+        return cnt_dk, cnt_kw
+
+    def lda_conj_theta(self, alpha, cnt_dk, seed, it):
+        D, K = cnt_dk.shape
+        out = np.zeros((D, K), np.float64)
+        f = self.fn("lda_conj_theta")
+        f.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.c_uint64, C.c_uint32]
+        f(D, K, dptr(alpha), iptr(cnt_dk), dptr(out), seed, it)
+        return out
+
+    def lda_conj_phi(self, beta, cnt_kw, seed, it):
+        K, V = cnt_kw.shape
+        out = np.zeros((K, V), np.float64)
+        f = self.fn("lda_conj_phi")
+        f.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.c_uint64, C.c_uint32]
+        f(K, V, dptr(beta), iptr(cnt_kw), dptr(out), seed, it)
+        return out
+
+    def lda_sweeps(self, doc_off, w, alpha, beta, theta, phi, z, seed, it0, n):
+        D, K = theta.shape
+        V = phi.shape[1]
+        cnt_dk = np.zeros((D, K), np.int32)
+        cnt_kw = np.zeros((K, V), np.int32)
+        f = self.fn("lda_sweeps")
+        f.argtypes = [C.c_int] * 3 + [_ip, _ip, _dp, _dp, _dp, _dp, _ip, _ip, _ip,
+                                      C.c_uint64, C.c_uint32, C.c_int]
+        f(D, K, V, iptr(doc_off), iptr(w), dptr(alpha), dptr(beta), dptr(theta), dptr(phi),
+          iptr(z), iptr(cnt_dk), iptr(cnt_kw), seed, it0, n)
+        return theta, phi, z

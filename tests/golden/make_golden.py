@@ -1,0 +1,107 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a checkout that has the reference sources (default /root/reference,
+override with REF_ROOT):  python tests/golden/make_golden.py
+
+* The reference's runtime (cbits) is compiled in place with the GSL shim and
+  the restated generated code (oracle/Makefile `ref`) and executed through
+  oracle/oracle.py with kind "ref"; its outputs are the expected values.
+* Model fixtures that the reference ships (examples/lda.py's d4_k4_v8 corpus)
+  are read out of the reference's example file with `ast`, not retyped.
+The fixtures are small .npz files; the tests read only these files, never the
+reference.
+"""
+import ast
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+
+from oracle import oracle as O  # noqa: E402
+
+
+def example_arrays(path, func_name):
+    """Literal np.array(...) assignments inside one function of a reference
+    example script, evaluated without running the script.  The examples are
+    Python 2, so `print x` statement lines are dropped before parsing."""
+    lines = [ln for ln in open(path).read().splitlines()
+             if not ln.strip().startswith(("print ", "get_ipython"))]
+    tree = ast.parse("\n".join(lines))
+    out = {}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.FunctionDef) and node.name == func_name:
+            for st in node.body:
+                if (isinstance(st, ast.Assign) and len(st.targets) == 1
+                        and isinstance(st.targets[0], ast.Name) and isinstance(st.value, ast.Call)
+                        and getattr(st.value.func, "attr", "") == "array" and st.value.args
+                        and isinstance(st.value.args[0], ast.List)):
+                    try:
+                        out[st.targets[0].id] = ast.literal_eval(st.value.args[0])
+                    except ValueError:
+                        pass
+    return out
+
+
+def lda_fixture_d4_k4_v8():
+    arrs = example_arrays(os.path.join(REF_ROOT, "examples", "lda.py"), "mk_synthetic_dataset_d4_k4_v8")
+    docs = [np.array(arrs[k], np.int32) for k in ("w1", "w2", "w3", "w4")]
+    N = np.array(arrs["N"], np.int32)
+    assert [len(d) for d in docs] == list(N)
+    return docs
+
+
+def make_primitives(ref):
+    shapes = np.array([0.01, 0.05, 0.1, 0.5, 0.99, 1.0, 1.01, 2.5, 3.7, 10.0, 50.0, 200.5])
+    gam = np.array([[ref.gamma_sample(s, r, 11, e, 3, O.TAG_PHI) for e in range(8)]
+                    for s, r in [(s, 1.0) for s in shapes] + [(2.0, 0.5), (0.3, 4.0)]])
+    rng = np.random.default_rng(5)
+    pmfs = rng.random((64, 7)) ** 3
+    pmfs[3, :] = 0.0
+    pmfs[3, 4] = 1.0
+    disc = np.array([ref.unnorm_disc_samp(p, 19, i, 2, O.TAG_Z) for i, p in enumerate(pmfs)], np.int32)
+    np.savez_compressed(os.path.join(HERE, "primitives.npz"), shapes=shapes, gamma=gam,
+                        pmfs=pmfs, disc=disc)
+
+
+def make_lda(ref):
+    # (1) the reference's own example corpus, 10 sweeps from the uniform init
+    docs = lda_fixture_d4_k4_v8()
+    D, K, V = 4, 4, 8
+    off = np.concatenate([[0], np.cumsum([len(d) for d in docs])]).astype(np.int32)
+    w = np.concatenate(docs).astype(np.int32)
+    alpha, beta = np.full(K, 0.1), np.full(V, 0.01)
+    theta, phi = np.full((D, K), 1.0 / K), np.full((K, V), 1.0 / V)
+    z = np.zeros(len(w), np.int32)
+    thetas, phis, zs = [], [], []
+    for s in range(10):
+        ref.lda_sweeps(off, w, alpha, beta, theta, phi, z, 0, s, 1)
+        thetas.append(theta.copy()); phis.append(phi.copy()); zs.append(z.copy())
+    np.savez_compressed(os.path.join(HERE, "lda_d4_k4_v8.npz"), doc_off=off, w=w, alpha=alpha,
+                        beta=beta, theta=np.array(thetas), phi=np.array(phis), z=np.array(zs))
+
+    # (2) a synthetic corpus of the benchmark's shape family, reduced size
+    from augurv2_b200.lda import synthetic_corpus
+    K, V, D = 12, 300, 40
+    off, w = synthetic_corpus(K, V, D, 60, 0.1, 0.01, seed=3)
+    alpha, beta = np.full(K, 0.1), np.full(V, 0.01)
+    rng = np.random.default_rng(4)
+    theta = rng.dirichlet(np.full(K, 0.5), size=D)
+    phi = rng.dirichlet(np.full(V, 0.1), size=K)
+    z = rng.integers(0, K, size=len(w)).astype(np.int32)
+    theta0, phi0, z0 = theta.copy(), phi.copy(), z.copy()
+    ref.lda_sweeps(off, w, alpha, beta, theta, phi, z, 7, 0, 3)
+    np.savez_compressed(os.path.join(HERE, "lda_k12_v300_d40.npz"), doc_off=off, w=w, alpha=alpha,
+                        beta=beta, theta0=theta0, phi0=phi0, z0=z0, theta=theta, phi=phi, z=z)
+
+
+if __name__ == "__main__":
+    O.build_oracle()
+    ref = O.Oracle("ref")
+    make_primitives(ref)
+    make_lda(ref)
+    print("golden fixtures written to", HERE)

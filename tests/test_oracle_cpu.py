@@ -1,0 +1,106 @@
+"""Pins the CPU oracle: Philox known-answer vectors, the golden fixtures made
+from the reference's own runtime, and (when the reference build is present)
+live bit-for-bit agreement with it."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def orc():
+    return O.Oracle("oracle")
+
+
+@pytest.fixture(scope="module")
+def ref():
+    if not O.available("ref"):
+        pytest.skip("reference build oracle/_ref not present")
+    return O.Oracle("ref")
+
+
+# Random123 known-answer vectors for philox4x32-10.
+KAT = [
+    ([0, 0, 0, 0], [0, 0], [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]),
+    ([0xffffffff] * 4, [0xffffffff] * 2, [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]),
+    ([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0],
+     [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]),
+]
+
+
+@pytest.mark.parametrize("ctr,key,expect", KAT)
+def test_philox_kat(orc, ctr, key, expect):
+    assert list(orc.philox_block(ctr, key)) == expect
+
+
+def test_uniforms_open_interval(orc):
+    u = orc.draws(1, 2, 3, 4, 20000)
+    assert u.min() > 0.0 and u.max() < 1.0
+    assert abs(u.mean() - 0.5) < 0.01
+    n = orc.draws(1, 2, 3, 5, 20000, normal=True)
+    assert abs(n.mean()) < 0.03 and abs(n.std() - 1.0) < 0.03
+
+
+def test_primitives_golden(orc):
+    g = np.load(os.path.join(GOLD, "primitives.npz"))
+    shapes = list(g["shapes"]) + [2.0, 0.3]
+    rates = [1.0] * len(g["shapes"]) + [0.5, 4.0]
+    got = np.array([[orc.gamma_sample(s, r, 11, e, 3, O.TAG_PHI) for e in range(8)]
+                    for s, r in zip(shapes, rates)])
+    np.testing.assert_array_equal(got, g["gamma"])
+    disc = [orc.unnorm_disc_samp(p, 19, i, 2, O.TAG_Z) for i, p in enumerate(g["pmfs"])]
+    np.testing.assert_array_equal(disc, g["disc"])
+
+
+def test_lda_golden_reference_fixture(orc):
+    """examples/lda.py d4_k4_v8 corpus: 10 sweeps equal the reference's."""
+    g = np.load(os.path.join(GOLD, "lda_d4_k4_v8.npz"))
+    D, K, V = 4, 4, 8
+    theta, phi = np.full((D, K), 1.0 / K), np.full((K, V), 1.0 / V)
+    z = np.zeros(len(g["w"]), np.int32)
+    for s in range(10):
+        orc.lda_sweeps(g["doc_off"], g["w"], g["alpha"], g["beta"], theta, phi, z, 0, s, 1)
+        np.testing.assert_array_equal(theta, g["theta"][s])
+        np.testing.assert_array_equal(phi, g["phi"][s])
+        np.testing.assert_array_equal(z, g["z"][s])
+
+
+def test_lda_golden_synthetic(orc):
+    g = np.load(os.path.join(GOLD, "lda_k12_v300_d40.npz"))
+    th, ph, z = g["theta0"].copy(), g["phi0"].copy(), g["z0"].copy()
+    orc.lda_sweeps(g["doc_off"], g["w"], g["alpha"], g["beta"], th, ph, z, 7, 0, 3)
+    np.testing.assert_array_equal(th, g["theta"])
+    np.testing.assert_array_equal(ph, g["phi"])
+    np.testing.assert_array_equal(z, g["z"])
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_lda_oracle_vs_reference_live(orc, ref, seed):
+    rng = np.random.default_rng(seed)
+    D, K, V = 7, 5, 23
+    lens = rng.integers(0, 15, size=D)          # includes empty documents
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.int32)
+    w = rng.integers(0, V, size=off[-1]).astype(np.int32)
+    alpha, beta = rng.random(K) + 0.05, rng.random(V) * 0.1 + 0.005
+    th0 = rng.dirichlet(np.ones(K), size=D); ph0 = rng.dirichlet(np.ones(V), size=K)
+    z0 = rng.integers(0, K, size=off[-1]).astype(np.int32)
+    a = orc.lda_sweeps(off, w, alpha, beta, th0.copy(), ph0.copy(), z0.copy(), seed, 5, 4)
+    b = ref.lda_sweeps(off, w, alpha, beta, th0.copy(), ph0.copy(), z0.copy(), seed, 5, 4)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_gamma_oracle_vs_reference_live(orc, ref):
+    for s in [0.001, 0.02, 0.7, 1.0, 1.5, 8.0, 1e3]:
+        for e in range(50):
+            assert orc.gamma_sample(s, 1.3, 3, e, 1, 2) == ref.gamma_sample(s, 1.3, 3, e, 1, 2)
+
+
+def test_gamma_moments(orc):
+    for s in [0.1, 1.0, 4.0]:
+        x = np.array([orc.gamma_sample(s, 2.0, 9, e, 0, 2) for e in range(20000)])
+        assert abs(x.mean() - s / 2.0) < 5 * np.sqrt(s / 4.0 / 20000)
