@@ -67,9 +67,10 @@ _SIGS = {
     "ab_lda_phi_stride": (i32, [i32]),
     "ab_lda_count": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp]),
     "ab_lda_conj_theta": (i32, [i32, i32, vp, vp, vp, u64, u32, vp]),
-    "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp]),
+    "ab_lda_phi_scratch_bytes": (sz, [i32, i32]),
+    "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp, vp]),
     "ab_lda_disc_z": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
-    "ab_lda_scratch_bytes": (sz, []),
+    "ab_lda_scratch_bytes": (sz, [i32, i32]),
     "ab_lda_create": (i32, [C.POINTER(LdaDesc), C.POINTER(vp)]),
     "ab_lda_init_state": (i32, [vp, u32, vp]),
     "ab_lda_run": (i32, [vp, i32, i32, vp]),

@@ -16,7 +16,8 @@
 // One sweep is three kernels:
 //   lda_theta_kernel  theta[d] ~ Dir(alpha + cnt_dk[d])      (reads cnt_dk)
 //   lda_phi_kernel    phi[k]   ~ Dir(beta + cnt_kw[k])       (reads, then
-//                     clears cnt_kw); one thread-block cluster per topic
+//                     clears cnt_kw); one draw per thread, the last CTA of
+//                     each topic normalises it
 //   lda_z_kernel      z ~ p(z | theta, phi), and the counts of the new z
 //                     (cnt_dk rows written whole, cnt_kw incremented)
 // The count statistics of the reference (conj_stat_*, rebuilt from zero each
@@ -28,16 +29,11 @@
 // (_rn intrinsics; this file is also compiled with -fmad=false), so given the
 // same theta, phi and Philox uniforms the assignments and counts equal the
 // reference's CPU sampler's bit for bit.
-#include <cooperative_groups.h>
-
 #include "common.cuh"
 #include "dist.cuh"
 
-namespace cg = cooperative_groups;
-
 namespace ab {
 
-constexpr int LDA_PHI_CLUSTER = 4;     // CTAs per topic row in the phi kernel
 constexpr int LDA_THREADS = 256;
 constexpr int LDA_MAX_K = 1024;
 
@@ -52,7 +48,7 @@ __device__ __forceinline__ uint32_t read_iter(const uint32_t* iter_dev, uint32_t
 // theta is bit-identical to the reference given identical gamma draws.
 // Block: R = 256 / K rows (or one row looped when K > 256).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(LDA_THREADS)
+__global__ void __launch_bounds__(LDA_THREADS, 5)
 lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
                  const int* __restrict__ cnt_dk, double* __restrict__ theta,
                  uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
@@ -87,100 +83,152 @@ lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
 
 // ---------------------------------------------------------------------------
 // phi[k][v] = g[k][v] / sum_v g[k][v], g ~ Gamma(beta_v + cnt[k][v], 1),
-// stored word-major into phiT[v][k].  One cluster of LDA_PHI_CLUSTER CTAs per
-// topic: each CTA draws its slice of V into phiT (and clears the counts it
-// read), reduces its partial sum in a fixed order, publishes it in shared
-// memory, and after a cluster barrier every CTA adds the partials of all
-// CTAs of the cluster (distributed shared memory) in rank order and
-// normalises its slice.  The sum is deterministic but not in the reference's
-// sequential order, so phi matches the reference to rounding, not bitwise.
+// stored word-major into phiT[v][k].  The K*V gamma draws are spread one per
+// thread over K * B CTAs (B CTAs per topic).  Each CTA writes its draws
+// unnormalised into phiT, clears the counts it read, and stores its fixed-
+// order partial sum in scratch; the last CTA of a topic to finish (counted
+// with an atomic ticket) adds the B partials in CTA order and normalises the
+// topic's column of phiT.  The sum is deterministic but not in the
+// reference's sequential order, so phi matches the reference to rounding,
+// not bitwise.
+// Scratch: uint32 ticket[K] (zero on entry, left zero) | double partial[K][B].
 // ---------------------------------------------------------------------------
-__global__ void __cluster_dims__(LDA_PHI_CLUSTER, 1, 1) __launch_bounds__(LDA_THREADS)
-lda_phi_kernel(int K, int V, int Kp, const double* __restrict__ beta,
+__global__ void __launch_bounds__(LDA_THREADS, 5)
+lda_phi_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta,
                int* __restrict__ cnt_kw, double* __restrict__ phiT, int clear_counts,
+               uint32_t* __restrict__ ticket, double* __restrict__ partial,
                uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
   __shared__ double red[33];
-  __shared__ double partial;
-  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ bool last;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
-  const int k = blockIdx.x / LDA_PHI_CLUSTER;
-  const int rank = (int)cluster.block_rank();
-  const int per = (V + LDA_PHI_CLUSTER - 1) / LDA_PHI_CLUSTER;
-  const int v0 = rank * per;
-  const int v1 = min(V, v0 + per);
-  double local = 0.0;
-  if (k < K) {
-    for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
-      const size_t idx = (size_t)k * V + v;
-      const int c = cnt_kw[idx];
-      if (clear_counts) cnt_kw[idx] = 0;
-      Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
-      const double g = gamma_draw(s, __dadd_rn(beta[v], (double)c), 1.0);
-      phiT[(size_t)v * Kp + k] = g;
-      local = __dadd_rn(local, g);
-    }
+  const int k = blockIdx.x / B;
+  const int b = blockIdx.x - k * B;
+  const int v = b * LDA_THREADS + threadIdx.x;
+  double g = 0.0;
+  if (v < V) {
+    const size_t idx = (size_t)k * V + v;
+    const int c = cnt_kw[idx];
+    if (clear_counts) cnt_kw[idx] = 0;
+    Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
+    g = gamma_draw(s, __dadd_rn(beta[v], (double)c), 1.0);
+    phiT[(size_t)v * Kp + k] = g;
   }
-  const double bsum = block_sum_f64(local, red);
-  if (threadIdx.x == 0) partial = bsum;
-  cluster.sync();
+  const double bsum = block_sum_f64(g, red);
+  if (threadIdx.x == 0) {
+    partial[(size_t)k * B + b] = bsum;
+    __threadfence();
+    last = atomicAdd(ticket + k, 1u) == (unsigned)(B - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
   double norm = 0.0;
-  for (int r = 0; r < LDA_PHI_CLUSTER; ++r) {
-    const double* p = cluster.map_shared_rank(&partial, r);
-    norm = __dadd_rn(norm, *p);
+  for (int i = 0; i < B; ++i) norm = __dadd_rn(norm, __ldcg(partial + (size_t)k * B + i));
+  for (int vv = threadIdx.x; vv < V; vv += blockDim.x) {
+    double* p = phiT + (size_t)vv * Kp + k;
+    *p = __ddiv_rn(__ldcg(p), norm);
   }
-  if (k < K) {
-    for (int v = v0 + threadIdx.x; v < v1; v += blockDim.x) {
-      const size_t o = (size_t)v * Kp + k;
-      phiT[o] = __ddiv_rn(phiT[o], norm);
-    }
-  }
-  cluster.sync();  // keep `partial` alive until every CTA has read it
+  if (threadIdx.x == 0) ticket[k] = 0u;
 }
 
+static inline int lda_phi_blocks(int V) { return (V + LDA_THREADS - 1) / LDA_THREADS; }
+
 // ---------------------------------------------------------------------------
-// z[t] for every token of document d (one CTA per document):
+// z[t] for every token of document d (one CTA per document, one thread per
+// token):
 //   pmf_k  = (1 * theta[d][k]) * phi[k][w]                (CgDisc.hs:132-139)
 //   norm   = sum_k pmf_k  (sequential)                    (augur_dist.c:800-803)
 //   z      = first i with u < sum_{j<=i} pmf_j / norm      (:805-812)
-// The products are recomputed in the second pass instead of stored; they are
-// the same binary64 values.  Counts of the new z: the document's row of
-// cnt_dk is accumulated in shared memory and stored whole; cnt_kw receives
-// warp-aggregated atomic increments (lanes with the same (z, w) key elect
-// one leader that adds the group size).
+// The norm pass reads the token's phi row with 16-byte loads and records the
+// running sum at 8 checkpoints.  The reference's running quotient sum is
+// replaced by a division-free test (comment in the code) evaluated first at
+// the checkpoints and then inside the one block that contains the answer;
+// only a u within rounding distance of a boundary runs the reference loop
+// itself.  The products are recomputed where needed; they are the same
+// binary64 values.
+// Counts of the new z: the document's row of cnt_dk is accumulated in shared
+// memory and stored whole; cnt_kw receives warp-aggregated atomic increments
+// (lanes with the same (z, w) key elect one leader that adds the group size).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(LDA_THREADS)
+constexpr int LDA_Z_THREADS = 128;
+constexpr int LDA_Z_CP = 8;            // checkpoints of the running sum
+
+__global__ void __launch_bounds__(LDA_Z_THREADS)
 lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
              const int* __restrict__ w, const double* __restrict__ theta,
              const double* __restrict__ phiT, int* __restrict__ z,
              int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
              uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
   extern __shared__ double smem[];
-  double* th = smem;                                   // [K]
-  int* hist = reinterpret_cast<int*>(smem + K);        // [K]
+  double* th = smem;                                    // [Kp] (zero padded)
+  int* hist = reinterpret_cast<int*>(smem + Kp);        // [K]
+  const int lane = threadIdx.x & 31;
   const int d = blockIdx.x;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
-  for (int k = threadIdx.x; k < K; k += blockDim.x) {
-    th[k] = theta[(size_t)d * K + k];
-    hist[k] = 0;
+  for (int k = threadIdx.x; k < Kp; k += blockDim.x) {
+    th[k] = k < K ? theta[(size_t)d * K + k] : 0.0;
+    if (k < K) hist[k] = 0;
   }
   __syncthreads();
   const int t0 = doc_off[d], t1 = doc_off[d + 1];
+  // Checkpoint block length (even, so blocks start on 16-byte boundaries).
+  const int S = (((K + LDA_Z_CP - 1) / LDA_Z_CP) + 1) & ~1;
+  const double m = (6.0 * K + 32.0) * 1.1102230246251565e-16;
+  const double lo = 1.0 - m, hi = 1.0 + m;
   for (int tb = t0; tb < t1; tb += blockDim.x) {
     const int t = tb + threadIdx.x;
     const bool active = t < t1;
-    int zk = 0, wt = 0;
+    const int wt = active ? w[t] : 0;
+    int zk = 0;
     if (active) {
-      wt = w[t];
       const double* row = phiT + (size_t)wt * Kp;
+      double cp[LDA_Z_CP];
       double norm = 0.0;
-      for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], __ldg(row + k)));
+#pragma unroll
+      for (int c = 0; c < LDA_Z_CP; ++c) {
+        const int k1 = min(K, (c + 1) * S);
+        for (int k = c * S; k < k1; k += 2) {
+          const double2 f = __ldg(reinterpret_cast<const double2*>(row + k));
+          const double2 g = *reinterpret_cast<const double2*>(th + k);
+          norm = __dadd_rn(norm, __dmul_rn(g.x, f.x));
+          if (k + 1 < k1) norm = __dadd_rn(norm, __dmul_rn(g.y, f.y));
+        }
+        cp[c] = norm;
+      }
       Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
       const double u = s.uniform();
-      double acc = __ddiv_rn(__dmul_rn(th[0], __ldg(row)), norm);
+      // Division-free decision.  With c_j the running sum of the products,
+      // u < acc_j (the reference's running sum of pmf_i / norm) holds when
+      // u*norm < c_j (1 - m) and fails when u*norm > c_j (1 + m); m bounds
+      // the rounding of both running sums, the quotients and the products
+      // (|error| <= (2j + 3) 2^-53 relative, plus subnormal slack).  c_j is
+      // nondecreasing, so a checkpoint with u*norm > c (1 + m) rules out its
+      // whole block.  A u within m of a boundary takes the reference loop.
+      bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
       zk = K - 1;
-      for (int i = 1; i < K; ++i) {
-        if (u < acc) { zk = i - 1; break; }
-        acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], __ldg(row + i)), norm));
+      if (!exact) {
+        const double un = __dmul_rn(u, norm);
+        int blk = LDA_Z_CP - 1;
+        double c = cp[LDA_Z_CP - 2];
+#pragma unroll
+        for (int i = LDA_Z_CP - 2; i >= 0; --i)
+          if (un <= __dmul_rn(cp[i], hi)) { blk = i; c = i > 0 ? cp[i - 1] : 0.0; }
+        const int j1 = min(K - 1, (blk + 1) * S);
+        for (int j = blk * S; j < j1; ++j) {
+          c = __dadd_rn(c, __dmul_rn(th[j], __ldg(row + j)));
+          if (un < __dmul_rn(c, lo)) { zk = j; break; }
+          if (un <= __dmul_rn(c, hi)) { exact = true; break; }
+        }
+      }
+      if (exact) {
+        norm = 0.0;
+        for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], __ldg(row + k)));
+        double acc = __ddiv_rn(__dmul_rn(th[0], __ldg(row)), norm);
+        zk = K - 1;
+        for (int i = 1; i < K; ++i) {
+          if (u < acc) { zk = i - 1; break; }
+          acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], __ldg(row + i)), norm));
+        }
       }
       z[t] = zk;
       atomicAdd(&hist[zk], 1);
@@ -191,7 +239,7 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
         const long long key = (long long)zk * V + wt;
         const unsigned peers = __match_any_sync(mask, key);
         const int leader = __ffs(peers) - 1;
-        if ((int)(threadIdx.x & 31) == leader) atomicAdd(cnt_kw + key, __popc(peers));
+        if (lane == leader) atomicAdd(cnt_kw + key, __popc(peers));
       }
     }
   }
@@ -252,10 +300,21 @@ int launch_lda_theta(int D, int K, const double* alpha, const int* cnt_dk, doubl
   return AB_OK;
 }
 
+size_t lda_phi_scratch(int K, int V) {
+  return 256 + (((size_t)K * 4 + 255) & ~(size_t)255) + sizeof(double) * (size_t)K * lda_phi_blocks(V);
+}
+
+// scratch: [0,256) reserved for the sweep runner's counters, then ticket[K]
+// (256-byte aligned), then partial[K][B].
 int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double* phiT, int clear,
-                   uint64_t seed, const uint32_t* iter_dev, uint32_t iter, cudaStream_t st) {
-  lda_phi_kernel<<<K * LDA_PHI_CLUSTER, LDA_THREADS, 0, st>>>(K, V, Kp, beta, cnt_kw, phiT, clear,
-                                                              seed, iter_dev, iter);
+                   void* scratch, uint64_t seed, const uint32_t* iter_dev, uint32_t iter,
+                   cudaStream_t st) {
+  const int B = lda_phi_blocks(V);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + 256);
+  double* partial = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256 +
+                                              ((((size_t)K * 4) + 255) & ~(size_t)255));
+  lda_phi_kernel<<<K * B, LDA_THREADS, 0, st>>>(K, V, Kp, B, beta, cnt_kw, phiT, clear, ticket,
+                                                partial, seed, iter_dev, iter);
   AB_LAUNCH_CHECK("lda_phi_kernel");
   return AB_OK;
 }
@@ -263,9 +322,9 @@ int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double
 int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
                  const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
-  const size_t smem = sizeof(double) * K + sizeof(int) * K;
-  lda_z_kernel<<<D, 128, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed,
-                                      iter_dev, iter, done_ctr);
+  const size_t smem = sizeof(double) * (size_t)Kp + sizeof(int) * (size_t)K;
+  lda_z_kernel<<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw,
+                                                seed, iter_dev, iter, done_ctr);
   AB_LAUNCH_CHECK("lda_z_kernel");
   return AB_OK;
 }
@@ -303,13 +362,20 @@ extern "C" int ab_lda_conj_theta(int D, int K, const double* alpha, const int* c
   return launch_lda_theta(D, K, alpha, cnt_dk, theta, seed, nullptr, iter, as_stream(stream));
 }
 
+extern "C" size_t ab_lda_phi_scratch_bytes(int K, int V) {
+  return (K > 0 && V > 0) ? lda_phi_scratch(K, V) : 0;
+}
+
 extern "C" int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
-                               int clear_counts, uint64_t seed, uint32_t iter, void* stream) {
+                               int clear_counts, uint64_t seed, uint32_t iter, void* scratch,
+                               void* stream) {
   int rc = check_lda_dims(1, K, V);
   if (rc) return rc;
-  AB_REQUIRE(beta && cnt_kw && phiT, AB_ERR_ARG, "ab_lda_conj_phi: null pointer");
-  return launch_lda_phi(K, V, lda_kp(K), beta, cnt_kw, phiT, clear_counts, seed, nullptr, iter,
-                        as_stream(stream));
+  AB_REQUIRE(beta && cnt_kw && phiT && scratch, AB_ERR_ARG, "ab_lda_conj_phi: null pointer");
+  cudaStream_t st = as_stream(stream);
+  AB_CUDA(cudaMemsetAsync(static_cast<char*>(scratch) + 256, 0, (size_t)K * 4, st));
+  return launch_lda_phi(K, V, lda_kp(K), beta, cnt_kw, phiT, clear_counts, scratch, seed, nullptr,
+                        iter, st);
 }
 
 extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int* w,
@@ -343,7 +409,8 @@ static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
   AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
   int rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, main);
   if (rc) return rc;
-  rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.seed, iter_dev, 0, side);
+  rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.scratch, d.seed, iter_dev, 0,
+                      side);
   if (rc) return rc;
   AB_CUDA(cudaEventRecord(h->join, side));
   AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
@@ -351,7 +418,9 @@ static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
                       d.seed, iter_dev, 0, done, main);
 }
 
-extern "C" size_t ab_lda_scratch_bytes(void) { return 256; }
+extern "C" size_t ab_lda_scratch_bytes(int K, int V) {
+  return (K > 0 && V > 0) ? lda_phi_scratch(K, V) : 0;
+}
 
 extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
   AB_REQUIRE(desc && out, AB_ERR_ARG, "ab_lda_create: null argument");
@@ -379,8 +448,8 @@ extern "C" int ab_lda_init_state(ab_lda* h, uint32_t iter, void* stream) {
   AB_REQUIRE(h, AB_ERR_ARG, "ab_lda_init_state: null handle");
   const ab_lda_desc& d = h->d;
   cudaStream_t st = as_stream(stream);
-  uint32_t hdr[2] = {iter, 0u};
-  AB_CUDA(cudaMemcpyAsync(d.scratch, hdr, sizeof(hdr), cudaMemcpyHostToDevice, st));
+  AB_CUDA(cudaMemsetAsync(d.scratch, 0, lda_phi_scratch(d.K, d.V), st));
+  AB_CUDA(cudaMemcpyAsync(d.scratch, &iter, sizeof(iter), cudaMemcpyHostToDevice, st));
   return launch_lda_count(d.D, d.K, d.V, d.doc_off, d.w, d.z, d.cnt_dk, d.cnt_kw, st);
 }
 

@@ -58,7 +58,7 @@ class LdaGibbs:
         self.z = torch.zeros(self.T, dtype=torch.int32, device=self.dev)
         self.cnt_dk = torch.zeros((self.D, self.K), dtype=torch.int32, device=self.dev)
         self.cnt_kw = torch.zeros((self.K, self.V), dtype=torch.int32, device=self.dev)
-        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes()), dtype=torch.uint8, device=self.dev)
+        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V)), dtype=torch.uint8, device=self.dev)
         self.set_state(theta=theta if theta is not None else np.full((self.D, self.K), 1.0 / self.K),
                        phi=phi if phi is not None else np.full((self.K, self.V), 1.0 / self.V),
                        z=z if z is not None else np.zeros(self.T, np.int32), iteration=iter0)

@@ -73,9 +73,12 @@ int ab_lda_conj_theta(int D, int K, const double* alpha, const int* cnt_dk, doub
 
 /* phi[k] ~ Dirichlet(beta + cnt_kw[k]) stored as phiT: replaces conj_samp_phi.
  * Element (k,v) draws from substream (k*V+v, iter, 3).  clear_counts != 0
- * zeroes cnt_kw after reading it. */
+ * zeroes cnt_kw after reading it.  `scratch` is caller-allocated device
+ * memory of ab_lda_phi_scratch_bytes(K, V) bytes (per-topic partial sums and
+ * completion tickets); calls sharing one scratch buffer must not overlap. */
+size_t ab_lda_phi_scratch_bytes(int K, int V);
 int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
-                    int clear_counts, uint64_t seed, uint32_t iter, void* stream);
+                    int clear_counts, uint64_t seed, uint32_t iter, void* scratch, void* stream);
 
 /* z[t] ~ p(z | theta, phi) for every token: replaces the generated disc_z
  * (CgDisc.hs:122-156) over augur_unnorm_disc_samp (cbits/augur_dist.c:
@@ -99,12 +102,12 @@ typedef struct ab_lda_desc {
   double* phiT;         /* [V][Kp] */
   int* cnt_dk;          /* [D][K] */
   int* cnt_kw;          /* [K][V] */
-  void* scratch;        /* ab_lda_scratch_bytes() bytes of device memory */
+  void* scratch;        /* ab_lda_scratch_bytes(K, V) bytes of device memory */
   uint64_t seed;
 } ab_lda_desc;
 
 typedef struct ab_lda ab_lda;
-size_t ab_lda_scratch_bytes(void);
+size_t ab_lda_scratch_bytes(int K, int V);
 /* Replaces augur_iface_init for the LDA model (CgStInit.hs:474-510); the
  * caller owns every buffer named by the descriptor. */
 int ab_lda_create(const ab_lda_desc* desc, ab_lda** out);

@@ -49,9 +49,14 @@ def phiT_of(phi):
     return out, Kp
 
 
-@pytest.mark.parametrize("seed", [0, 1])
-def test_disc_z_and_counts_bit_exact(orc, seed):
-    off, w, theta, phi = random_problem(seed)
+@pytest.mark.parametrize("seed,K,V", [(0, 50, 700), (1, 50, 700), (2, 1, 30), (3, 2, 30), (4, 3, 40),
+                                      (5, 17, 90), (6, 64, 300), (7, 200, 500), (8, 1024, 64)])
+def test_disc_z_and_counts_bit_exact(orc, seed, K, V):
+    off, w, theta, phi = random_problem(seed, D=60 if K > 100 else 150, K=K, V=V)
+    if seed % 3 == 2:                                 # exact zeros in theta and phi
+        theta[:, ::3] = 0.0
+        theta[theta.sum(1) == 0, 0] = 1.0
+        phi[::2, ::5] = 0.0
     D, K = theta.shape
     V = phi.shape[1]
     phiT, _ = phiT_of(phi)
@@ -75,9 +80,9 @@ def test_count_kernel(orc):
     z = np.random.default_rng(3).integers(0, K, size=len(w)).astype(np.int32)
     cdk = torch.full((D, K), 7, dtype=torch.int32, device="cuda")
     ckw = torch.full((K, V), 7, dtype=torch.int32, device="cuda")
-    N.check(N.lib().ab_lda_count(D, K, V, N.ptr(dev(off, torch.int32)), N.ptr(dev(w, torch.int32)),
-                                 N.ptr(dev(z, torch.int32)), N.ptr(cdk), N.ptr(ckw), N.stream_ptr()),
-            "count")
+    g = [dev(off, torch.int32), dev(w, torch.int32), dev(z, torch.int32)]  # keep alive
+    N.check(N.lib().ab_lda_count(D, K, V, N.ptr(g[0]), N.ptr(g[1]), N.ptr(g[2]), N.ptr(cdk), N.ptr(ckw),
+                                 N.stream_ptr()), "count")
     c_dk, c_kw = orc.lda_conj_stat(off, w, z, D, K, V)
     np.testing.assert_array_equal(cdk.cpu().numpy(), c_dk)
     np.testing.assert_array_equal(ckw.cpu().numpy(), c_kw)
@@ -90,8 +95,9 @@ def test_conj_theta_matches_oracle(orc):
     cnt[::7] = 0
     alpha = np.full(K, 0.1)
     out = torch.zeros((D, K), dtype=torch.float64, device="cuda")
-    N.check(N.lib().ab_lda_conj_theta(D, K, N.ptr(dev(alpha, torch.float64)), N.ptr(dev(cnt, torch.int32)),
-                                      N.ptr(out), 77, 4, N.stream_ptr()), "conj_theta")
+    g = [dev(alpha, torch.float64), dev(cnt, torch.int32)]  # keep alive
+    N.check(N.lib().ab_lda_conj_theta(D, K, N.ptr(g[0]), N.ptr(g[1]), N.ptr(out), 77, 4, N.stream_ptr()),
+            "conj_theta")
     ref = orc.lda_conj_theta(alpha, cnt, 77, 4)
     got = out.cpu().numpy()
     np.testing.assert_allclose(got, ref, rtol=RTOL, atol=0)
@@ -106,8 +112,11 @@ def test_conj_phi_matches_oracle(orc, K, V):
     phiT, Kp = phiT_of(np.zeros((K, V)))
     ckw = dev(cnt, torch.int32)
     out = dev(phiT, torch.float64)
-    N.check(N.lib().ab_lda_conj_phi(K, V, N.ptr(dev(beta, torch.float64)), N.ptr(ckw), N.ptr(out), 1,
-                                    55, 2, N.stream_ptr()), "conj_phi")
+    bt = dev(beta, torch.float64)  # keep alive
+    scratch = torch.full((int(N.lib().ab_lda_phi_scratch_bytes(K, V)),), 0xAB, dtype=torch.uint8,
+                         device="cuda")
+    N.check(N.lib().ab_lda_conj_phi(K, V, N.ptr(bt), N.ptr(ckw), N.ptr(out), 1, 55, 2, N.ptr(scratch),
+                                    N.stream_ptr()), "conj_phi")
     ref = orc.lda_conj_phi(beta, cnt, 55, 2)
     got = out.cpu().numpy()[:, :K].T
     np.testing.assert_allclose(got, ref, rtol=RTOL, atol=1e-300)
