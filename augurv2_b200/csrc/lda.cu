@@ -13,11 +13,12 @@
 //   cnt_dk   int32 [D][K]   document-topic counts
 //   cnt_kw   int32 [K][V]   topic-word counts
 //
-// One sweep is three kernels:
+// One sweep is four kernels (theta runs concurrently with the phi pair):
 //   lda_theta_kernel  theta[d] ~ Dir(alpha + cnt_dk[d])      (reads cnt_dk)
-//   lda_phi_kernel    phi[k]   ~ Dir(beta + cnt_kw[k])       (reads, then
-//                     clears cnt_kw); one draw per thread, the last CTA of
-//                     each topic normalises it
+//   lda_phi_draw_kernel + lda_phi_norm_kernel
+//                     phi[k]   ~ Dir(beta + cnt_kw[k])       (reads, then
+//                     clears cnt_kw); one draw per thread, then a parallel
+//                     normalisation pass
 //   lda_z_kernel      z ~ p(z | theta, phi), and the counts of the new z
 //                     (cnt_dk rows written whole, cnt_kw incremented)
 // The count statistics of the reference (conj_stat_*, rebuilt from zero each
@@ -83,21 +84,23 @@ lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
 
 // ---------------------------------------------------------------------------
 // phi[k][v] = g[k][v] / sum_v g[k][v], g ~ Gamma(beta_v + cnt[k][v], 1),
-// stored word-major into phiT[v][k].  The K*V gamma draws are spread one per
-// thread over K * B CTAs (B CTAs per topic).  Each CTA writes its draws
-// unnormalised into phiT, clears the counts it read, and stores its fixed-
-// order partial sum in scratch; the last CTA of a topic to finish (counted
-// with an atomic ticket) adds the B partials in CTA order and normalises the
-// topic's column of phiT.  The sum is deterministic but not in the
-// reference's sequential order, so phi matches the reference to rounding,
-// not bitwise.
-// Scratch: uint32 ticket[K] (zero on entry, left zero) | double partial[K][B].
+// stored word-major into phiT[v][k].  Two kernels:
+//  lda_phi_draw_kernel  one gamma draw per thread over K * B CTAs (B CTAs per
+//                       topic); writes g unnormalised into phiT, clears the
+//                       counts it read and stores the CTA's fixed-order
+//                       partial sum in scratch (partial[k][b]); the last CTA
+//                       of a topic (atomic ticket) adds the B partials in CTA
+//                       order into nrm[k];
+//  lda_phi_norm_kernel  divides phiT by nrm, row by row and coalesced.
+// The sum is deterministic but not in the reference's sequential order, so
+// phi matches the reference to rounding, not bitwise.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(LDA_THREADS, 5)
-lda_phi_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta,
-               int* __restrict__ cnt_kw, double* __restrict__ phiT, int clear_counts,
-               uint32_t* __restrict__ ticket, double* __restrict__ partial,
-               uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta,
+                    int* __restrict__ cnt_kw, double* __restrict__ phiT, int clear_counts,
+                    double* __restrict__ partial, uint32_t* __restrict__ ticket,
+                    double* __restrict__ nrm, uint64_t seed, const uint32_t* iter_dev,
+                    uint32_t iter_fixed) {
   __shared__ double red[33];
   __shared__ bool last;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
@@ -114,122 +117,205 @@ lda_phi_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta,
     phiT[(size_t)v * Kp + k] = g;
   }
   const double bsum = block_sum_f64(g, red);
+  // The last CTA of topic k (atomic ticket) adds the topic's B partials in
+  // CTA order and publishes the normaliser.
   if (threadIdx.x == 0) {
     partial[(size_t)k * B + b] = bsum;
     __threadfence();
     last = atomicAdd(ticket + k, 1u) == (unsigned)(B - 1);
+    if (last) {
+      __threadfence();
+      double acc = 0.0;
+      for (int i = 0; i < B; ++i) acc = __dadd_rn(acc, __ldcg(partial + (size_t)k * B + i));
+      nrm[k] = acc;
+      ticket[k] = 0u;
+    }
   }
+}
+
+constexpr int LDA_NORM_ROWS = 32;   // phiT rows per CTA of the normalisation
+
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_phi_norm_kernel(int K, int V, int Kp, const double* __restrict__ nrm_g,
+                    double* __restrict__ phiT) {
+  extern __shared__ double nrm[];   // [K]
+  for (int k = threadIdx.x; k < K; k += blockDim.x) nrm[k] = nrm_g[k];
   __syncthreads();
-  if (!last) return;
-  __threadfence();
-  double norm = 0.0;
-  for (int i = 0; i < B; ++i) norm = __dadd_rn(norm, __ldcg(partial + (size_t)k * B + i));
-  for (int vv = threadIdx.x; vv < V; vv += blockDim.x) {
-    double* p = phiT + (size_t)vv * Kp + k;
-    *p = __ddiv_rn(__ldcg(p), norm);
+  // one warp per row, lanes over k
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int v_end = min(V, (int)(blockIdx.x + 1) * LDA_NORM_ROWS);
+  for (int v = blockIdx.x * LDA_NORM_ROWS + warp; v < v_end; v += nw) {
+    double* rowp = phiT + (size_t)v * Kp;
+    for (int k = lane; k < K; k += 32) rowp[k] = __ddiv_rn(rowp[k], nrm[k]);
   }
-  if (threadIdx.x == 0) ticket[k] = 0u;
 }
 
 static inline int lda_phi_blocks(int V) { return (V + LDA_THREADS - 1) / LDA_THREADS; }
 
 // ---------------------------------------------------------------------------
-// z[t] for every token of document d (one CTA per document, one thread per
-// token):
+// z[t] for every token of document d (one CTA per document):
 //   pmf_k  = (1 * theta[d][k]) * phi[k][w]                (CgDisc.hs:132-139)
 //   norm   = sum_k pmf_k  (sequential)                    (augur_dist.c:800-803)
 //   z      = first i with u < sum_{j<=i} pmf_j / norm      (:805-812)
-// The norm pass reads the token's phi row with 16-byte loads and records the
-// running sum at 8 checkpoints.  The reference's running quotient sum is
-// replaced by a division-free test (comment in the code) evaluated first at
-// the checkpoints and then inside the one block that contains the answer;
+// Each warp takes 32 consecutive tokens.  With STAGED (K <= 64) the warp
+// copies the 32 phi rows into shared memory with asynchronous 16-byte copies,
+// one row per copy instruction (coalesced: a row is one contiguous segment,
+// and all 32 rows are in flight at once), with a row pitch
+// of an odd number of 16-byte units so that the per-lane row reads that
+// follow are bank-conflict free; otherwise each lane reads its own row from
+// global memory.  Each lane then computes its token.  The norm pass records
+// the running sum at 8 checkpoints; the reference's running quotient sum is
+// replaced by a division-free test (comment in token_draw) evaluated first
+// at the checkpoints and then inside the one block that contains the answer;
 // only a u within rounding distance of a boundary runs the reference loop
-// itself.  The products are recomputed where needed; they are the same
-// binary64 values.
+// itself.  Products are recomputed where needed; they are the same binary64
+// values.
 // Counts of the new z: the document's row of cnt_dk is accumulated in shared
 // memory and stored whole; cnt_kw receives warp-aggregated atomic increments
 // (lanes with the same (z, w) key elect one leader that adds the group size).
 // ---------------------------------------------------------------------------
 constexpr int LDA_Z_THREADS = 128;
 constexpr int LDA_Z_CP = 8;            // checkpoints of the running sum
+constexpr int LDA_Z_STAGE_MAX_K = 64;
 
-__global__ void __launch_bounds__(LDA_Z_THREADS)
+__device__ __forceinline__ int token_draw(int K, int half_kp, int nsuper, int R, int S,
+                                          const double* __restrict__ th, const double* row,
+                                          double u, double lo, double hi) {
+  const double2* row2 = reinterpret_cast<const double2*>(row);
+  const double2* th2 = reinterpret_cast<const double2*>(th);
+  // Four interleaved partial sums shorten the floating-point dependency chain;
+  // the fast test below tolerates any summation order of these nonnegative
+  // products (its margin bounds the rounding of any order), and the exact
+  // fallback recomputes the sequential sum.
+  double cp[LDA_Z_CP];
+#pragma unroll
+  for (int i = 0; i < LDA_Z_CP; ++i) cp[i] = 0.0;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  for (int sc = 0; sc < nsuper; ++sc) {
+    double2 f[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int q = sc * 8 + i;
+      f[i] = q < half_kp ? row2[q] : make_double2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+      const int q = sc * 8 + i;
+      const double2 g0 = th2[q], g1 = th2[q + 1];   // th is zero padded to KT
+      a0 = __dadd_rn(a0, __dmul_rn(g0.x, f[i].x));
+      a1 = __dadd_rn(a1, __dmul_rn(g0.y, f[i].y));
+      a2 = __dadd_rn(a2, __dmul_rn(g1.x, f[i + 1].x));
+      a3 = __dadd_rn(a3, __dmul_rn(g1.y, f[i + 1].y));
+    }
+    const int ci = sc / R;
+    if (sc % R == R - 1 || sc == nsuper - 1) {
+      const double c = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
+#pragma unroll
+      for (int i = 0; i < LDA_Z_CP; ++i)
+        if (i == ci) cp[i] = c;
+    }
+  }
+  double norm = __dadd_rn(__dadd_rn(a0, a1), __dadd_rn(a2, a3));
+#pragma unroll
+  for (int i = 1; i < LDA_Z_CP; ++i)
+    if (i > (nsuper - 1) / R) cp[i] = norm;
+  // Division-free decision.  With c_j the running sum of the products,
+  // u < acc_j (the reference's running sum of pmf_i / norm) holds when
+  // u*norm < c_j (1 - m) and fails when u*norm > c_j (1 + m); m bounds the
+  // rounding of both running sums, the quotients and the products
+  // (|error| <= (2j + 3) 2^-53 relative, plus subnormal slack).  c_j is
+  // nondecreasing, so a checkpoint with u*norm > c (1 + m) rules out its
+  // whole block.  A u within m of a boundary takes the reference loop.
+  bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
+  int zk = K - 1;
+  if (!exact) {
+    const double un = __dmul_rn(u, norm);
+    int blk = LDA_Z_CP - 1;
+    double c = cp[LDA_Z_CP - 2];
+#pragma unroll
+    for (int i = LDA_Z_CP - 2; i >= 0; --i)
+      if (un <= __dmul_rn(cp[i], hi)) { blk = i; c = i > 0 ? cp[i - 1] : 0.0; }
+    const int j1 = min(K - 1, (blk + 1) * S);
+    for (int j = blk * S; j < j1; ++j) {
+      c = __dadd_rn(c, __dmul_rn(th[j], row[j]));
+      if (un < __dmul_rn(c, lo)) { zk = j; break; }
+      if (un <= __dmul_rn(c, hi)) { exact = true; break; }
+    }
+  }
+  if (exact) {
+    norm = 0.0;
+    for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], row[k]));
+    double acc = __ddiv_rn(__dmul_rn(th[0], row[0]), norm);
+    zk = K - 1;
+    for (int i = 1; i < K; ++i) {
+      if (u < acc) { zk = i - 1; break; }
+      acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], row[i]), norm));
+    }
+  }
+  return zk;
+}
+
+template <bool STAGED>
+__global__ void __launch_bounds__(LDA_Z_THREADS, 4)
 lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
              const int* __restrict__ w, const double* __restrict__ theta,
              const double* __restrict__ phiT, int* __restrict__ z,
              int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
              uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
   extern __shared__ double smem[];
-  double* th = smem;                                    // [Kp] (zero padded)
-  int* hist = reinterpret_cast<int*>(smem + Kp);        // [K]
+  const int KT = 16 * ((K + 15) / 16);                  // theta padded to whole super-chunks
+  double* th = smem;                                    // [KT] (zero padded)
+  int* hist = reinterpret_cast<int*>(smem + KT);        // [K]
+  const int half_kp = Kp / 2;
+  const int pitch2 = half_kp | 1;                       // row pitch in 16-byte units (odd)
+  double2* stage = reinterpret_cast<double2*>(smem + KT + ((K + 3) & ~3) / 2 + 2) +
+                   (size_t)(threadIdx.x >> 5) * 32 * pitch2;
   const int lane = threadIdx.x & 31;
   const int d = blockIdx.x;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
-  for (int k = threadIdx.x; k < Kp; k += blockDim.x) {
+  for (int k = threadIdx.x; k < KT; k += blockDim.x) {
     th[k] = k < K ? theta[(size_t)d * K + k] : 0.0;
     if (k < K) hist[k] = 0;
   }
   __syncthreads();
   const int t0 = doc_off[d], t1 = doc_off[d + 1];
-  // Checkpoint block length (even, so blocks start on 16-byte boundaries).
-  const int S = (((K + LDA_Z_CP - 1) / LDA_Z_CP) + 1) & ~1;
+  // Super-chunks of 16 doubles; a checkpoint block spans R of them.
+  const int nsuper = (K + 15) / 16;
+  const int R = (nsuper + LDA_Z_CP - 1) / LDA_Z_CP;
+  const int S = 16 * R;                 // checkpoint block length in elements
   const double m = (6.0 * K + 32.0) * 1.1102230246251565e-16;
   const double lo = 1.0 - m, hi = 1.0 + m;
-  for (int tb = t0; tb < t1; tb += blockDim.x) {
-    const int t = tb + threadIdx.x;
+  const int nwarps = blockDim.x >> 5;
+  for (int tb = t0 + (threadIdx.x >> 5) * 32; tb < t1; tb += nwarps * 32) {
+    const int t = tb + lane;
     const bool active = t < t1;
     const int wt = active ? w[t] : 0;
+    const double* row;
+    if (STAGED) {
+      // Asynchronous 16-byte copies global -> shared (cp.async, L2 only):
+      // all 32 rows are in flight at once and no registers hold them.
+      const int nrow = min(32, t1 - tb);
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const int wr = __shfl_sync(0xffffffffu, wt, r);
+        if (r < nrow && lane < half_kp) {
+          const double2* src = reinterpret_cast<const double2*>(phiT + (size_t)wr * Kp) + lane;
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + r * pitch2 + lane);
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+        }
+      }
+      asm volatile("cp.async.commit_group;\n" ::: "memory");
+      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+      __syncwarp();
+      row = reinterpret_cast<const double*>(stage + lane * pitch2);
+    } else {
+      row = phiT + (size_t)wt * Kp;
+    }
     int zk = 0;
     if (active) {
-      const double* row = phiT + (size_t)wt * Kp;
-      double cp[LDA_Z_CP];
-      double norm = 0.0;
-#pragma unroll
-      for (int c = 0; c < LDA_Z_CP; ++c) {
-        const int k1 = min(K, (c + 1) * S);
-        for (int k = c * S; k < k1; k += 2) {
-          const double2 f = __ldg(reinterpret_cast<const double2*>(row + k));
-          const double2 g = *reinterpret_cast<const double2*>(th + k);
-          norm = __dadd_rn(norm, __dmul_rn(g.x, f.x));
-          if (k + 1 < k1) norm = __dadd_rn(norm, __dmul_rn(g.y, f.y));
-        }
-        cp[c] = norm;
-      }
       Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
       const double u = s.uniform();
-      // Division-free decision.  With c_j the running sum of the products,
-      // u < acc_j (the reference's running sum of pmf_i / norm) holds when
-      // u*norm < c_j (1 - m) and fails when u*norm > c_j (1 + m); m bounds
-      // the rounding of both running sums, the quotients and the products
-      // (|error| <= (2j + 3) 2^-53 relative, plus subnormal slack).  c_j is
-      // nondecreasing, so a checkpoint with u*norm > c (1 + m) rules out its
-      // whole block.  A u within m of a boundary takes the reference loop.
-      bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
-      zk = K - 1;
-      if (!exact) {
-        const double un = __dmul_rn(u, norm);
-        int blk = LDA_Z_CP - 1;
-        double c = cp[LDA_Z_CP - 2];
-#pragma unroll
-        for (int i = LDA_Z_CP - 2; i >= 0; --i)
-          if (un <= __dmul_rn(cp[i], hi)) { blk = i; c = i > 0 ? cp[i - 1] : 0.0; }
-        const int j1 = min(K - 1, (blk + 1) * S);
-        for (int j = blk * S; j < j1; ++j) {
-          c = __dadd_rn(c, __dmul_rn(th[j], __ldg(row + j)));
-          if (un < __dmul_rn(c, lo)) { zk = j; break; }
-          if (un <= __dmul_rn(c, hi)) { exact = true; break; }
-        }
-      }
-      if (exact) {
-        norm = 0.0;
-        for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], __ldg(row + k)));
-        double acc = __ddiv_rn(__dmul_rn(th[0], __ldg(row)), norm);
-        zk = K - 1;
-        for (int i = 1; i < K; ++i) {
-          if (u < acc) { zk = i - 1; break; }
-          acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], __ldg(row + i)), norm));
-        }
-      }
+      zk = token_draw(K, half_kp, nsuper, R, S, th, row, u, lo, hi);
       z[t] = zk;
       atomicAdd(&hist[zk], 1);
     }
@@ -242,6 +328,7 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
         if (lane == leader) atomicAdd(cnt_kw + key, __popc(peers));
       }
     }
+    if (STAGED) __syncwarp();   // the stage is rewritten by the next chunk
   }
   __syncthreads();
   if (cnt_dk != nullptr)
@@ -300,31 +387,48 @@ int launch_lda_theta(int D, int K, const double* alpha, const int* cnt_dk, doubl
   return AB_OK;
 }
 
+// scratch: [0,256) reserved for the sweep runner's counters, then
+// ticket[K] (uint32, zero between calls), nrm[K], partial[K][B] (doubles),
+// each region 256-byte aligned.
+static inline size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
 size_t lda_phi_scratch(int K, int V) {
-  return 256 + (((size_t)K * 4 + 255) & ~(size_t)255) + sizeof(double) * (size_t)K * lda_phi_blocks(V);
+  return 256 + al256(4 * (size_t)K) + al256(8 * (size_t)K) + sizeof(double) * (size_t)K * lda_phi_blocks(V);
 }
 
-// scratch: [0,256) reserved for the sweep runner's counters, then ticket[K]
-// (256-byte aligned), then partial[K][B].
 int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double* phiT, int clear,
                    void* scratch, uint64_t seed, const uint32_t* iter_dev, uint32_t iter,
                    cudaStream_t st) {
   const int B = lda_phi_blocks(V);
-  uint32_t* ticket = reinterpret_cast<uint32_t*>(static_cast<char*>(scratch) + 256);
-  double* partial = reinterpret_cast<double*>(static_cast<char*>(scratch) + 256 +
-                                              ((((size_t)K * 4) + 255) & ~(size_t)255));
-  lda_phi_kernel<<<K * B, LDA_THREADS, 0, st>>>(K, V, Kp, B, beta, cnt_kw, phiT, clear, ticket,
-                                                partial, seed, iter_dev, iter);
-  AB_LAUNCH_CHECK("lda_phi_kernel");
+  char* base = static_cast<char*>(scratch) + 256;
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(base);
+  double* nrm = reinterpret_cast<double*>(base + al256(4 * (size_t)K));
+  double* partial = reinterpret_cast<double*>(base + al256(4 * (size_t)K) + al256(8 * (size_t)K));
+  lda_phi_draw_kernel<<<K * B, LDA_THREADS, 0, st>>>(K, V, Kp, B, beta, cnt_kw, phiT, clear, partial,
+                                                     ticket, nrm, seed, iter_dev, iter);
+  AB_LAUNCH_CHECK("lda_phi_draw_kernel");
+  lda_phi_norm_kernel<<<ceil_div(V, LDA_NORM_ROWS), LDA_THREADS, sizeof(double) * K, st>>>(
+      K, V, Kp, nrm, phiT);
+  AB_LAUNCH_CHECK("lda_phi_norm_kernel");
   return AB_OK;
 }
 
 int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
                  const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
-  const size_t smem = sizeof(double) * (size_t)Kp + sizeof(int) * (size_t)K;
-  lda_z_kernel<<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw,
-                                                seed, iter_dev, iter, done_ctr);
+  // theta [KT] doubles, hist [K] ints (rounded to whole 16 bytes), then the stage
+  const size_t KT = 16 * (size_t)((K + 15) / 16);
+  const size_t base = sizeof(double) * (KT + ((K + 3) & ~3) / 2 + 2);
+  if (K <= LDA_Z_STAGE_MAX_K) {
+    const size_t smem = base + 16 * (size_t)(LDA_Z_THREADS / 32) * 32 * ((Kp / 2) | 1);
+    AB_CUDA(cudaFuncSetAttribute(lda_z_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    lda_z_kernel<true><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk,
+                                                        cnt_kw, seed, iter_dev, iter, done_ctr);
+  } else {
+    lda_z_kernel<false><<<D, LDA_Z_THREADS, base, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk,
+                                                         cnt_kw, seed, iter_dev, iter, done_ctr);
+  }
   AB_LAUNCH_CHECK("lda_z_kernel");
   return AB_OK;
 }
@@ -373,7 +477,7 @@ extern "C" int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, do
   if (rc) return rc;
   AB_REQUIRE(beta && cnt_kw && phiT && scratch, AB_ERR_ARG, "ab_lda_conj_phi: null pointer");
   cudaStream_t st = as_stream(stream);
-  AB_CUDA(cudaMemsetAsync(static_cast<char*>(scratch) + 256, 0, (size_t)K * 4, st));
+  AB_CUDA(cudaMemsetAsync(static_cast<char*>(scratch) + 256, 0, 4 * (size_t)K, st));
   return launch_lda_phi(K, V, lda_kp(K), beta, cnt_kw, phiT, clear_counts, scratch, seed, nullptr,
                         iter, st);
 }

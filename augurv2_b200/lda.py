@@ -8,7 +8,7 @@ Model (compiler/augur/test/lda.rv, examples/lda.py:12-22):
 Schedule: ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z].
 
 Device state lives in torch tensors owned by this object; every sweep runs
-as a replay of a captured CUDA graph of three kernels (lda.cu).
+as a replay of a captured CUDA graph of four kernels (lda.cu).
 """
 import ctypes as C
 

@@ -174,7 +174,7 @@ def run_ours(args, rank, world, local_rank):
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+int32", "data": "synthetic (LDA generative process, seed 0)",
             "config": cfg, "tokens_per_step": T,
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 4 * args.steps,
             "clocks": clocks.summary(),
             "roofline": {"bound": "hbm", "kernel": "lda_z_kernel", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,

@@ -74,8 +74,9 @@ int ab_lda_conj_theta(int D, int K, const double* alpha, const int* cnt_dk, doub
 /* phi[k] ~ Dirichlet(beta + cnt_kw[k]) stored as phiT: replaces conj_samp_phi.
  * Element (k,v) draws from substream (k*V+v, iter, 3).  clear_counts != 0
  * zeroes cnt_kw after reading it.  `scratch` is caller-allocated device
- * memory of ab_lda_phi_scratch_bytes(K, V) bytes (per-topic partial sums and
- * completion tickets); calls sharing one scratch buffer must not overlap. */
+ * memory of ab_lda_phi_scratch_bytes(K, V) bytes (per-CTA partial sums of
+ * the gamma draws, per-topic normalisers and completion tickets); calls
+ * sharing one scratch buffer must not overlap. */
 size_t ab_lda_phi_scratch_bytes(int K, int V);
 int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
                     int clear_counts, uint64_t seed, uint32_t iter, void* scratch, void* stream);
@@ -90,7 +91,7 @@ int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int* w, const d
                   uint32_t iter, void* stream);
 
 /* Sweep runner: the whole augur_step of the LDA schedule (CgKern.hs:232-238)
- * as a captured CUDA graph of three kernels. */
+ * as a captured CUDA graph of four kernels. */
 typedef struct ab_lda_desc {
   int D, K, V;
   const int* doc_off;   /* [D+1] */
