@@ -11,12 +11,8 @@
 #include <augur_dist.h>
 
 typedef struct AugurMod {
-  /* HLR block state */
-  AugurVec_t* theta;   /* Vec Real [K] */
-  double* b;           /* Real */
-  double* v;           /* Real */
-  /* GMM means (ESlice / MWG) */
-  AugurVec_t* mu;      /* Vec (Vec Real) [K][d] flattened per component */
+  double* par;         /* HLR: [theta[0..D-1], b, v] */
+  AugurVec_t* mu;      /* GMM means (ESlice / MWG), [K] rows of d */
 } AugurMod_t;
 
 typedef struct AugurAux {

@@ -169,3 +169,414 @@ void orc_lda_sweeps(int D, int K, int V, const int* doc_off, const int* w,
     orc_lda_disc_z(D, K, V, doc_off, w, theta, phi, z, seed, it);
   }
 }
+
+/* ------------------------------------------------------------------------
+ * Hierarchical logistic regression (compiler/augur/test/hlr.rv and the
+ * InvGamma-variance variant without bias):
+ *   v ~ Exponential(lam) | InvGamma(a0, s0);  b ~ Normal(0, v) (optional);
+ *   theta[k] ~ Normal(0, v);  y[n] ~ Bernoulli(sigmoid(theta . x[n] + b)).
+ * Parameters are one vector par = [theta[0..D-1], b, v].  A block is a list
+ * of indices into par in the schedule's order (HMC [v, b, theta] -> D+1, D,
+ * 0..D-1).  `compat` selects the reference's own density formulas
+ * (cbits/augur_dist.c:59-72,231-247,345-394), including its Normal log
+ * density -log(var) - t^2/(2 var) and its dNormal/dvar of -var/2 + ...;
+ * compat = 0 uses the textbook densities with numerically stable logistic
+ * terms.
+ * --------------------------------------------------------------------- */
+#define ORC_LARGE 1e8
+typedef struct {
+  int N, D, has_b, vprior, compat; /* vprior: 0 Exponential(lam), 1 InvGamma(a0, s0) */
+  double lam, a0, s0;
+  const double* X; /* N x D row-major */
+  const int* y;
+} orc_hlr;
+
+static double orc_expit(double x) { return 1.0 / (1.0 + exp(-x)); }
+
+static double orc_normal_ll(const orc_hlr* m, double pt, double mean, double var) {
+  if (m->compat) {
+    if (var > 0.0) { double t = pt - mean; return (-log(var)) - (0.5 * t * t / var); }
+    return -ORC_LARGE;
+  }
+  if (!(var > 0.0)) return -INFINITY;
+  double t = pt - mean;
+  return -0.5 * log(2.0 * 3.14159265358979323846 * var) - 0.5 * t * t / var;
+}
+static double orc_normal_dotpt(double pt, double mean, double var) { return -(pt - mean) / var; }
+static double orc_normal_dotarg2(const orc_hlr* m, double pt, double mean, double var) {
+  double t = pt - mean;
+  if (m->compat) return (-0.5 * var) + (0.5 * (t * t) / (var * var));
+  return (-0.5 / var) + (0.5 * (t * t) / (var * var));
+}
+static double orc_vprior_ll(const orc_hlr* m, double v) {
+  if (m->vprior == 0) {                     /* augur_exponential_ll, augur_dist.c:231-238 */
+    if (m->lam > 0.0 && v > 0.0) return log(m->lam) - m->lam * v;
+    return m->compat ? -ORC_LARGE : -INFINITY;
+  }
+  if (!(v > 0.0)) return m->compat ? -ORC_LARGE : -INFINITY;  /* augur_invgamma_ll :345-347 */
+  return m->a0 * log(m->s0) - lgamma(m->a0) - (m->a0 + 1.0) * log(v) - m->s0 / v;
+}
+static double orc_vprior_dot(const orc_hlr* m, double v) {
+  if (m->vprior == 0) return (m->lam > 0.0 && v > 0.0) ? -m->lam : 0.0;   /* :240-246 */
+  return -(m->a0 + 1.0) / v + m->s0 / (v * v);                             /* :349-351 */
+}
+
+/* Data factor of one row: log Bern(y | sigmoid(t)) and d/dt of it. */
+static double orc_bern_ll(const orc_hlr* m, int y, double t) {
+  if (m->compat) {                          /* augur_bernoulli_ll(y, augur_expit(t)) */
+    double p = orc_expit(t);
+    if (p >= 0.0 && p <= 1.0) return log(y * p + (1 - y) * (1.0 - p));
+    return -ORC_LARGE;
+  }
+  double sp = (t > 0 ? t : 0.0) + log1p(exp(-fabs(t)));   /* softplus */
+  return y ? t - sp : -sp;
+}
+static double orc_bern_dt(const orc_hlr* m, int y, double t) {
+  if (m->compat) {                          /* dotarg1 (:68-71) x expit_grad_0 (augur_math.c:56-59) */
+    double p = orc_expit(t);
+    double denom = (y * p + (1 - y) * (1.0 - p));
+    double adj3 = (y + y - 1) / denom;
+    double e = orc_expit(t);
+    return adj3 * (e * (1.0 - e));
+  }
+  return (double)y - orc_expit(t);
+}
+
+static int orc_in_block(const int* idx, int P, int lo, int hi) {
+  for (int j = 0; j < P; ++j) if (idx[j] >= lo && idx[j] < hi) return 1;
+  return 0;
+}
+
+/* Full conditional of the block (CgLike.hs:139-147,254-258): factors that
+ * mention a block variable, in model order, each Pi factor a sequential
+ * sum over its index, accumulated onto ll = 0. */
+double orc_hlr_ll(const orc_hlr* m, const double* par, const int* idx, int P) {
+  const int D = m->D;
+  const double b = m->has_b ? par[D] : 0.0, v = par[D + 1];
+  const int in_th = orc_in_block(idx, P, 0, D);
+  const int in_b = m->has_b && orc_in_block(idx, P, D, D + 1);
+  const int in_v = orc_in_block(idx, P, D + 1, D + 2);
+  double ll = 0.0;
+  if (in_v) ll += orc_vprior_ll(m, v);
+  if (m->has_b && (in_b || in_v)) ll += orc_normal_ll(m, b, 0.0, v);
+  if (in_th || in_v) {
+    double s = 0.0;
+    for (int k = 0; k < D; ++k) s += orc_normal_ll(m, par[k], 0.0, v);
+    ll += s;
+  }
+  if (in_th || in_b) {
+    double s = 0.0;
+    for (int n = 0; n < m->N; ++n) {
+      const double* x = m->X + (size_t)n * D;
+      double dot = 0.0;
+      for (int k = 0; k < D; ++k) dot += par[k] * x[k];
+      s += orc_bern_ll(m, m->y[n], dot + b);
+    }
+    ll += s;
+  }
+  return ll;
+}
+
+/* Gradient of orc_hlr_ll with respect to the block (CgGrad.hs:165-376):
+ * adjoints start at zero; factors in model order; the data factor adds
+ * adj_t * x[n] per row in row order. */
+void orc_hlr_grad(const orc_hlr* m, const double* par, const int* idx, int P, double* g) {
+  const int D = m->D;
+  const double b = m->has_b ? par[D] : 0.0, v = par[D + 1];
+  double* full = (double*)calloc((size_t)D + 2, sizeof(double));
+  const int in_th = orc_in_block(idx, P, 0, D);
+  const int in_b = m->has_b && orc_in_block(idx, P, D, D + 1);
+  const int in_v = orc_in_block(idx, P, D + 1, D + 2);
+  if (in_v) full[D + 1] += orc_vprior_dot(m, v);
+  if (m->has_b && (in_b || in_v)) {
+    if (in_b) full[D] += orc_normal_dotpt(b, 0.0, v);
+    if (in_v) full[D + 1] += orc_normal_dotarg2(m, b, 0.0, v);
+  }
+  if (in_th || in_v) {
+    for (int k = 0; k < D; ++k) {
+      if (in_th) full[k] += orc_normal_dotpt(par[k], 0.0, v);
+      if (in_v) full[D + 1] += orc_normal_dotarg2(m, par[k], 0.0, v);
+    }
+  }
+  if (in_th || in_b) {
+    for (int n = 0; n < m->N; ++n) {
+      const double* x = m->X + (size_t)n * D;
+      double dot = 0.0;
+      for (int k = 0; k < D; ++k) dot += par[k] * x[k];
+      double r = orc_bern_dt(m, m->y[n], dot + b);
+      if (in_b) full[D] += r;
+      if (in_th) for (int k = 0; k < D; ++k) full[k] += r * x[k];
+    }
+  }
+  for (int j = 0; j < P; ++j) g[j] = full[idx[j]];
+  free(full);
+}
+
+/* Batched helper for parity tests: ll and gradient for C parameter vectors. */
+void orc_hlr_ll_grad_batch(const orc_hlr* m, int C, const double* pars, const int* idx, int P,
+                           double* ll, double* g) {
+  for (int c = 0; c < C; ++c) {
+    const double* par = pars + (size_t)c * (m->D + 2);
+    ll[c] = orc_hlr_ll(m, par, idx, P);
+    orc_hlr_grad(m, par, idx, P, g + (size_t)c * P);
+  }
+}
+
+/* ---- HMC: cbits/augur_mcmclib.h:343-424 (h_augur_mcmc_leapfrog, _hmc) ----
+ * Substreams: momentum element j of chain c: (c*P + j, iter, MOM|comp<<8);
+ * jitter and accept: (c, iter, HMC|comp<<8) positions 0, 1 (jitter), 2
+ * (accept u).  `simsteps_out` reports L; returns 1 on accept. */
+static void orc_set_block(double* par, const int* idx, int P, const double* q) {
+  for (int j = 0; j < P; ++j) par[idx[j]] = q[j];
+}
+static void orc_get_block(const double* par, const int* idx, int P, double* q) {
+  for (int j = 0; j < P; ++j) q[j] = par[idx[j]];
+}
+
+int orc_hlr_hmc(const orc_hlr* m, double* par, const int* idx, int P, double simlen, double eps,
+                uint64_t seed, uint32_t iter, uint32_t chain, uint32_t comp, int* simsteps_out,
+                double* prop_out) {
+  const int NP = m->D + 2;
+  double* p0 = (double*)malloc(sizeof(double) * P);
+  double* ps = (double*)malloc(sizeof(double) * P);
+  double* g = (double*)malloc(sizeof(double) * P);
+  double* th0 = (double*)malloc(sizeof(double) * P);
+  double* ths = (double*)malloc(sizeof(double) * P);
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  for (int j = 0; j < P; ++j) {
+    orc_stream s = orc_make(seed, chain * (uint32_t)P + j, iter, ORC_TAG_MOM | (comp << 8));
+    p0[j] = orc_normal(&s);
+  }
+  orc_stream h = orc_make(seed, chain, iter, ORC_TAG_HMC | (comp << 8));
+  double scale_eps = 0.8 + orc_uniform(&h) * (1.2 - 0.8);
+  double stepsize = scale_eps * eps;
+  double sj = 0.9 + orc_uniform(&h) * (1.1 - 0.9);
+  /* augur_max is unsigned (cbits/augur_util.c:61-64) */
+  unsigned rl = (unsigned)round(sj * simlen / stepsize);
+  int simsteps = (int)(rl > 1u ? rl : 1u);
+  memcpy(prop, par, sizeof(double) * NP);
+  orc_get_block(par, idx, P, th0);
+  memcpy(ths, th0, sizeof(double) * P);
+  /* leapfrog (:343-375) */
+  orc_hlr_grad(m, par, idx, P, g);
+  for (int j = 0; j < P; ++j) ps[j] = p0[j] + stepsize / 2.0 * g[j];
+  for (int l = 0; l < simsteps; ++l) {
+    for (int j = 0; j < P; ++j) ths[j] = ths[j] + stepsize * ps[j];
+    orc_set_block(prop, idx, P, ths);
+    if (l != simsteps - 1) {
+      orc_hlr_grad(m, prop, idx, P, g);
+      for (int j = 0; j < P; ++j) ps[j] = ps[j] + stepsize * g[j];
+    }
+  }
+  orc_hlr_grad(m, prop, idx, P, g);
+  for (int j = 0; j < P; ++j) ps[j] = ps[j] + stepsize / 2.0 * g[j];
+  double k0 = 0.0, k1 = 0.0;
+  for (int j = 0; j < P; ++j) k0 += p0[j] * p0[j];
+  for (int j = 0; j < P; ++j) k1 += ps[j] * ps[j];
+  double auxll = k0 / 2.0 - k1 / 2.0;
+  /* augur_mcmc_ar (:70-83) */
+  double currll = orc_hlr_ll(m, par, idx, P);
+  double propll = orc_hlr_ll(m, prop, idx, P);
+  double u = orc_uniform(&h);
+  int acc = log(u) < propll - currll + auxll;
+  if (prop_out) memcpy(prop_out, prop, sizeof(double) * NP);
+  if (acc) memcpy(par, prop, sizeof(double) * NP);
+  if (simsteps_out) *simsteps_out = simsteps;
+  free(p0); free(ps); free(g); free(th0); free(ths); free(prop);
+  return acc;
+}
+
+/* ---- NUTS: cbits/augur_mcmclib.h:575-776, restated with its exact control
+ * flow (two gradients per leaf, the stacks of augur_blkstk.c, the subtree
+ * endpoints taken from the most recent j == 1 push, the proposal kept only
+ * if the final doubling accepted one).  deltaMax = 1000 (:152).  Substreams:
+ * momentum (c*P + j, iter, MOM|comp<<8); every other draw sequentially from
+ * (c, iter, NUTS|comp<<8): exponential slice, then per doubling the
+ * direction coin, the subtree coins in recursion order, the outer coin. */
+#define ORC_STK_MAX 16
+typedef struct {
+  double* b[ORC_STK_MAX];
+  int hd;
+} orc_stk;
+
+typedef struct {
+  const orc_hlr* m;
+  const int* idx;
+  int P;
+  double* mod;      /* full parameter vector whose block is the working theta */
+  double* g;
+  double stepsize, logu;
+  orc_stream* h;
+  orc_stk tp, ts, ms; /* theta_prop, theta, mom stacks */
+  double* work;
+  int overflow, leaves;
+} orc_nuts;
+
+static void orc_push(orc_nuts* t, orc_stk* s, const double* v) {
+  s->hd++;
+  if (s->hd >= ORC_STK_MAX) { t->overflow = 1; s->hd = ORC_STK_MAX - 1; return; }
+  memcpy(s->b[s->hd], v, sizeof(double) * t->P);
+}
+static double* orc_pop(orc_stk* s) { double* r = s->b[s->hd < 0 ? 0 : s->hd]; s->hd--; return r; }
+static double* orc_peek(orc_stk* s) { return s->b[s->hd < 0 ? 0 : s->hd]; }
+
+static double orc_dot(const double* a, const double* b, int P) {
+  double acc = 0.0;
+  for (int j = 0; j < P; ++j) acc += a[j] * b[j];
+  return acc;
+}
+
+static int orc_update_s(const orc_nuts* t, int s, const double* tp, const double* mp,
+                        const double* tm, const double* mm) {
+  if (s == 1) {
+    for (int j = 0; j < t->P; ++j) t->work[j] = tp[j] + -1.0 * tm[j];
+    int ut1 = orc_dot(t->work, mp, t->P) >= 0.0;
+    int ut2 = orc_dot(t->work, mm, t->P) >= 0.0;
+    if (ut1 && ut2) return 1;
+  }
+  return 0;
+}
+
+static void orc_leapfrog1(orc_nuts* t, double* theta, double* mom) {
+  const int P = t->P;
+  const double s = t->stepsize;
+  orc_set_block(t->mod, t->idx, P, theta);
+  orc_hlr_grad(t->m, t->mod, t->idx, P, t->g);
+  for (int j = 0; j < P; ++j) mom[j] = mom[j] + s / 2.0 * t->g[j];
+  for (int j = 0; j < P; ++j) theta[j] = theta[j] + s * mom[j];
+  orc_set_block(t->mod, t->idx, P, theta);
+  orc_hlr_grad(t->m, t->mod, t->idx, P, t->g);
+  for (int j = 0; j < P; ++j) mom[j] = mom[j] + s / 2.0 * t->g[j];
+}
+
+typedef struct { int n, s; } orc_nret;
+
+static orc_nret orc_build(orc_nuts* t, double* theta, double* mom, int j, int dir) {
+  orc_nret r;
+  if (j == 0) {
+    orc_leapfrog1(t, theta, mom);
+    t->leaves++;
+    orc_push(t, &t->tp, theta);
+    double ll = orc_hlr_ll(t->m, t->mod, t->idx, t->P) - 0.5 * orc_dot(mom, mom, t->P);
+    r.n = t->logu <= ll;
+    r.s = t->logu < 1000.0 + ll;
+    return r;
+  }
+  orc_nret left = orc_build(t, theta, mom, j - 1, dir);
+  if (left.s == 1) {
+    if (j == 1) { orc_push(t, &t->ts, theta); orc_push(t, &t->ms, mom); }
+    orc_nret right = orc_build(t, theta, mom, j - 1, dir);
+    double* p1 = orc_pop(&t->tp);
+    double* p2 = orc_pop(&t->tp);
+    double bias = ((double)right.n) / (left.n + right.n);
+    if (!(orc_uniform(t->h) < bias)) orc_push(t, &t->tp, p2);
+    else orc_push(t, &t->tp, p1);
+    left.n += right.n;
+    const double *tp, *mp, *tm, *mm;
+    if (dir == 0) { tp = orc_peek(&t->ts); mp = orc_peek(&t->ms); tm = theta; mm = mom; }
+    else { tm = orc_peek(&t->ts); mm = orc_peek(&t->ms); tp = theta; mp = mom; }
+    left.s = orc_update_s(t, right.s, tp, mp, tm, mm);
+    if (j > 1) { orc_pop(&t->ts); orc_pop(&t->ms); }
+  }
+  return left;
+}
+
+/* Returns the number of doublings; *leaves_out the leapfrog leaves; 
+ * *overflow_out = 1 if a stack passed the reference's 16 entries (the
+ * reference's behaviour is then undefined). */
+int orc_hlr_nuts(const orc_hlr* m, double* par, const int* idx, int P, double eps, uint64_t seed,
+                 uint32_t iter, uint32_t chain, uint32_t comp, int max_depth, int* leaves_out,
+                 int* overflow_out) {
+  const int NP = m->D + 2;
+  orc_nuts t;
+  memset(&t, 0, sizeof(t));
+  t.m = m; t.idx = idx; t.P = P;
+  double* mem = (double*)calloc((size_t)P * (3 * ORC_STK_MAX + 7) + NP, sizeof(double));
+  double* th0 = mem; double* thm = th0 + P; double* mm = thm + P; double* thp = mm + P;
+  double* mp = thp + P; double* thprop = mp + P; t.work = thprop + P;
+  t.g = t.work + P; t.mod = t.g + P;
+  double* sb = t.mod + NP;
+  for (int i = 0; i < ORC_STK_MAX; ++i) {
+    t.tp.b[i] = sb + (size_t)(3 * i) * P;
+    t.ts.b[i] = sb + (size_t)(3 * i + 1) * P;
+    t.ms.b[i] = sb + (size_t)(3 * i + 2) * P;
+  }
+  t.tp.hd = t.ts.hd = t.ms.hd = -1;
+  memcpy(t.mod, par, sizeof(double) * NP);
+  orc_get_block(par, idx, P, th0);
+  memcpy(thm, th0, sizeof(double) * P);
+  for (int j = 0; j < P; ++j) {
+    orc_stream s = orc_make(seed, chain * (uint32_t)P + j, iter, ORC_TAG_MOM | (comp << 8));
+    mm[j] = orc_normal(&s);
+  }
+  memcpy(thp, th0, sizeof(double) * P);
+  memcpy(mp, mm, sizeof(double) * P);
+  orc_stream h = orc_make(seed, chain, iter, ORC_TAG_NUTS | (comp << 8));
+  t.h = &h;
+  double e = -1.0 * log(orc_uniform(&h));
+  t.logu = orc_hlr_ll(m, par, idx, P) - 0.5 * orc_dot(mm, mm, P) - e;
+  int n = 1, j = 0, s = 1;
+  for (;;) {
+    int f_cpy = 0;
+    orc_nret r;
+    t.ts.hd = -1; t.ms.hd = -1;
+    if (orc_uniform(&h) < 0.5) {
+      t.stepsize = -eps;
+      memcpy(thprop, thm, sizeof(double) * P);
+      r = orc_build(&t, thprop, mm, j, 0);
+      memcpy(thm, thprop, sizeof(double) * P);
+    } else {
+      t.stepsize = eps;
+      memcpy(thprop, thp, sizeof(double) * P);
+      r = orc_build(&t, thprop, mp, j, 1);
+      memcpy(thp, thprop, sizeof(double) * P);
+    }
+    double* pp = orc_pop(&t.tp);
+    if (r.s == 1) {
+      /* augur_min takes and returns unsigned int (cbits/augur_util.c:56-59),
+       * so the ratio is truncated: the bias is 1 when n' >= n, else 0. */
+      unsigned ratio = (unsigned)(((double)r.n) / n);
+      double bias = (double)(ratio < 1u ? ratio : 1u);
+      if (orc_uniform(&h) < bias) { memcpy(thprop, pp, sizeof(double) * P); f_cpy = 1; }
+    }
+    n += r.n;
+    s = orc_update_s(&t, r.s, thp, mp, thm, mm);
+    j += 1;
+    if (s != 1 || j >= max_depth || t.overflow) {
+      if (f_cpy) memcpy(th0, thprop, sizeof(double) * P);
+      break;
+    }
+  }
+  orc_set_block(par, idx, P, th0);
+  if (leaves_out) *leaves_out = t.leaves;
+  if (overflow_out) *overflow_out = t.overflow;
+  free(mem);
+  return j;
+}
+
+/* ---- MWG on a scalar of par: cbits/augur_mcmclib.h:89-105,178-193 with
+ * the generated prop_/swap_ of CgUserProp.hs:131-210.  Proposal
+ * Normal(x, var); compat uses the generated log-correction
+ * ll(x; x, var) - ll(x'; x, var) (both evaluated at the current state);
+ * otherwise the symmetric random walk's correction 0.  Substream
+ * (c, iter, MWG|comp<<8): normal, then the accept uniform. */
+int orc_hlr_mwg(const orc_hlr* m, double* par, int which, double var, uint64_t seed,
+                uint32_t iter, uint32_t chain, uint32_t comp) {
+  const int NP = m->D + 2;
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  memcpy(prop, par, sizeof(double) * NP);
+  orc_stream s = orc_make(seed, chain, iter, ORC_TAG_MWG | (comp << 8));
+  const double x = par[which];
+  const double xp = x + sqrt(var) * orc_normal(&s);
+  prop[which] = xp;
+  double corr = 0.0;
+  if (m->compat) corr = orc_normal_ll(m, x, x, var) - orc_normal_ll(m, xp, x, var);
+  int idx[1] = {which};
+  double currll = orc_hlr_ll(m, par, idx, 1);
+  double propll = orc_hlr_ll(m, prop, idx, 1);
+  double u = orc_uniform(&s);
+  int acc = log(u) < propll - currll + corr;
+  if (acc) par[which] = xp;
+  free(prop);
+  return acc;
+}

@@ -20,5 +20,6 @@ double gsl_rng_uniform(const gsl_rng* r);
 /* Shim extensions: select the Philox substream a generator draws from. */
 void orc_shim_set_seed(uint64_t seed);
 void orc_shim_seek(const gsl_rng* r, uint32_t elem, uint32_t iter, uint32_t tag);
+void orc_shim_seek_elementwise(const gsl_rng* r, uint32_t elem0, uint32_t iter, uint32_t tag);
 uint32_t orc_shim_pos(const gsl_rng* r);
 #endif

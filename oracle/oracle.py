@@ -141,3 +141,132 @@ class Oracle:
         f(D, K, V, iptr(doc_off), iptr(w), dptr(alpha), dptr(beta), dptr(theta), dptr(phi),
           iptr(z), iptr(cnt_dk), iptr(cnt_kw), seed, it0, n)
         return theta, phi, z
+
+
+# ---- HLR -------------------------------------------------------------------
+class OrcHlr(C.Structure):
+    _fields_ = [("N", C.c_int), ("D", C.c_int), ("has_b", C.c_int), ("vprior", C.c_int),
+                ("compat", C.c_int), ("lam", C.c_double), ("a0", C.c_double), ("s0", C.c_double),
+                ("X", _dp), ("y", _ip)]
+
+
+class HlrModel:
+    """Data and hyper-parameters of one HLR instance (oracle side).
+    vprior: "exponential" (hlr.rv, rate lam) or "invgamma" (a0, s0)."""
+
+    def __init__(self, X, y, has_b=True, vprior="exponential", lam=1.0, a0=1.0, s0=1.0, compat=True):
+        self.X = np.ascontiguousarray(X, dtype=np.float64)
+        self.y = np.ascontiguousarray(y, dtype=np.int32)
+        self.N, self.D = self.X.shape
+        self.has_b, self.compat = int(has_b), int(compat)
+        self.vprior = {"exponential": 0, "invgamma": 1}[vprior]
+        self.lam, self.a0, self.s0 = float(lam), float(a0), float(s0)
+
+    def struct(self):
+        return OrcHlr(self.N, self.D, self.has_b, self.vprior, self.compat, self.lam, self.a0, self.s0,
+                      dptr(self.X), iptr(self.y))
+
+    def flat(self):
+        return (self.N, self.D, self.has_b, self.vprior, self.lam, self.a0, self.s0,
+                dptr(self.X), iptr(self.y))
+
+
+_FLAT = [C.c_int] * 4 + [C.c_double] * 3 + [_dp, _ip]
+
+
+def _hlr_call(o, name, m, restype, extra_types, *extra):
+    f = o.fn(name, restype)
+    if o.kind == "ref":
+        if not m.compat:
+            raise ValueError("the reference build only has the reference's own densities")
+        f.argtypes = _FLAT + extra_types
+        return f(*m.flat(), *extra)
+    s = m.struct()
+    f.argtypes = [C.POINTER(OrcHlr)] + extra_types
+    return f(C.byref(s), *extra)
+
+
+def _idx(idx):
+    return np.ascontiguousarray(idx, dtype=np.int32)
+
+
+def hlr_ll(o, m, par, idx):
+    par = np.ascontiguousarray(par, np.float64); idx = _idx(idx)
+    return _hlr_call(o, "hlr_ll", m, C.c_double, [_dp, _ip, C.c_int], dptr(par), iptr(idx), len(idx))
+
+
+def hlr_grad(o, m, par, idx):
+    par = np.ascontiguousarray(par, np.float64); idx = _idx(idx)
+    g = np.zeros(len(idx))
+    _hlr_call(o, "hlr_grad", m, None, [_dp, _ip, C.c_int, _dp], dptr(par), iptr(idx), len(idx), dptr(g))
+    return g
+
+
+def hlr_hmc(o, m, par, idx, simlen, eps, seed, it, chain=0, comp=0):
+    """One HMC transition; par is updated in place."""
+    idx = _idx(idx)
+    if o.kind == "ref":
+        return _hlr_call(o, "hlr_hmc", m, C.c_int,
+                         [_dp, _ip, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32,
+                          C.c_uint32], dptr(par), iptr(idx), len(idx), simlen, eps, seed, it, chain, comp)
+    L = C.c_int()
+    prop = np.zeros(m.D + 2)
+    acc = _hlr_call(o, "hlr_hmc", m, C.c_int,
+                    [_dp, _ip, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32,
+                     C.c_uint32, C.POINTER(C.c_int), _dp],
+                    dptr(par), iptr(idx), len(idx), simlen, eps, seed, it, chain, comp, C.byref(L), dptr(prop))
+    return acc, L.value, prop
+
+
+def hlr_nuts(o, m, par, idx, eps, seed, it, chain=0, comp=0, max_depth=64):
+    idx = _idx(idx)
+    if o.kind == "ref":
+        with _quiet_stdout():
+            _hlr_call(o, "hlr_nuts", m, None,
+                      [_dp, _ip, C.c_int, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32],
+                      dptr(par), iptr(idx), len(idx), eps, seed, it, chain, comp)
+        return None
+    leaves, ovf = C.c_int(), C.c_int()
+    depth = _hlr_call(o, "hlr_nuts", m, C.c_int,
+                      [_dp, _ip, C.c_int, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                       C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+                      dptr(par), iptr(idx), len(idx), eps, seed, it, chain, comp, max_depth,
+                      C.byref(leaves), C.byref(ovf))
+    return depth, leaves.value, ovf.value
+
+
+def hlr_mwg(o, m, par, which, var, seed, it, chain=0, comp=0):
+    return _hlr_call(o, "hlr_mwg", m, C.c_int,
+                     [_dp, C.c_int, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32],
+                     dptr(par), which, var, seed, it, chain, comp)
+
+
+class _quiet_stdout:
+    """Silences the C-level stdout (the reference's NUTS prints its stacks)."""
+
+    def __enter__(self):
+        import sys
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        libc = C.CDLL(None)
+        libc.fflush(None)
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def hlr_synthetic(N, D, seed, vprior="invgamma", has_b=False, x_dtype=np.float64):
+    """Config-style synthetic HLR data: X ~ N(0,1), sigma^2 ~ InvGamma(1,1),
+    beta ~ N(0, sigma^2 I), y ~ Bernoulli(sigmoid(X beta (+ b)))."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((N, D)).astype(x_dtype)
+    s2 = 1.0 / rng.gamma(1.0, 1.0)
+    beta = rng.standard_normal(D) * np.sqrt(s2)
+    b = rng.standard_normal() * np.sqrt(s2) if has_b else 0.0
+    t = X.astype(np.float64) @ beta + b
+    y = (rng.random(N) < 1.0 / (1.0 + np.exp(-t))).astype(np.int32)
+    return X, y, beta, s2

@@ -150,3 +150,260 @@ int ref_unnorm_disc_samp(const double* pmf, int K, uint64_t seed, uint32_t elem,
   orc_shim_seek(rng, elem, iter, tag);
   return augur_unnorm_disc_samp(rng, &v);
 }
+
+/* ------------------------------------------------------------------------
+ * HLR (compiler/augur/test/hlr.rv; InvGamma-variance variant without bias)
+ * Restated generated ll_/grad_/prop_/swap_ functions over the reference's
+ * distribution library, driven by the reference's own h_augur_mcmc_hmc,
+ * h_augur_mcmc_nuts and augur_mcmc_mwg (cbits/augur_mcmclib.h).
+ * Parameter vector par = [theta[0..D-1], b, v]; a block is an index list in
+ * schedule order.  Only the reference's own (compat) densities exist here.
+ * --------------------------------------------------------------------- */
+#include <augur_mcmclib.h>
+#include <augur_blkop.h>
+
+typedef struct {
+  int N, D, has_b, vprior;
+  double lam, a0, s0;
+  const double* X;
+  const int* y;
+  const int* idx;
+  int P;
+  double* gbuf;   /* adjoint block storage, block order */
+} ref_hlr_t;
+
+static ref_hlr_t g_hlr;
+
+static int in_blk(int lo, int hi) {
+  for (int j = 0; j < g_hlr.P; ++j) if (g_hlr.idx[j] >= lo && g_hlr.idx[j] < hi) return 1;
+  return 0;
+}
+
+static double hlr_vprior_ll(double v) {
+  return g_hlr.vprior == 0 ? augur_exponential_ll(v, g_hlr.lam)
+                           : augur_invgamma_ll(v, g_hlr.a0, g_hlr.s0);
+}
+static double hlr_vprior_dot(double v) {
+  return g_hlr.vprior == 0 ? augur_exponential_dotpt(v, g_hlr.lam)
+                           : augur_invgamma_dotpt(v, g_hlr.a0, g_hlr.s0);
+}
+
+/* ll_<blk>: CgLike.hs:139-147 (factors in model order, Pi -> MapRed). */
+static double ref_hlr_ll_fn(AugurAux_t aux, AugurMod_t mod) {
+  const int D = g_hlr.D;
+  double* par = mod.par;
+  double b = g_hlr.has_b ? par[D] : 0.0, v = par[D + 1];
+  int in_th = in_blk(0, D), in_b = g_hlr.has_b && in_blk(D, D + 1), in_v = in_blk(D + 1, D + 2);
+  AugurVec_t th = dvec(par, D);
+  double ll = 0.0;
+  if (in_v) ll += hlr_vprior_ll(v);
+  if (g_hlr.has_b && (in_b || in_v)) ll += augur_normal_ll(b, 0.0, v);
+  if (in_th || in_v) {
+    double s = 0.0;
+    for (int k = 0; k < D; ++k) s += augur_normal_ll(par[k], 0.0, v);
+    ll += s;
+  }
+  if (in_th || in_b) {
+    double s = 0.0;
+    for (int n = 0; n < g_hlr.N; ++n) {
+      AugurVec_t xn = dvec((double*)g_hlr.X + (size_t)n * D, D);
+      double t = augur_dotprod(&th, &xn) + b;
+      s += augur_bernoulli_ll(g_hlr.y[n], augur_expit(t));
+    }
+    ll += s;
+  }
+  return ll;
+}
+
+/* grad_<blk>: CgGrad.hs:165-376; accumulates onto the zeroed adjoint block. */
+static void ref_hlr_grad_fn(AugurAux_t aux, AugurMod_t mod) {
+  const int D = g_hlr.D;
+  double* par = mod.par;
+  double b = g_hlr.has_b ? par[D] : 0.0, v = par[D + 1];
+  int in_th = in_blk(0, D), in_b = g_hlr.has_b && in_blk(D, D + 1), in_v = in_blk(D + 1, D + 2);
+  double* full = (double*)calloc((size_t)D + 2, sizeof(double));
+  AugurVec_t th = dvec(par, D);
+  double* dst = (double*)malloc(sizeof(double) * (size_t)D);
+  AugurVec_t vdst = dvec(dst, D);
+  if (in_v) full[D + 1] += hlr_vprior_dot(v);
+  if (g_hlr.has_b && (in_b || in_v)) {
+    if (in_b) full[D] += augur_normal_dotpt(b, 0.0, v);
+    if (in_v) full[D + 1] += augur_normal_dotarg2(b, 0.0, v);
+  }
+  if (in_th || in_v) {
+    for (int k = 0; k < D; ++k) {
+      if (in_th) full[k] += augur_normal_dotpt(par[k], 0.0, v);
+      if (in_v) full[D + 1] += augur_normal_dotarg2(par[k], 0.0, v);
+    }
+  }
+  if (in_th || in_b) {
+    for (int n = 0; n < g_hlr.N; ++n) {
+      AugurVec_t xn = dvec((double*)g_hlr.X + (size_t)n * D, D);
+      double t2 = augur_dotprod(&th, &xn) + b;
+      double t3 = augur_expit(t2);
+      double adj3 = augur_bernoulli_dotarg1(g_hlr.y[n], t3);
+      double adj2 = adj3 * augur_expit_grad_0(t2);
+      if (in_b) full[D] += adj2 * 1;
+      if (in_th) {
+        augur_dotprod_grad_0(&vdst, adj2 * 1, &th, &xn);
+        for (int k = 0; k < D; ++k) full[k] += dst[k];
+      }
+    }
+  }
+  for (int j = 0; j < g_hlr.P; ++j) g_hlr.gbuf[j] += full[g_hlr.idx[j]];
+  free(full);
+  free(dst);
+}
+
+/* A block over the entries idx of `base` (one AUGUR_DBL component per index,
+ * which is how a block of scalars is grouped; the data layout is what the
+ * block operations see). */
+typedef struct { AugurBlk_t blk; AugurTyp_t* typs; void** ptrs; } ref_blk;
+
+static ref_blk mk_blk_idx(double* base, const int* idx, int P) {
+  ref_blk r;
+  r.typs = (AugurTyp_t*)malloc(sizeof(AugurTyp_t) * P);
+  r.ptrs = (void**)malloc(sizeof(void*) * P);
+  for (int j = 0; j < P; ++j) { r.typs[j] = AUGUR_DBL; r.ptrs[j] = base + idx[j]; }
+  h_augur_blk_mk_group(&r.blk, P, r.typs, r.ptrs);
+  return r;
+}
+
+static ref_blk mk_blk_dense(double* base, int P) {
+  ref_blk r;
+  r.typs = (AugurTyp_t*)malloc(sizeof(AugurTyp_t) * P);
+  r.ptrs = (void**)malloc(sizeof(void*) * P);
+  for (int j = 0; j < P; ++j) { r.typs[j] = AUGUR_DBL; r.ptrs[j] = base + j; }
+  h_augur_blk_mk_group(&r.blk, P, r.typs, r.ptrs);
+  return r;
+}
+
+static void free_blk(ref_blk* r) {
+  free(r->blk.typs); free(r->blk.blks); free(r->typs); free(r->ptrs);
+}
+
+static gsl_rng* g_aux_rng = NULL;
+
+static void ref_hlr_setup(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                          const double* X, const int* y, const int* idx, int P, uint64_t seed) {
+  orc_shim_set_seed(seed);
+  if (g_aux_rng == NULL) {
+    g_aux_rng = gsl_rng_alloc(gsl_rng_default);
+    initMcmc();                 /* h_rng and MCMC defaults (deltaMax = 1000) */
+  }
+  g_hlr.N = N; g_hlr.D = D; g_hlr.has_b = has_b; g_hlr.vprior = vprior;
+  g_hlr.lam = lam; g_hlr.a0 = a0; g_hlr.s0 = s0;
+  g_hlr.X = X; g_hlr.y = y; g_hlr.idx = idx; g_hlr.P = P;
+}
+
+double ref_hlr_ll(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                  const double* X, const int* y, const double* par, const int* idx, int P) {
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, idx, P, 0);
+  AugurAux_t aux; AugurMod_t mod;
+  aux.rng = g_aux_rng; mod.par = (double*)par;
+  return ref_hlr_ll_fn(aux, mod);
+}
+
+void ref_hlr_grad(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                  const double* X, const int* y, const double* par, const int* idx, int P, double* g) {
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, idx, P, 0);
+  AugurAux_t aux; AugurMod_t mod;
+  aux.rng = g_aux_rng; mod.par = (double*)par;
+  memset(g, 0, sizeof(double) * P);
+  g_hlr.gbuf = g;
+  ref_hlr_grad_fn(aux, mod);
+}
+
+/* One HMC transition through the reference's h_augur_mcmc_hmc. */
+int ref_hlr_hmc(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                const double* X, const int* y, double* par, const int* idx, int P, double simlen,
+                double eps, uint64_t seed, uint32_t iter, uint32_t chain, uint32_t comp) {
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, idx, P, seed);
+  const int NP = D + 2;
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  double* mem = (double*)calloc((size_t)3 * P, sizeof(double));
+  memcpy(prop, par, sizeof(double) * NP);
+  g_hlr.gbuf = mem;
+  ref_blk th0 = mk_blk_idx(par, idx, P), ths = mk_blk_idx(prop, idx, P);
+  ref_blk gb = mk_blk_dense(mem, P), p0 = mk_blk_dense(mem + P, P), ps = mk_blk_dense(mem + 2 * P, P);
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = g_aux_rng; curr.par = par; pr.par = prop;
+  orc_shim_seek_elementwise(g_aux_rng, chain * (uint32_t)P, iter, ORC_TAG_MOM | (comp << 8));
+  orc_shim_seek(h_rng, chain, iter, ORC_TAG_HMC | (comp << 8));
+  double before = par[idx[0]];
+  MCMC.aux = aux; MCMC.curr = curr; MCMC.prop = pr;   /* as the generated init does */
+  h_augur_mcmc_hmc(AUGUR_CPU, aux, curr, pr, &th0.blk, &ths.blk, &gb.blk, &p0.blk, &ps.blk, simlen,
+                   eps, ref_hlr_grad_fn, ref_hlr_ll_fn);
+  int moved = 0;
+  for (int j = 0; j < P; ++j) if (par[idx[j]] != prop[idx[j]]) moved = 1;
+  (void)before;
+  free_blk(&th0); free_blk(&ths); free_blk(&gb); free_blk(&p0); free_blk(&ps);
+  free(prop); free(mem);
+  return !moved;   /* invariant curr == prop holds after the kernel; 1 = states agree */
+}
+
+/* One NUTS transition through the reference's h_augur_mcmc_nuts.  The
+ * reference prints its proposal stack at every inner node. */
+void ref_hlr_nuts(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                  const double* X, const int* y, double* par, const int* idx, int P, double eps,
+                  uint64_t seed, uint32_t iter, uint32_t chain, uint32_t comp) {
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, idx, P, seed);
+  const int NP = D + 2;
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  double* mem = (double*)calloc((size_t)7 * P, sizeof(double));
+  memcpy(prop, par, sizeof(double) * NP);
+  g_hlr.gbuf = mem;
+  ref_blk th0 = mk_blk_idx(par, idx, P), thp = mk_blk_idx(prop, idx, P);
+  ref_blk gb = mk_blk_dense(mem, P), work = mk_blk_dense(mem + P, P);
+  ref_blk tm = mk_blk_dense(mem + 2 * P, P), mm = mk_blk_dense(mem + 3 * P, P);
+  ref_blk tpl = mk_blk_dense(mem + 4 * P, P), mpl = mk_blk_dense(mem + 5 * P, P);
+  ref_blk shape = mk_blk_dense(mem + 6 * P, P);
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = g_aux_rng; curr.par = par; pr.par = prop;
+  orc_shim_seek_elementwise(g_aux_rng, chain * (uint32_t)P, iter, ORC_TAG_MOM | (comp << 8));
+  orc_shim_seek(h_rng, chain, iter, ORC_TAG_NUTS | (comp << 8));
+  MCMC.aux = aux; MCMC.curr = curr; MCMC.prop = pr;   /* as the generated init does */
+  h_augur_mcmc_nuts(AUGUR_CPU, aux, curr, pr, &th0.blk, &thp.blk, &gb.blk, &work.blk, &tm.blk,
+                    &mm.blk, &tpl.blk, &mpl.blk, &shape.blk, eps, ref_hlr_grad_fn, ref_hlr_ll_fn);
+  free_blk(&th0); free_blk(&thp); free_blk(&gb); free_blk(&work); free_blk(&tm); free_blk(&mm);
+  free_blk(&tpl); free_blk(&mpl); free_blk(&shape);
+  free(prop); free(mem);
+}
+
+/* MWG on one scalar of par through augur_mcmc_mwg, with the generated
+ * prop_/swap_ (CgUserProp.hs:131-186): x' ~ Normal(x, var), llCorrect =
+ * ll(x; x, var) - ll(x'; x, var). */
+static int g_mwg_which;
+static double g_mwg_var, g_mwg_corr;
+
+static void ref_mwg_prop(AugurAux_t aux, AugurMod_t curr, AugurMod_t prop) {
+  double x = curr.par[g_mwg_which];
+  double xp = augur_normal_sample(aux.rng, x, g_mwg_var);
+  prop.par[g_mwg_which] = xp;
+  g_mwg_corr = augur_normal_ll(x, x, g_mwg_var) - augur_normal_ll(xp, x, g_mwg_var);
+}
+
+static void ref_mwg_swap(AugurAux_t aux, AugurMod_t curr, AugurMod_t prop, int dir) {
+  if (dir == 0) curr.par[g_mwg_which] = prop.par[g_mwg_which];
+  else prop.par[g_mwg_which] = curr.par[g_mwg_which];
+}
+
+int ref_hlr_mwg(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                const double* X, const int* y, double* par, int which, double var, uint64_t seed,
+                uint32_t iter, uint32_t chain, uint32_t comp) {
+  static int one[1];
+  one[0] = which;
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, one, 1, seed);
+  const int NP = D + 2;
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  memcpy(prop, par, sizeof(double) * NP);
+  g_mwg_which = which; g_mwg_var = var;
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = g_aux_rng; curr.par = par; pr.par = prop;
+  orc_shim_seek(g_aux_rng, chain, iter, ORC_TAG_MWG | (comp << 8));
+  double before = par[which];
+  MCMC.aux = aux; MCMC.curr = curr; MCMC.prop = pr;   /* as the generated init does */
+  augur_mcmc_mwg(aux, curr, pr, &g_mwg_corr, ref_mwg_prop, ref_mwg_swap, ref_hlr_ll_fn);
+  free(prop);
+  return par[which] != before;
+}

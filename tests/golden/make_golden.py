@@ -99,9 +99,50 @@ def make_lda(ref):
                         beta=beta, theta0=theta0, phi0=phi0, z0=z0, theta=theta, phi=phi, z=z)
 
 
+def make_hlr(ref):
+    """HLR on the reference's hlr.rv model (Exponential variance prior with
+    bias) and on the InvGamma variant without bias: log-densities, gradients
+    and HMC / NUTS / MWG transitions of the reference's own kernels."""
+    out = {}
+    for name, (N, D, has_b, vprior) in {"hlr": (120, 6, True, "exponential"),
+                                        "ighlr": (150, 4, False, "invgamma")}.items():
+        X, y, beta, s2 = O.hlr_synthetic(N, D, seed=N + D, has_b=has_b)
+        m = O.HlrModel(X, y, has_b=has_b, vprior=vprior, lam=1.0, a0=1.0, s0=1.0, compat=True)
+        rng = np.random.default_rng(N)
+        par0 = np.concatenate([beta * 0.7, [0.2 if has_b else 0.0], [max(0.3, s2)]])
+        blocks = {"theta": list(range(D)), "v": [D + 1], "joint": [D + 1] + ([D] if has_b else []) + list(range(D))}
+        if has_b:
+            blocks["b"] = [D]
+        pars = par0 + 0.1 * rng.standard_normal((5, D + 2))
+        pars[:, D + 1] = np.abs(pars[:, D + 1]) + 0.1
+        if not has_b:
+            pars[:, D] = 0.0
+        rec = {"X": X, "y": y, "pars": pars, "N": N, "D": D, "has_b": int(has_b), "vprior": m.vprior}
+        for bname, idx in blocks.items():
+            rec["ll_" + bname] = np.array([O.hlr_ll(ref, m, p, idx) for p in pars])
+            rec["grad_" + bname] = np.array([O.hlr_grad(ref, m, p, idx) for p in pars])
+            rec["idx_" + bname] = np.array(idx, np.int32)
+        # chains of transitions (seed 7): HMC on theta, NUTS on the joint block, MWG on v
+        p = par0.copy(); hmc = []
+        for it in range(6):
+            O.hlr_hmc(ref, m, p, blocks["theta"], 0.3, 0.05, 7, it)
+            hmc.append(p.copy())
+        p = par0.copy(); nuts = []
+        for it in range(6):
+            O.hlr_nuts(ref, m, p, blocks["joint"], 0.05, 7, it)
+            nuts.append(p.copy())
+        p = par0.copy(); mwg = []
+        for it in range(6):
+            O.hlr_mwg(ref, m, p, D + 1, 0.5, 7, it)
+            mwg.append(p.copy())
+        rec.update(par0=par0, hmc=np.array(hmc), nuts=np.array(nuts), mwg=np.array(mwg))
+        np.savez_compressed(os.path.join(HERE, name + "_golden.npz"), **rec)
+
+
 if __name__ == "__main__":
     O.build_oracle()
     ref = O.Oracle("ref")
     make_primitives(ref)
     make_lda(ref)
+    make_hlr(ref)
     print("golden fixtures written to", HERE)

@@ -104,3 +104,74 @@ def test_gamma_moments(orc):
     for s in [0.1, 1.0, 4.0]:
         x = np.array([orc.gamma_sample(s, 2.0, 9, e, 0, 2) for e in range(20000)])
         assert abs(x.mean() - s / 2.0) < 5 * np.sqrt(s / 4.0 / 20000)
+
+
+# ---- HLR ------------------------------------------------------------------
+def _hlr_model(g, compat=True):
+    vprior = "exponential" if int(g["vprior"]) == 0 else "invgamma"
+    return O.HlrModel(g["X"], g["y"], has_b=bool(g["has_b"]), vprior=vprior, lam=1.0, a0=1.0,
+                      s0=1.0, compat=compat)
+
+
+@pytest.mark.parametrize("name", ["hlr", "ighlr"])
+def test_hlr_golden_ll_grad(orc, name):
+    g = np.load(os.path.join(GOLD, name + "_golden.npz"))
+    m = _hlr_model(g)
+    for key in [k for k in g.files if k.startswith("ll_")]:
+        b = key[3:]
+        idx = g["idx_" + b]
+        ll = np.array([O.hlr_ll(orc, m, p, idx) for p in g["pars"]])
+        gr = np.array([O.hlr_grad(orc, m, p, idx) for p in g["pars"]])
+        np.testing.assert_array_equal(ll, g[key])
+        np.testing.assert_array_equal(gr, g["grad_" + b])
+
+
+@pytest.mark.parametrize("name", ["hlr", "ighlr"])
+def test_hlr_golden_transitions(orc, name):
+    g = np.load(os.path.join(GOLD, name + "_golden.npz"))
+    m = _hlr_model(g)
+    D = int(g["D"])
+    p = g["par0"].copy()
+    for it in range(6):
+        O.hlr_hmc(orc, m, p, g["idx_theta"], 0.3, 0.05, 7, it)
+        np.testing.assert_array_equal(p, g["hmc"][it])
+    p = g["par0"].copy()
+    for it in range(6):
+        O.hlr_nuts(orc, m, p, g["idx_joint"], 0.05, 7, it)
+        np.testing.assert_array_equal(p, g["nuts"][it])
+    p = g["par0"].copy()
+    for it in range(6):
+        O.hlr_mwg(orc, m, p, D + 1, 0.5, 7, it)
+        np.testing.assert_array_equal(p, g["mwg"][it])
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_hlr_oracle_vs_reference_live(orc, ref, seed):
+    X, y, beta, s2 = O.hlr_synthetic(90, 3, seed, has_b=True)
+    m = O.HlrModel(X, y, has_b=True, vprior="exponential")
+    D = 3
+    par = np.concatenate([beta, [0.1], [1.0]])
+    for idx in [[0, 1, 2], [3], [4], [4, 3, 0, 1, 2]]:
+        assert O.hlr_ll(orc, m, par, idx) == O.hlr_ll(ref, m, par, idx)
+        np.testing.assert_array_equal(O.hlr_grad(orc, m, par, idx), O.hlr_grad(ref, m, par, idx))
+    for it in range(4):
+        a, b = par.copy(), par.copy()
+        O.hlr_nuts(orc, m, a, [4, 3, 0, 1, 2], 0.1, seed, it)
+        O.hlr_nuts(ref, m, b, [4, 3, 0, 1, 2], 0.1, seed, it)
+        np.testing.assert_array_equal(a, b)
+
+
+def test_hlr_gradient_finite_difference(orc):
+    """Exact-density gradient against central differences (the idea of
+    h_augur_chk_grad, cbits/augur_mcmclib.h:199-250)."""
+    X, y, beta, s2 = O.hlr_synthetic(300, 4, 5, has_b=True)
+    m = O.HlrModel(X, y, has_b=True, vprior="exponential", compat=False)
+    par = np.concatenate([beta * 0.3, [0.2], [0.8]])
+    idx = [5, 4, 0, 1, 2, 3]
+    g = O.hlr_grad(orc, m, par, idx)
+    h = 1e-6
+    for j, i in enumerate(idx):
+        pp, pm = par.copy(), par.copy()
+        pp[i] += h; pm[i] -= h
+        fd = (O.hlr_ll(orc, m, pp, idx) - O.hlr_ll(orc, m, pm, idx)) / (2 * h)
+        assert abs(fd - g[j]) <= 1e-5 * max(1.0, abs(g[j]))
