@@ -75,6 +75,10 @@ _SIGS = {
     "ab_lda_init_state": (i32, [vp, u32, vp]),
     "ab_lda_run": (i32, [vp, i32, i32, vp]),
     "ab_lda_destroy": (i32, [vp]),
+    # HLR
+    "ab_hlr_ll_grad": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp]),
+    "ab_hlr_chain_scratch_bytes": (sz, [i32, i32]),
+    "ab_hlr_run_chains": (i32, [vp, vp, vp, i32, vp, vp, i32, vp, i32, u32, u64, vp, vp, vp]),
 }
 
 

@@ -118,6 +118,58 @@ int ab_lda_init_state(ab_lda* h, uint32_t iter, void* stream);
 int ab_lda_run(ab_lda* h, int n_sweeps, int use_graph, void* stream);
 int ab_lda_destroy(ab_lda* h);
 
+/* ======================================================================= *
+ * Hierarchical logistic regression (compiler/augur/test/hlr.rv; and the
+ * variant with an InvGamma variance prior and no bias).  Parameters of one
+ * chain: f64 par[D+2] = [theta[0..D-1], b, v].  A block is a list of indices
+ * into par in the schedule's order (HMC [v, b, theta] -> D+1, D, 0..D-1).
+ * ======================================================================= */
+enum { AB_F32 = 0, AB_BF16 = 1 };
+
+typedef struct ab_hlr_model {
+  int N, D, ldx;        /* rows, features, row stride of X (elements)         */
+  int has_b;            /* model has the bias b ~ Normal(0, v)                */
+  int vprior;           /* 0: v ~ Exponential(lam); 1: v ~ InvGamma(a0, s0)   */
+  int compat;           /* 1: the reference's own density formulas (its Normal
+                           log density -log(var) - t^2/2var and dNormal/dvar)  */
+  int x_dtype;          /* AB_F32 or AB_BF16                                  */
+  double lam, a0, s0;
+  const void* X;        /* device [N][ldx] */
+  const int* y;         /* device [N], 0/1 */
+} ab_hlr_model;
+
+/* One schedule component: kind 0 = HMC [block] [simlen, eps]
+ * (h_augur_mcmc_hmc, cbits/augur_mcmclib.h:389-424), 1 = NUTS [block] [eps]
+ * (h_augur_mcmc_nuts, :693-776; max_depth bounds the doublings), 2 = MWG on
+ * one scalar with a Normal(x, mwg_var) proposal (augur_mcmc_mwg, :178-193).
+ * The block is idx[idx_off .. idx_off+P-1] of the index array. */
+typedef struct ab_hlr_comp {
+  int kind, P, idx_off, max_depth;
+  double simlen, eps, mwg_var;
+} ab_hlr_comp;
+
+/* Block log full-conditional and its gradient for C parameter vectors:
+ * replaces the generated ll_<blk> / grad_<blk> functions (CgLike.hs:139-147,
+ * CgGrad.hs:345-376).  ll f64[C]; grad f64[C][P] (may be NULL).  The block
+ * indices are given both on the device (read by the kernel) and on the host
+ * (validated). */
+int ab_hlr_ll_grad(const ab_hlr_model* model, const int* idx_dev, const int* idx_host, int P, int C,
+                   const double* pars, double* ll, double* grad, void* stream);
+
+/* n_iter augur_step calls of a schedule of components for C independent
+ * chains (one thread block per chain, the whole iteration on chip).
+ * pars f64[C][D+2] in/out; stats f64[C][n_comps][4] accumulates {accepts,
+ * NUTS depth, NUTS leaves, stack overflows}.  scratch:
+ * ab_hlr_chain_scratch_bytes(C, D) bytes, needed when a NUTS component is
+ * present.  Substreams: momentum (c*P+j, iter, 4|comp<<8), HMC jitter and
+ * accept (c, iter, 5|comp<<8), NUTS (c, iter, 6|comp<<8), MWG (c, iter,
+ * 11|comp<<8). */
+size_t ab_hlr_chain_scratch_bytes(int C, int D);
+int ab_hlr_run_chains(const ab_hlr_model* model, const ab_hlr_comp* comps_host, const void* comps_dev,
+                      int n_comps, const int* idx_dev, const int* idx_host, int C, double* pars,
+                      int n_iter, uint32_t iter0, uint64_t seed, double* stats, void* scratch,
+                      void* stream);
+
 #ifdef __cplusplus
 }
 #endif
