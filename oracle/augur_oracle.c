@@ -580,3 +580,351 @@ int orc_hlr_mwg(const orc_hlr* m, double* par, int which, double var, uint64_t s
   free(prop);
   return acc;
 }
+
+/* ------------------------------------------------------------------------
+ * Gaussian mixtures (compiler/augur/test/mvgmm.rv, hmvgmm.rv).
+ * Square d x d row-major matrices, operations restated from
+ * cbits/augur_matop.c:312-420 and the samplers of cbits/augur_dist.c:543-757,
+ * each with the reference's loop order.
+ * --------------------------------------------------------------------- */
+#define M_(A, i, j) (A)[(size_t)(i) * d + (j)]
+
+/* augur_mat_cholesky (:312-328): lower factor in place, upper unchanged. */
+void orc_mat_cholesky(double* A, int d) {
+  for (int i = 0; i < d; i++)
+    for (int j = 0; j < i + 1; j++) {
+      double s = 0.0;
+      for (int k = 0; k < j; k++) s += M_(A, i, k) * M_(A, j, k);
+      if (i == j) M_(A, i, j) = sqrt(M_(A, i, i) - s);
+      else M_(A, i, j) = 1.0 / M_(A, j, j) * (M_(A, i, j) - s);
+    }
+}
+
+/* augur_mat_lower_trmi (:335-345). */
+void orc_mat_lower_trmi(double* L, int d) {
+  for (int c = 0; c < d; c++)
+    for (int m = 0; m < d; m++) {
+      double b = (c == m) ? 1.0 : 0.0;
+      for (int i = 0; i < m; i++) b -= M_(L, m, i) * M_(L, i, c);
+      M_(L, m, c) = b / M_(L, m, m);
+    }
+}
+
+/* augur_mat_cholesky_invert (:363-375) with augur_mat_lower_trtcpy (:351-357). */
+void orc_mat_cholesky_invert(double* A, int d) {
+  orc_mat_lower_trmi(A, d);
+  for (int c = 0; c < d; c++)
+    for (int r = c; r < d; r++) {
+      double acc = 0.0;
+      for (int k = c; k < d; k++) acc += M_(A, k, r) * M_(A, k, c);
+      M_(A, r, c) = acc;
+    }
+  for (int c = 0; c < d; c++)
+    for (int r = c + 1; r < d; r++) M_(A, c, r) = M_(A, r, c);
+}
+
+/* augur_mat_trtrmm (:381-392): L2 = L1 L2. */
+static void orc_mat_trtrmm(const double* L1, double* L2, int d) {
+  for (int i = d; i > 0 && i--;) {
+    for (int j = 0; j < d; j++) {
+      double tmp = 0.0;
+      for (int k = 0; k < i; k++) tmp += M_(L1, i, k) * M_(L2, k, j);
+      tmp += M_(L1, i, i) * M_(L2, i, j);
+      M_(L2, i, j) = tmp;
+    }
+  }
+}
+
+/* augur_mat_trvm (:398-406): v = L v. */
+static void orc_mat_trvm(const double* L, double* v, int d) {
+  for (int i = d - 1; i >= 0; i--) {
+    double tmp = 0.0;
+    for (int j = 0; j <= i; j++) tmp += M_(L, i, j) * v[j];
+    v[i] = tmp;
+  }
+}
+
+/* augur_mat_mvm (:412-420): dst = A v. */
+static void orc_mat_mvm(double* dst, const double* A, const double* v, int d) {
+  for (int i = 0; i < d; i++) {
+    double tmp = 0.0;
+    for (int j = 0; j < d; j++) tmp += M_(A, i, j) * v[j];
+    dst[i] = tmp;
+  }
+}
+
+/* augur_mvnormal_ll (augur_dist.c:548-568). */
+double orc_mvnormal_ll(const double* pt, const double* mean, const double* cov, int d) {
+  double* L = (double*)malloc(sizeof(double) * d * d);
+  double* w = (double*)malloc(sizeof(double) * d);
+  for (int i = 0; i < d; i++) w[i] = pt[i] - mean[i];
+  memcpy(L, cov, sizeof(double) * d * d);
+  orc_mat_cholesky(L, d);
+  double det = 1.0;
+  for (int i = 0; i < d; i++) det *= M_(L, i, i);
+  det *= det;
+  orc_mat_lower_trmi(L, d);
+  orc_mat_trvm(L, w, d);
+  double expon = 0.0;
+  for (int i = 0; i < d; i++) expon += w[i] * w[i];
+  double c = -0.5 * ((double)d) * log(2.0 * 3.14159265358979323846264338327950288);
+  free(L); free(w);
+  return c - 0.5 * log(det) - 0.5 * expon;
+}
+
+/* augur_mvnormal_sample (:622-630): result = chol(cov) z + mean. */
+static void orc_mvnormal_sample(orc_stream* s, double* result, const double* mean, const double* cov, int d) {
+  double* L = (double*)malloc(sizeof(double) * d * d);
+  for (int i = 0; i < d; i++) result[i] = orc_normal(s);
+  memcpy(L, cov, sizeof(double) * d * d);
+  orc_mat_cholesky(L, d);
+  orc_mat_trvm(L, result, d);
+  for (int i = 0; i < d; i++) result[i] = result[i] + mean[i];
+  free(L);
+}
+
+/* augur_mvnormal_mvnormal_conj (:633-669).  `sum` is scaled in place by
+ * 1/cnt as in the reference. */
+static void orc_mvn_mvn_conj(orc_stream* s, double* result, const double* mu0, const double* cov0,
+                             double* sum, int cnt, const double* cov, int d) {
+  double* L0 = (double*)malloc(sizeof(double) * d * d);
+  double* L = (double*)malloc(sizeof(double) * d * d);
+  double* w0 = (double*)malloc(sizeof(double) * d);
+  double* mean = (double*)malloc(sizeof(double) * d);
+  memcpy(L0, cov0, sizeof(double) * d * d);
+  orc_mat_cholesky(L0, d);
+  orc_mat_cholesky_invert(L0, d);
+  memcpy(L, cov, sizeof(double) * d * d);
+  orc_mat_cholesky(L, d);
+  orc_mat_cholesky_invert(L, d);
+  for (int i = 0; i < d * d; i++) L[i] = cnt * L[i];             /* augur_mat_ms */
+  orc_mat_mvm(result, L0, mu0, d);
+  double sc = cnt == 0 ? 1.0 : 1.0 / cnt;                         /* augur_vec_scale */
+  for (int i = 0; i < d; i++) sum[i] = sc * sum[i];
+  orc_mat_mvm(w0, L, sum, d);
+  for (int i = 0; i < d; i++) result[i] = result[i] + w0[i];
+  for (int i = 0; i < d * d; i++) L0[i] = L0[i] + L[i];           /* augur_mat_plus */
+  orc_mat_cholesky(L0, d);
+  orc_mat_cholesky_invert(L0, d);
+  orc_mat_mvm(mean, L0, result, d);
+  orc_mvnormal_sample(s, result, mean, L0, d);
+  free(L0); free(L); free(w0); free(mean);
+}
+
+/* bartlett_decomp (:722-738) with augur_chisquared_sample (:213-220). */
+static void orc_bartlett(orc_stream* s, int n, double* A, int d) {
+  for (int i = 0; i < d; i++)
+    for (int j = 0; j < d; j++) {
+      if (j < i) M_(A, i, j) = orc_normal(s);
+      else if (j > i) M_(A, i, j) = 0.0;
+      else {
+        double chi = 0.0;
+        for (int t = 0; t < n - i; t++) { double z = orc_normal(s); chi += z * z; }
+        M_(A, i, j) = sqrt(chi);
+      }
+    }
+}
+
+/* augur_invwishart_sample (:740-749). */
+static void orc_invwishart_sample(orc_stream* s, double* result, int df, const double* scale, int d) {
+  double* L = (double*)malloc(sizeof(double) * d * d);
+  memcpy(L, scale, sizeof(double) * d * d);
+  orc_mat_cholesky(L, d);
+  orc_mat_cholesky_invert(L, d);
+  orc_mat_cholesky(L, d);
+  orc_bartlett(s, df, result, d);
+  orc_mat_trtrmm(L, result, d);
+  orc_mat_cholesky_invert(result, d);
+  free(L);
+}
+
+/* Dirichlet-Categorical conjugate draw of a K-vector (augur_dist.c:526-538),
+ * element substream (k, iter, tag). */
+static void orc_dirichlet_vec(int K, const double* alpha, const int* cnt, double* out, uint64_t seed,
+                              uint32_t iter, uint32_t tag) {
+  orc_dirichlet_rows(1, K, alpha, cnt, out, seed, iter, tag);
+}
+
+typedef struct {
+  int N, d, K, shared_cov;     /* shared_cov: mvgmm (one covs); else hmvgmm cov[K] */
+  const double* Y;             /* N x d */
+  const double* mu0;           /* d */
+  const double* cov0;          /* d x d */
+  const double* alpha;         /* K (hmvgmm) */
+  int df;                      /* InvWishart df (hmvgmm) */
+  const double* scale0;        /* d x d (hmvgmm) */
+} orc_gmm;
+
+/* disc_z (CgDisc.hs:122-156): pmf[k] = (1 * pis[k]) * mvnormal_pdf(y, mu[k],
+ * cov[k]) (augur_mvnormal_pdf = exp(ll)), then augur_unnorm_disc_samp.
+ * Substream (n, iter, Z). */
+void orc_gmm_disc_z(const orc_gmm* g, const double* pis, const double* mu, const double* cov,
+                    int* z, uint64_t seed, uint32_t iter) {
+  const int d = g->d, K = g->K;
+  double* pmf = (double*)malloc(sizeof(double) * K);
+  for (int n = 0; n < g->N; n++) {
+    for (int k = 0; k < K; k++) {
+      const double* ck = g->shared_cov ? cov : cov + (size_t)k * d * d;
+      double prob = 1.0;
+      prob *= pis[k];
+      prob *= exp(orc_mvnormal_ll(g->Y + (size_t)n * d, mu + (size_t)k * d, ck, d));
+      pmf[k] = prob;
+    }
+    orc_stream s = orc_make(seed, (uint32_t)n, iter, ORC_TAG_Z);
+    z[n] = orc_unnorm_disc(&s, pmf, K);
+  }
+  free(pmf);
+}
+
+/* Statistics of CgConj.hs:186-246 (AtomicPar over n, sequential here):
+ * cnt[k], sum[k] = sum of y, obs[k] = sum of (y - mu[z])(y - mu[z])^T. */
+void orc_gmm_stats(const orc_gmm* g, const int* z, const double* mu, int* cnt, double* sum, double* obs) {
+  const int d = g->d, K = g->K;
+  memset(cnt, 0, sizeof(int) * K);
+  if (sum) memset(sum, 0, sizeof(double) * K * d);
+  if (obs) memset(obs, 0, sizeof(double) * K * d * d);
+  double* diff = (double*)malloc(sizeof(double) * d);
+  for (int n = 0; n < g->N; n++) {
+    const int k = z[n];
+    const double* y = g->Y + (size_t)n * d;
+    cnt[k] += 1;
+    if (sum) for (int i = 0; i < d; i++) sum[(size_t)k * d + i] += y[i];
+    if (obs) {
+      for (int i = 0; i < d; i++) diff[i] = y[i] - mu[(size_t)k * d + i];
+      double* O = obs + (size_t)k * d * d;
+      for (int i = 0; i < d; i++)
+        for (int j = 0; j < d; j++) O[(size_t)i * d + j] += diff[i] * diff[j];
+    }
+  }
+  free(diff);
+}
+
+/* ConjGibbs [pis]: Dirichlet(alpha + cnt), element substream (k, iter, PI). */
+void orc_gmm_conj_pis(const orc_gmm* g, const int* cnt, double* pis, uint64_t seed, uint32_t iter) {
+  orc_dirichlet_vec(g->K, g->alpha, cnt, pis, seed, iter, ORC_TAG_PI);
+}
+
+/* ConjGibbs [mu]: per k augur_mvnormal_mvnormal_conj with the covariance of
+ * component k (patched argument, CgConj.hs:260-266), substream (k, iter, MU). */
+void orc_gmm_conj_mu(const orc_gmm* g, const int* cnt, double* sum, const double* cov, double* mu,
+                     uint64_t seed, uint32_t iter) {
+  const int d = g->d;
+  for (int k = 0; k < g->K; k++) {
+    orc_stream s = orc_make(seed, (uint32_t)k, iter, ORC_TAG_MU);
+    const double* ck = g->shared_cov ? cov : cov + (size_t)k * d * d;
+    orc_mvn_mvn_conj(&s, mu + (size_t)k * d, g->mu0, g->cov0, sum + (size_t)k * d, cnt[k], ck, d);
+  }
+}
+
+/* ConjGibbs [cov]: augur_invwishart_mvnormal_conj (:751-757): obs += scale0,
+ * then InvWishart(cnt + df, obs), substream (k, iter, COV).  obs is updated
+ * in place as in the reference. */
+void orc_gmm_conj_cov(const orc_gmm* g, const int* cnt, double* obs, double* cov, uint64_t seed,
+                      uint32_t iter) {
+  const int d = g->d;
+  for (int k = 0; k < g->K; k++) {
+    double* O = obs + (size_t)k * d * d;
+    for (int i = 0; i < d * d; i++) O[i] += g->scale0[i];
+    orc_stream s = orc_make(seed, (uint32_t)k, iter, ORC_TAG_COV);
+    orc_invwishart_sample(&s, cov + (size_t)k * d * d, cnt[k] + g->df, O, d);
+  }
+}
+
+/* One augur_step of ConjGibbs [pis] (*) ConjGibbs [mu] (*) ConjGibbs [cov]
+ * (*) DiscGibbs [z] (hmvgmm), or ConjGibbs [mu] (*) DiscGibbs [z] (mvgmm;
+ * pis and cov fixed). */
+void orc_gmm_sweep(const orc_gmm* g, double* pis, double* mu, double* cov, int* z, uint64_t seed,
+                   uint32_t iter) {
+  const int d = g->d, K = g->K;
+  int* cnt = (int*)malloc(sizeof(int) * K);
+  double* sum = (double*)malloc(sizeof(double) * K * d);
+  double* obs = (double*)malloc(sizeof(double) * K * d * d);
+  if (!g->shared_cov) {
+    orc_gmm_stats(g, z, mu, cnt, NULL, NULL);
+    orc_gmm_conj_pis(g, cnt, pis, seed, iter);
+  }
+  orc_gmm_stats(g, z, mu, cnt, sum, NULL);
+  orc_gmm_conj_mu(g, cnt, sum, cov, mu, seed, iter);
+  if (!g->shared_cov) {
+    orc_gmm_stats(g, z, mu, cnt, NULL, obs);
+    orc_gmm_conj_cov(g, cnt, obs, cov, seed, iter);
+  }
+  orc_gmm_disc_z(g, pis, mu, cov, z, seed, iter);
+  free(cnt); free(sum); free(obs);
+}
+
+/* Full conditional of mu[k] (CgLike.hs:236-265 llFnDeclOne): its prior
+ * MvNormal(mu0, cov0), then the sum over points of component k. */
+double orc_gmm_ll_mu(const orc_gmm* g, const double* muk, int k, const double* cov, const int* z) {
+  const int d = g->d;
+  const double* ck = g->shared_cov ? cov : cov + (size_t)k * d * d;
+  double ll = 0.0;
+  ll += orc_mvnormal_ll(muk, g->mu0, g->cov0, d);
+  double s = 0.0;
+  for (int n = 0; n < g->N; n++)
+    if (z[n] == k) s += orc_mvnormal_ll(g->Y + (size_t)n * d, muk, ck, d);
+  ll += s;
+  return ll;
+}
+
+/* ESlice [mu]: augur_mcmc_eslice (augur_mcmclib.h:439-485) per component,
+ * substream (k, iter, ESLICE): nu ~ N(mu0, cov0) (d normals), u, theta,
+ * then one uniform per shrink.  Returns the number of shrink steps. */
+int orc_gmm_eslice(const orc_gmm* g, double* mu, const double* cov, const int* z, uint64_t seed,
+                   uint32_t iter) {
+  const int d = g->d;
+  const double PI2 = 2.0 * 3.14159265358979323846264338327950288;
+  double* nu = (double*)malloc(sizeof(double) * d);
+  double* prop = (double*)malloc(sizeof(double) * d);
+  int shrinks = 0;
+  for (int k = 0; k < g->K; k++) {
+    double* cur = mu + (size_t)k * d;
+    orc_stream s = orc_make(seed, (uint32_t)k, iter, ORC_TAG_ESLICE);
+    orc_mvnormal_sample(&s, nu, g->mu0, g->cov0, d);
+    double u = orc_uniform(&s);
+    double log_y = orc_gmm_ll_mu(g, cur, k, cov, z) + log(u);
+    double theta = 0.0 + orc_uniform(&s) * (PI2 - 0.0);
+    double tmin = theta - PI2, tmax = theta;
+    for (;;) {
+      double diff = tmax - tmin;
+      if (diff < 1e-8) break;
+      for (int i = 0; i < d; i++) {
+        double mean_i = g->mu0[i];
+        double a = (cur[i] - mean_i) * cos(theta);
+        double b = (nu[i] - mean_i) * sin(theta);
+        prop[i] = a + b + mean_i;
+      }
+      double pll = orc_gmm_ll_mu(g, prop, k, cov, z);
+      if (pll > log_y) { memcpy(cur, prop, sizeof(double) * d); break; }
+      if (theta < 0) tmin = theta; else tmax = theta;
+      theta = tmin + orc_uniform(&s) * (tmax - tmin);
+      shrinks++;
+    }
+  }
+  free(nu); free(prop);
+  return shrinks;
+}
+
+/* MWG [mu] ~ MvNormal(mu[k], covp) for k <- 0 until K (CgUserProp.hs:131-260)
+ * with the generated correction ll(mu; mu, covp) - ll(mu'; mu, covp) when
+ * compat, else 0 (symmetric walk); substream (k, iter, MWG): d normals then
+ * the accept uniform.  Returns the number of accepts. */
+int orc_gmm_mwg(const orc_gmm* g, double* mu, const double* cov, const int* z, const double* covp,
+                int compat, uint64_t seed, uint32_t iter) {
+  const int d = g->d;
+  double* prop = (double*)malloc(sizeof(double) * d);
+  int acc = 0;
+  for (int k = 0; k < g->K; k++) {
+    double* cur = mu + (size_t)k * d;
+    orc_stream s = orc_make(seed, (uint32_t)k, iter, ORC_TAG_MWG);
+    orc_mvnormal_sample(&s, prop, cur, covp, d);
+    double corr = compat ? orc_mvnormal_ll(cur, cur, covp, d) - orc_mvnormal_ll(prop, cur, covp, d) : 0.0;
+    double cl = orc_gmm_ll_mu(g, cur, k, cov, z);
+    double pl = orc_gmm_ll_mu(g, prop, k, cov, z);
+    double u = orc_uniform(&s);
+    if (log(u) < pl - cl + corr) { memcpy(cur, prop, sizeof(double) * d); acc++; }
+  }
+  free(prop);
+  return acc;
+}
+#undef M_

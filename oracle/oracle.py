@@ -270,3 +270,138 @@ def hlr_synthetic(N, D, seed, vprior="invgamma", has_b=False, x_dtype=np.float64
     t = X.astype(np.float64) @ beta + b
     y = (rng.random(N) < 1.0 / (1.0 + np.exp(-t))).astype(np.int32)
     return X, y, beta, s2
+
+
+# ---- Gaussian mixtures --------------------------------------------------------
+class GmmC(C.Structure):
+    _fields_ = [("N", C.c_int), ("d", C.c_int), ("K", C.c_int), ("shared_cov", C.c_int),
+                ("Y", _dp), ("mu0", _dp), ("cov0", _dp), ("alpha", _dp), ("df", C.c_int),
+                ("scale0", _dp)]
+
+
+class GmmModel:
+    """mvgmm (shared covariance `covs`, fixed weights) when shared_cov, else
+    hmvgmm (weights ~ Dir(alpha), covariances ~ InvWishart(df, scale0))."""
+
+    def __init__(self, Y, K, mu0, cov0, shared_cov, alpha=None, df=0, scale0=None):
+        self.Y = np.ascontiguousarray(Y, np.float64)
+        self.N, self.d = self.Y.shape
+        self.K = int(K)
+        self.mu0 = np.ascontiguousarray(mu0, np.float64)
+        self.cov0 = np.ascontiguousarray(cov0, np.float64)
+        self.shared = int(bool(shared_cov))
+        self.alpha = np.ascontiguousarray(alpha if alpha is not None else np.ones(K), np.float64)
+        self.df = int(df)
+        self.scale0 = np.ascontiguousarray(scale0 if scale0 is not None else np.eye(self.d), np.float64)
+
+    def struct(self):
+        return GmmC(self.N, self.d, self.K, self.shared, dptr(self.Y), dptr(self.mu0), dptr(self.cov0),
+                    dptr(self.alpha), self.df, dptr(self.scale0))
+
+
+def _gmm(o, name, g, restype, types, *args):
+    f = o.fn(name, restype)
+    f.argtypes = [C.POINTER(GmmC)] + types
+    s = g.struct()
+    return f(C.byref(s), *args)
+
+
+_S = [C.c_uint64, C.c_uint32]
+
+
+def gmm_disc_z(o, g, pis, mu, cov, seed, it):
+    z = np.zeros(g.N, np.int32)
+    _gmm(o, "gmm_disc_z", g, None, [_dp, _dp, _dp, _ip] + _S, dptr(np.ascontiguousarray(pis, np.float64)),
+         dptr(np.ascontiguousarray(mu, np.float64)), dptr(np.ascontiguousarray(cov, np.float64)), iptr(z),
+         seed, it)
+    return z
+
+
+def gmm_stats(o, g, z, mu):
+    cnt = np.zeros(g.K, np.int32)
+    s = np.zeros((g.K, g.d))
+    obs = np.zeros((g.K, g.d, g.d))
+    _gmm(o, "gmm_stats", g, None, [_ip, _dp, _ip, _dp, _dp], iptr(np.ascontiguousarray(z, np.int32)),
+         dptr(np.ascontiguousarray(mu, np.float64)), iptr(cnt), dptr(s), dptr(obs))
+    return cnt, s, obs
+
+
+def gmm_sweep(o, g, pis, mu, cov, z, seed, it):
+    """One sweep in place (arrays must be float64 / int32 contiguous)."""
+    _gmm(o, "gmm_sweep", g, None, [_dp, _dp, _dp, _ip] + _S, dptr(pis), dptr(mu), dptr(cov), iptr(z), seed, it)
+
+
+def gmm_conj_pis(o, g, cnt, seed, it):
+    pis = np.zeros(g.K)
+    _gmm(o, "gmm_conj_pis", g, None, [_ip, _dp] + _S, iptr(np.ascontiguousarray(cnt, np.int32)), dptr(pis), seed, it)
+    return pis
+
+
+def gmm_conj_mu(o, g, cnt, s, cov, seed, it):
+    mu = np.zeros((g.K, g.d))
+    s = np.array(s, np.float64, copy=True)
+    _gmm(o, "gmm_conj_mu", g, None, [_ip, _dp, _dp, _dp] + _S, iptr(np.ascontiguousarray(cnt, np.int32)),
+         dptr(s), dptr(np.ascontiguousarray(cov, np.float64)), dptr(mu), seed, it)
+    return mu
+
+
+def gmm_conj_cov(o, g, cnt, obs, seed, it):
+    cov = np.zeros((g.K, g.d, g.d))
+    obs = np.array(obs, np.float64, copy=True)
+    _gmm(o, "gmm_conj_cov", g, None, [_ip, _dp, _dp] + _S, iptr(np.ascontiguousarray(cnt, np.int32)),
+         dptr(obs), dptr(cov), seed, it)
+    return cov
+
+
+def gmm_eslice(o, g, mu, cov, z, seed, it):
+    mu = np.array(mu, np.float64, copy=True)
+    _gmm(o, "gmm_eslice", g, C.c_int if o.kind == "oracle" else None, [_dp, _dp, _ip] + _S, dptr(mu),
+         dptr(np.ascontiguousarray(cov, np.float64)), iptr(np.ascontiguousarray(z, np.int32)), seed, it)
+    return mu
+
+
+def gmm_mwg(o, g, mu, cov, z, covp, seed, it, compat=True):
+    mu = np.array(mu, np.float64, copy=True)
+    covp = np.ascontiguousarray(covp, np.float64)
+    zc = np.ascontiguousarray(z, np.int32)
+    cv = np.ascontiguousarray(cov, np.float64)
+    if o.kind == "ref":
+        _gmm(o, "gmm_mwg", g, None, [_dp, _dp, _ip, _dp] + _S, dptr(mu), dptr(cv), iptr(zc), dptr(covp), seed, it)
+    else:
+        _gmm(o, "gmm_mwg", g, C.c_int, [_dp, _dp, _ip, _dp, C.c_int] + _S, dptr(mu), dptr(cv), iptr(zc),
+             dptr(covp), int(compat), seed, it)
+    return mu
+
+
+def gmm_ll_mu(o, g, muk, k, cov, z):
+    return _gmm(o, "gmm_ll_mu", g, C.c_double, [_dp, C.c_int, _dp, _ip],
+                dptr(np.ascontiguousarray(muk, np.float64)), k, dptr(np.ascontiguousarray(cov, np.float64)),
+                iptr(np.ascontiguousarray(z, np.int32)))
+
+
+def mvnormal_ll(o, pt, mean, cov):
+    f = o.fn("mvnormal_ll", C.c_double)
+    f.argtypes = [_dp, _dp, _dp, C.c_int]
+    return f(dptr(np.ascontiguousarray(pt, np.float64)), dptr(np.ascontiguousarray(mean, np.float64)),
+             dptr(np.ascontiguousarray(cov, np.float64)), len(pt))
+
+
+def gmm_synthetic(N, K, d, seed, mean_scale=5.0, df_extra=2, y_dtype=np.float32):
+    """Config-style mixture data: means ~ N(0, mean_scale^2 I), covariances ~
+    Wishart(d + df_extra, I), weights ~ Dirichlet(1); y stored as float32
+    (values exactly representable in binary64)."""
+    rng = np.random.default_rng(seed)
+    mus = rng.standard_normal((K, d)) * mean_scale
+    covs = []
+    for _ in range(K):
+        A = rng.standard_normal((d + df_extra, d))
+        covs.append(A.T @ A / (d + df_extra))
+    pis = rng.dirichlet(np.ones(K))
+    z = rng.choice(K, size=N, p=pis)
+    Y = np.empty((N, d))
+    for k in range(K):
+        m = z == k
+        if m.any():
+            Lc = np.linalg.cholesky(covs[k])
+            Y[m] = mus[k] + rng.standard_normal((m.sum(), d)) @ Lc.T
+    return Y.astype(y_dtype).astype(np.float64), z.astype(np.int32), mus, np.array(covs), pis

@@ -407,3 +407,241 @@ int ref_hlr_mwg(int N, int D, int has_b, int vprior, double lam, double a0, doub
   free(prop);
   return par[which] != before;
 }
+
+/* ------------------------------------------------------------------------
+ * Gaussian mixtures (compiler/augur/test/mvgmm.rv, hmvgmm.rv): the generated
+ * disc_z, conj_stat_/conj_samp_ for pis / mu / cov, eslice_mu and mwg_mu
+ * restated over the reference's matrix and distribution library.
+ * --------------------------------------------------------------------- */
+typedef struct {
+  int N, d, K, shared_cov;
+  const double* Y;
+  const double* mu0;
+  const double* cov0;
+  const double* alpha;
+  int df;
+  const double* scale0;
+} ref_gmm_t;
+
+static AugurMat_t dmat(double* p, int d) {
+  AugurMat_t m;
+  m.ty = AUGUR_DBL; m.row = (uint_t)d; m.col = (uint_t)d; m.data = p;
+  return m;
+}
+
+void ref_gmm_disc_z(const ref_gmm_t* g, const double* pis, const double* mu, const double* cov, int* z,
+                    uint64_t seed, uint32_t iter) {
+  const int d = g->d, K = g->K;
+  gsl_rng* rng = ref_rng(seed);
+  double* pmf = (double*)malloc(sizeof(double) * K);
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* wb = (double*)malloc(sizeof(double) * d);
+  AugurVec_t vpmf = dvec(pmf, K), vpis = dvec((double*)pis, K), w = dvec(wb, d);
+  AugurMat_t L = dmat(Lb, d);
+  for (int n = 0; n < g->N; n++) {
+    AugurVec_t y = dvec((double*)g->Y + (size_t)n * d, d);
+    for (int k = 0; k < K; k++) {
+      AugurVec_t mk = dvec((double*)mu + (size_t)k * d, d);
+      AugurMat_t ck = dmat((double*)(g->shared_cov ? cov : cov + (size_t)k * d * d), d);
+      double prob = 1.0;
+      prob *= augur_categorical_pdf(k, &vpis);
+      prob *= augur_mvnormal_pdf(&y, &mk, &ck, &L, &w);
+      pmf[k] = prob;
+    }
+    orc_shim_seek(rng, (uint32_t)n, iter, ORC_TAG_Z);
+    z[n] = augur_unnorm_disc_samp(rng, &vpmf);
+  }
+  free(pmf); free(Lb); free(wb);
+}
+
+/* conj_stat_* (CgConj.hs:186-246): counts, sum of y (augur_vec_atm_plus),
+ * sum of (y - mu[z])(y - mu[z])^T (augur_vec_minus + augur_mat_atm_inc_vtmt). */
+void ref_gmm_stats(const ref_gmm_t* g, const int* z, const double* mu, int* cnt, double* sum, double* obs) {
+  const int d = g->d, K = g->K;
+  memset(cnt, 0, sizeof(int) * K);
+  if (sum) memset(sum, 0, sizeof(double) * K * d);
+  if (obs) memset(obs, 0, sizeof(double) * K * d * d);
+  double* db = (double*)malloc(sizeof(double) * d);
+  AugurVec_t diff = dvec(db, d);
+  for (int n = 0; n < g->N; n++) {
+    const int k = z[n];
+    AugurVec_t y = dvec((double*)g->Y + (size_t)n * d, d);
+    AUGUR_ATMINCI(cnt + k, 1);
+    if (sum) { AugurVec_t sk = dvec(sum + (size_t)k * d, d); augur_vec_atm_plus(&sk, &y); }
+    if (obs) {
+      AugurVec_t mk = dvec((double*)mu + (size_t)k * d, d);
+      augur_vec_minus(&diff, &y, &mk);
+      AugurMat_t ok = dmat(obs + (size_t)k * d * d, d);
+      augur_mat_atm_inc_vtmt(&ok, &diff);
+    }
+  }
+  free(db);
+}
+
+void ref_gmm_conj_pis(const ref_gmm_t* g, const int* cnt, double* pis, uint64_t seed, uint32_t iter) {
+  ref_dirichlet_rows(1, g->K, g->alpha, cnt, pis, seed, iter, ORC_TAG_PI);
+}
+
+void ref_gmm_conj_mu(const ref_gmm_t* g, const int* cnt, double* sum, const double* cov, double* mu,
+                     uint64_t seed, uint32_t iter) {
+  const int d = g->d;
+  gsl_rng* rng = ref_rng(seed);
+  double* L0b = (double*)malloc(sizeof(double) * d * d);
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* w0b = (double*)malloc(sizeof(double) * d);
+  AugurMat_t L0 = dmat(L0b, d), L = dmat(Lb, d);
+  AugurVec_t w0 = dvec(w0b, d);
+  AugurVec_t mu0 = dvec((double*)g->mu0, d);
+  AugurMat_t cov0 = dmat((double*)g->cov0, d);
+  for (int k = 0; k < g->K; k++) {
+    AugurVec_t res = dvec(mu + (size_t)k * d, d);
+    AugurVec_t sk = dvec(sum + (size_t)k * d, d);
+    AugurMat_t ck = dmat((double*)(g->shared_cov ? cov : cov + (size_t)k * d * d), d);
+    orc_shim_seek(rng, (uint32_t)k, iter, ORC_TAG_MU);
+    augur_mvnormal_mvnormal_conj(rng, &res, &mu0, &cov0, &sk, cnt[k], &ck, &L0, &w0, &L);
+  }
+  free(L0b); free(Lb); free(w0b);
+}
+
+void ref_gmm_conj_cov(const ref_gmm_t* g, const int* cnt, double* obs, double* cov, uint64_t seed,
+                      uint32_t iter) {
+  const int d = g->d;
+  gsl_rng* rng = ref_rng(seed);
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* Wb = (double*)malloc(sizeof(double) * d * d);
+  double* db = (double*)malloc(sizeof(double) * d);
+  AugurMat_t L = dmat(Lb, d), W = dmat(Wb, d), sc = dmat((double*)g->scale0, d);
+  AugurVec_t diff = dvec(db, d);
+  for (int k = 0; k < g->K; k++) {
+    AugurMat_t res = dmat(cov + (size_t)k * d * d, d);
+    AugurMat_t ok = dmat(obs + (size_t)k * d * d, d);
+    orc_shim_seek(rng, (uint32_t)k, iter, ORC_TAG_COV);
+    augur_invwishart_mvnormal_conj(rng, &res, g->df, &sc, &ok, cnt[k], &diff, &L, &W);
+  }
+  free(Lb); free(Wb); free(db);
+}
+
+void ref_gmm_sweep(const ref_gmm_t* g, double* pis, double* mu, double* cov, int* z, uint64_t seed,
+                   uint32_t iter) {
+  const int d = g->d, K = g->K;
+  int* cnt = (int*)malloc(sizeof(int) * K);
+  double* sum = (double*)malloc(sizeof(double) * K * d);
+  double* obs = (double*)malloc(sizeof(double) * K * d * d);
+  if (!g->shared_cov) {
+    ref_gmm_stats(g, z, mu, cnt, NULL, NULL);
+    ref_gmm_conj_pis(g, cnt, pis, seed, iter);
+  }
+  ref_gmm_stats(g, z, mu, cnt, sum, NULL);
+  ref_gmm_conj_mu(g, cnt, sum, cov, mu, seed, iter);
+  if (!g->shared_cov) {
+    ref_gmm_stats(g, z, mu, cnt, NULL, obs);
+    ref_gmm_conj_cov(g, cnt, obs, cov, seed, iter);
+  }
+  ref_gmm_disc_z(g, pis, mu, cov, z, seed, iter);
+  free(cnt); free(sum); free(obs);
+}
+
+/* ll_mu(k) (llFnDeclOne): prior of mu[k] then the points of component k. */
+static const ref_gmm_t* g_gmm;
+static const double* g_gmm_cov;
+static const int* g_gmm_z;
+static int g_gmm_k;
+
+static double ref_gmm_ll_mu_fn(AugurAux_t aux, AugurMod_t mod) {
+  const int d = g_gmm->d, k = g_gmm_k;
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* wb = (double*)malloc(sizeof(double) * d);
+  AugurMat_t L = dmat(Lb, d);
+  AugurVec_t w = dvec(wb, d);
+  AugurVec_t muk = *AUGUR_VEC_GETV(mod.mu, k);
+  AugurVec_t mu0 = dvec((double*)g_gmm->mu0, d);
+  AugurMat_t cov0 = dmat((double*)g_gmm->cov0, d);
+  AugurMat_t ck = dmat((double*)(g_gmm->shared_cov ? g_gmm_cov : g_gmm_cov + (size_t)k * d * d), d);
+  double ll = 0.0;
+  ll += augur_mvnormal_ll(&muk, &mu0, &cov0, &L, &w);
+  double s = 0.0;
+  for (int n = 0; n < g_gmm->N; n++)
+    if (g_gmm_z[n] == k) {
+      AugurVec_t y = dvec((double*)g_gmm->Y + (size_t)n * d, d);
+      s += augur_mvnormal_ll(&y, &muk, &ck, &L, &w);
+    }
+  ll += s;
+  free(Lb); free(wb);
+  return ll;
+}
+
+/* eslice_mu (CgESlice.hs:93-144) over augur_mcmc_eslice. */
+void ref_gmm_eslice(const ref_gmm_t* g, double* mu, const double* cov, const int* z, uint64_t seed,
+                    uint32_t iter) {
+  const int d = g->d, K = g->K;
+  gsl_rng* rng = ref_rng(seed);
+  double* prop = (double*)malloc(sizeof(double) * K * d);
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* nub = (double*)malloc(sizeof(double) * d);
+  AugurVec_t* rows_c = (AugurVec_t*)malloc(sizeof(AugurVec_t) * K);
+  AugurVec_t* rows_p = (AugurVec_t*)malloc(sizeof(AugurVec_t) * K);
+  memcpy(prop, mu, sizeof(double) * K * d);
+  for (int k = 0; k < K; k++) { rows_c[k] = dvec(mu + (size_t)k * d, d); rows_p[k] = dvec(prop + (size_t)k * d, d); }
+  AugurVec_t vc, vp;
+  vc.ty = AUGUR_VEC; vc.stride = 0; vc.elems = K; vc.data = rows_c;
+  vp.ty = AUGUR_VEC; vp.stride = 0; vp.elems = K; vp.data = rows_p;
+  AugurVec_t mu0 = dvec((double*)g->mu0, d), nu = dvec(nub, d);
+  AugurMat_t cov0 = dmat((double*)g->cov0, d), L = dmat(Lb, d);
+  g_gmm = g; g_gmm_cov = cov; g_gmm_z = z;
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = rng; curr.mu = &vc; pr.mu = &vp;
+  for (int k = 0; k < K; k++) {
+    g_gmm_k = k;
+    orc_shim_seek(rng, (uint32_t)k, iter, ORC_TAG_ESLICE);
+    augur_mcmc_eslice(aux, curr, pr, rows_c + k, rows_p + k, &mu0, &cov0, &L, &nu, ref_gmm_ll_mu_fn);
+  }
+  free(prop); free(Lb); free(nub); free(rows_c); free(rows_p);
+}
+
+/* mwg_mu with the proposal MvNormal(mu[k], covp) (CgUserProp.hs:131-260). */
+static const double* g_mwg_covp;
+static double g_mwg_corr_mu;
+
+static void ref_gmm_mwg_prop(AugurAux_t aux, AugurMod_t curr, AugurMod_t prop) {
+  const int d = g_gmm->d, k = g_gmm_k;
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* wb = (double*)malloc(sizeof(double) * d);
+  AugurMat_t L = dmat(Lb, d), cp = dmat((double*)g_mwg_covp, d);
+  AugurVec_t w = dvec(wb, d);
+  AugurVec_t* ck = AUGUR_VEC_GETV(curr.mu, k);
+  AugurVec_t* pk = AUGUR_VEC_GETV(prop.mu, k);
+  augur_mvnormal_sample(aux.rng, pk, ck, &cp, &L, &w);
+  g_mwg_corr_mu = augur_mvnormal_ll(ck, ck, &cp, &L, &w) - augur_mvnormal_ll(pk, ck, &cp, &L, &w);
+  free(Lb); free(wb);
+}
+
+static void ref_gmm_mwg_swap(AugurAux_t aux, AugurMod_t curr, AugurMod_t prop, int dir) {
+  const int d = g_gmm->d, k = g_gmm_k;
+  AugurVec_t* ck = AUGUR_VEC_GETV(curr.mu, k);
+  AugurVec_t* pk = AUGUR_VEC_GETV(prop.mu, k);
+  if (dir == 0) memcpy(ck->data, pk->data, sizeof(double) * d);
+  else memcpy(pk->data, ck->data, sizeof(double) * d);
+}
+
+void ref_gmm_mwg(const ref_gmm_t* g, double* mu, const double* cov, const int* z, const double* covp,
+                 uint64_t seed, uint32_t iter) {
+  const int d = g->d, K = g->K;
+  gsl_rng* rng = ref_rng(seed);
+  double* prop = (double*)malloc(sizeof(double) * K * d);
+  AugurVec_t* rows_c = (AugurVec_t*)malloc(sizeof(AugurVec_t) * K);
+  AugurVec_t* rows_p = (AugurVec_t*)malloc(sizeof(AugurVec_t) * K);
+  memcpy(prop, mu, sizeof(double) * K * d);
+  for (int k = 0; k < K; k++) { rows_c[k] = dvec(mu + (size_t)k * d, d); rows_p[k] = dvec(prop + (size_t)k * d, d); }
+  AugurVec_t vc, vp;
+  vc.ty = AUGUR_VEC; vc.stride = 0; vc.elems = K; vc.data = rows_c;
+  vp.ty = AUGUR_VEC; vp.stride = 0; vp.elems = K; vp.data = rows_p;
+  g_gmm = g; g_gmm_cov = cov; g_gmm_z = z; g_mwg_covp = covp;
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = rng; curr.mu = &vc; pr.mu = &vp;
+  for (int k = 0; k < K; k++) {
+    g_gmm_k = k;
+    orc_shim_seek(rng, (uint32_t)k, iter, ORC_TAG_MWG);
+    augur_mcmc_mwg(aux, curr, pr, &g_mwg_corr_mu, ref_gmm_mwg_prop, ref_gmm_mwg_swap, ref_gmm_ll_mu_fn);
+  }
+  free(prop); free(rows_c); free(rows_p);
+}

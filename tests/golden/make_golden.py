@@ -47,6 +47,34 @@ def example_arrays(path, func_name):
     return out
 
 
+def example_values(path, func_name, names):
+    """Values of simple assignments (`mu = [np.array([...]), ...]`,
+    `covs = np.matrix([...])`) inside one function of a reference example."""
+    lines = [ln for ln in open(path).read().splitlines()
+             if not ln.strip().startswith(("print ", "get_ipython"))]
+    tree = ast.parse("\n".join(lines))
+
+    def ev(node):
+        if isinstance(node, ast.Call) and getattr(node.func, "attr", "") in ("array", "matrix"):
+            return np.array(ast.literal_eval(node.args[0]), dtype=np.float64)
+        if isinstance(node, ast.List):
+            return [ev(e) for e in node.elts]
+        return ast.literal_eval(node)
+
+    out = {}
+    for node in ast.walk(tree):
+        if isinstance(node, ast.FunctionDef) and node.name == func_name:
+            for st in ast.walk(node):
+                if isinstance(st, ast.Assign):
+                    for tgt in st.targets:
+                        if isinstance(tgt, ast.Name) and tgt.id in names:
+                            try:
+                                out[tgt.id] = ev(st.value)
+                            except (ValueError, TypeError, AttributeError, IndexError):
+                                pass
+    return out
+
+
 def lda_fixture_d4_k4_v8():
     arrs = example_arrays(os.path.join(REF_ROOT, "examples", "lda.py"), "mk_synthetic_dataset_d4_k4_v8")
     docs = [np.array(arrs[k], np.int32) for k in ("w1", "w2", "w3", "w4")]
@@ -139,10 +167,49 @@ def make_hlr(ref):
         np.savez_compressed(os.path.join(HERE, name + "_golden.npz"), **rec)
 
 
+def make_gmm(ref):
+    """mvgmm with the centres and covariance of the reference's example
+    (examples/mvgmm.py mk_synthetic_dataset_k3_d2; points drawn here with a
+    seed), and an hmvgmm instance of the benchmark's construction."""
+    vals = example_values(os.path.join(REF_ROOT, "examples", "mvgmm.py"), "mk_synthetic_dataset_k3_d2",
+                          {"mu", "covs"})
+    centres, covs = np.array(vals["mu"]), np.array(vals["covs"])
+    K, d, N = centres.shape[0], centres.shape[1], 60
+    rng = np.random.default_rng(60)
+    Lc = np.linalg.cholesky(covs)
+    Y = np.array([centres[n % K] + Lc @ rng.standard_normal(d) for n in range(N)])
+    Y = Y.astype(np.float32).astype(np.float64)
+    mu0, cov0 = np.zeros(d), np.eye(d)
+    pis = np.full(K, 1.0 / K)
+    g = O.GmmModel(Y, K, mu0, cov0, True)
+    mu, z = np.zeros((K, d)), np.zeros(N, np.int32)
+    mus, zs = [], []
+    for it in range(8):
+        O.gmm_sweep(ref, g, pis, mu, covs, z, 1, it)
+        mus.append(mu.copy()); zs.append(z.copy())
+    es = O.gmm_eslice(ref, g, mus[-1], covs, zs[-1], 2, 0)
+    mw = O.gmm_mwg(ref, g, mus[-1], covs, zs[-1], cov0, 2, 0)
+    np.savez_compressed(os.path.join(HERE, "mvgmm_k3_d2.npz"), Y=Y, covs=covs, pis=pis, mu0=mu0, cov0=cov0,
+                        mu=np.array(mus), z=np.array(zs), eslice=es, mwg=mw)
+
+    K, d, N = 4, 5, 400
+    Y, z0, mus_t, covs_t, pis_t = O.gmm_synthetic(N, K, d, seed=7)
+    g = O.GmmModel(Y, K, np.zeros(d), 25 * np.eye(d), False, alpha=np.ones(K), df=d + 2, scale0=np.eye(d))
+    pis, mu, cov, z = pis_t.copy(), mus_t.copy(), covs_t.copy(), z0.copy()
+    rec = dict(Y=Y, mu_init=mus_t, cov_init=covs_t, pis_init=pis_t, z_init=z0)
+    P, M, Cv, Z = [], [], [], []
+    for it in range(4):
+        O.gmm_sweep(ref, g, pis, mu, cov, z, 3, it)
+        P.append(pis.copy()); M.append(mu.copy()); Cv.append(cov.copy()); Z.append(z.copy())
+    rec.update(pis=np.array(P), mu=np.array(M), cov=np.array(Cv), z=np.array(Z))
+    np.savez_compressed(os.path.join(HERE, "hmvgmm_k4_d5.npz"), **rec)
+
+
 if __name__ == "__main__":
     O.build_oracle()
     ref = O.Oracle("ref")
     make_primitives(ref)
     make_lda(ref)
     make_hlr(ref)
+    make_gmm(ref)
     print("golden fixtures written to", HERE)

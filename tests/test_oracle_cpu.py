@@ -175,3 +175,53 @@ def test_hlr_gradient_finite_difference(orc):
         pp[i] += h; pm[i] -= h
         fd = (O.hlr_ll(orc, m, pp, idx) - O.hlr_ll(orc, m, pm, idx)) / (2 * h)
         assert abs(fd - g[j]) <= 1e-5 * max(1.0, abs(g[j]))
+
+
+# ---- Gaussian mixtures ---------------------------------------------------------
+def test_mvgmm_golden_reference_example(orc):
+    g = np.load(os.path.join(GOLD, "mvgmm_k3_d2.npz"))
+    K, d = g["mu"].shape[1:]
+    m = O.GmmModel(g["Y"], K, g["mu0"], g["cov0"], True)
+    mu, z = np.zeros((K, d)), np.zeros(len(g["Y"]), np.int32)
+    pis = g["pis"].copy()
+    for it in range(8):
+        O.gmm_sweep(orc, m, pis, mu, g["covs"].copy(), z, 1, it)
+        np.testing.assert_array_equal(mu, g["mu"][it])
+        np.testing.assert_array_equal(z, g["z"][it])
+    np.testing.assert_array_equal(O.gmm_eslice(orc, m, g["mu"][-1], g["covs"], g["z"][-1], 2, 0), g["eslice"])
+    np.testing.assert_array_equal(O.gmm_mwg(orc, m, g["mu"][-1], g["covs"], g["z"][-1], g["cov0"], 2, 0), g["mwg"])
+
+
+def test_hmvgmm_golden(orc):
+    g = np.load(os.path.join(GOLD, "hmvgmm_k4_d5.npz"))
+    K, d = g["mu_init"].shape
+    m = O.GmmModel(g["Y"], K, np.zeros(d), 25 * np.eye(d), False, alpha=np.ones(K), df=d + 2, scale0=np.eye(d))
+    pis, mu, cov, z = (g["pis_init"].copy(), g["mu_init"].copy(), g["cov_init"].copy(), g["z_init"].copy())
+    for it in range(4):
+        O.gmm_sweep(orc, m, pis, mu, cov, z, 3, it)
+        np.testing.assert_array_equal(pis, g["pis"][it])
+        np.testing.assert_array_equal(mu, g["mu"][it])
+        np.testing.assert_array_equal(cov, g["cov"][it])
+        np.testing.assert_array_equal(z, g["z"][it])
+
+
+def test_gmm_oracle_vs_reference_live(orc, ref):
+    Y, z, mus, covs, pis = O.gmm_synthetic(150, 3, 4, seed=9)
+    m = O.GmmModel(Y, 3, np.zeros(4), 9 * np.eye(4), False, alpha=np.full(3, 2.0), df=7, scale0=2 * np.eye(4))
+    np.testing.assert_array_equal(O.gmm_disc_z(orc, m, pis, mus, covs, 8, 2),
+                                  O.gmm_disc_z(ref, m, pis, mus, covs, 8, 2))
+    for a, b in zip(O.gmm_stats(orc, m, z, mus), O.gmm_stats(ref, m, z, mus)):
+        np.testing.assert_array_equal(a, b)
+    cnt, s, obs = O.gmm_stats(orc, m, z, mus)
+    np.testing.assert_array_equal(O.gmm_conj_mu(orc, m, cnt, s, covs, 8, 2), O.gmm_conj_mu(ref, m, cnt, s, covs, 8, 2))
+    np.testing.assert_array_equal(O.gmm_conj_cov(orc, m, cnt, obs, 8, 2), O.gmm_conj_cov(ref, m, cnt, obs, 8, 2))
+    np.testing.assert_array_equal(O.gmm_eslice(orc, m, mus, covs, z, 8, 2), O.gmm_eslice(ref, m, mus, covs, z, 8, 2))
+
+
+def test_mvnormal_ll_matches_scipy(orc):
+    from scipy.stats import multivariate_normal
+    rng = np.random.default_rng(0)
+    A = rng.standard_normal((6, 6))
+    cov = A @ A.T + 6 * np.eye(6)
+    x, mu = rng.standard_normal(6), rng.standard_normal(6)
+    assert abs(O.mvnormal_ll(orc, x, mu, cov) - multivariate_normal(mu, cov).logpdf(x)) < 1e-10
