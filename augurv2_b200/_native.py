@@ -79,6 +79,17 @@ _SIGS = {
     "ab_hlr_ll_grad": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp]),
     "ab_hlr_chain_scratch_bytes": (sz, [i32, i32]),
     "ab_hlr_run_chains": (i32, [vp, vp, vp, i32, vp, vp, i32, vp, i32, u32, u64, vp, vp, vp]),
+    # GMM
+    "ab_gmm_table_doubles": (sz, [i32, i32]),
+    "ab_gmm_prep": (i32, [i32, i32, vp, vp, vp, vp]),
+    "ab_gmm_disc_z": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_stats_scratch_bytes": (sz, [i32, i32]),
+    "ab_gmm_stats": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "ab_gmm_conj_pis": (i32, [i32, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_conj_mu": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_conj_cov": (i32, [i32, i32, i32, vp, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_eslice": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, u64, u32, u32, vp, vp]),
+    "ab_gmm_mwg": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, i32, i32, vp, u64, u32, u32, vp, vp]),
 }
 
 

@@ -117,7 +117,7 @@ class HlrChains:
         if init is None:
             init = np.zeros((self.C, D + 2))
             init[:, D + 1] = 1.0
-        init = np.broadcast_to(np.asarray(init, np.float64), (self.C, D + 2))
+        init = np.broadcast_to(np.asarray(init, np.float64), (self.C, D + 2)).copy()
         self.pars = torch.as_tensor(np.ascontiguousarray(init)).to(dev)
         self.stats = torch.zeros((self.C, self.ncomp, 4), dtype=torch.float64, device=dev)
         need_nuts = any(c.kind == NUTS for c in comps)

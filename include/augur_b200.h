@@ -170,6 +170,65 @@ int ab_hlr_run_chains(const ab_hlr_model* model, const ab_hlr_comp* comps_host, 
                       int n_iter, uint32_t iter0, uint64_t seed, double* stats, void* scratch,
                       void* stream);
 
+/* ======================================================================= *
+ * Gaussian mixtures (compiler/augur/test/mvgmm.rv: shared covariance, fixed
+ * weights; hmvgmm.rv: weights ~ Dirichlet(alpha), cov[k] ~ InvWishart).
+ * Layouts: Y f32 [N][d]; z int32 [N]; pis f64 [K]; mu f64 [K][d];
+ * cov f64 [Kc][d][d] (Kc = 1 when shared); tables Linv f64 [slots][d][d] and
+ * hdet f64 [slots].  Binary64 throughout; d <= 64, K <= 64.
+ * ======================================================================= */
+
+/* Per-covariance tables of augur_mvnormal_ll (cbits/augur_dist.c:548-568):
+ * Linv = inverse of the lower Cholesky factor, hdet = log(det)/2, for Kc
+ * covariances. */
+size_t ab_gmm_table_doubles(int Kc, int d);
+int ab_gmm_prep(int Kc, int d, const double* cov, double* Linv, double* hdet, void* stream);
+
+/* z[n] ~ p(z | pis, mu, cov): replaces the generated disc_z with pmf_k =
+ * pis[k] * augur_mvnormal_pdf(y_n, mu[k], cov[k]) and augur_unnorm_disc_samp
+ * (CgDisc.hs:122-156); point n draws one uniform from (n, iter, 1|comp<<8). */
+int ab_gmm_disc_z(int N, int d, int K, int shared_cov, const float* Y, const double* pis, const double* mu,
+                  const double* Linv, const double* hdet, int* z, uint64_t seed, uint32_t iter, uint32_t comp,
+                  void* stream);
+
+/* Conjugate statistics of z (CgConj.hs:186-246): counts cnt int32 [K] always;
+ * sum f64 [K][d] of y if `sum` is non-NULL; obs f64 [K][d][d] =
+ * sum (y - mu[z])(y - mu[z])^T if `obs` is non-NULL (needs mu).  scratch:
+ * ab_gmm_stats_scratch_bytes(d, K) bytes (per-block partial tables). */
+size_t ab_gmm_stats_scratch_bytes(int d, int K);
+int ab_gmm_stats(int N, int d, int K, const float* Y, const int* z, const double* mu, int* cnt, double* sum,
+                 double* obs, void* scratch, void* stream);
+
+/* ConjGibbs [pis]: Dirichlet(alpha + cnt) (augur_dirichlet_categorical_conj,
+ * cbits/augur_dist.c:526-538), element k from (k, iter, 7|comp<<8). */
+int ab_gmm_conj_pis(int K, const double* alpha, const int* cnt, double* pis, uint64_t seed, uint32_t iter,
+                    uint32_t comp, void* stream);
+
+/* ConjGibbs [mu]: augur_mvnormal_mvnormal_conj (cbits/augur_dist.c:633-669)
+ * per component with covariance cov[shared ? 0 : k]; (k, iter, 8|comp<<8). */
+int ab_gmm_conj_mu(int K, int d, int shared_cov, const double* mu0, const double* cov0, const int* cnt,
+                   const double* sum, const double* cov, double* mu, uint64_t seed, uint32_t iter, uint32_t comp,
+                   void* stream);
+
+/* ConjGibbs [cov]: augur_invwishart_mvnormal_conj (cbits/augur_dist.c:751-757,
+ * InvWishart(cnt + df, obs + scale0) by Bartlett); (k, iter, 9|comp<<8). */
+int ab_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs, double* cov,
+                    uint64_t seed, uint32_t iter, uint32_t comp, void* stream);
+
+/* ESlice [mu]: augur_mcmc_eslice (cbits/augur_mcmclib.h:439-485) for every
+ * component (one thread block each) over the full conditional of mu[k]
+ * (prior table in slot prior_slot); (k, iter, 10|comp<<8).  shrinks int32[K]. */
+int ab_gmm_eslice(int N, int d, int K, int shared_cov, const float* Y, const int* z, const double* mu0,
+                  const double* cov0, const double* Linv, const double* hdet, int prior_slot, double* mu,
+                  uint64_t seed, uint32_t iter, uint32_t comp, int* shrinks, void* stream);
+
+/* MWG [mu] ~ MvNormal(mu[k], covp) (augur_mcmc_mwg, cbits/augur_mcmclib.h:
+ * 178-193, generated prop_/swap_ of CgUserProp.hs:131-210); compat uses the
+ * generated log-correction.  (k, iter, 11|comp<<8).  accepts int32[K] += . */
+int ab_gmm_mwg(int N, int d, int K, int shared_cov, const float* Y, const int* z, const double* mu0,
+               const double* covp, const double* Linv, const double* hdet, int prior_slot, int prop_slot,
+               int compat, double* mu, uint64_t seed, uint32_t iter, uint32_t comp, int* accepts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
