@@ -69,6 +69,7 @@ _SIGS = {
     "ab_lda_conj_theta": (i32, [i32, i32, vp, vp, vp, u64, u32, vp]),
     "ab_lda_phi_scratch_bytes": (sz, [i32, i32]),
     "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp, vp]),
+    "ab_lda_conj_phi_noalloc": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp]),
     "ab_lda_disc_z": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
     "ab_lda_scratch_bytes": (sz, [i32, i32]),
     "ab_lda_create": (i32, [C.POINTER(LdaDesc), C.POINTER(vp)]),

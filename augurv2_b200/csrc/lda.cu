@@ -30,6 +30,8 @@
 // (_rn intrinsics; this file is also compiled with -fmad=false), so given the
 // same theta, phi and Philox uniforms the assignments and counts equal the
 // reference's CPU sampler's bit for bit.
+#include <mutex>
+
 #include "common.cuh"
 #include "dist.cuh"
 
@@ -492,6 +494,52 @@ extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int*
              "ab_lda_disc_z: pass both count tables or neither");
   return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, nullptr,
                       iter, nullptr, as_stream(stream));
+}
+
+// ---- variant of ab_lda_conj_phi that allocates nothing ----------------------
+// Some callers cannot call cudaMalloc: a host framework that owns all device
+// memory through its own pool and cannot hand out a raw scratch buffer, or a
+// plugin that must not allocate while it runs.  For them the phi draw takes
+// its scratch (per-CTA partial sums, per-topic normalisers and completion
+// tickets) from this file-scope device array instead of a caller buffer.
+// Every GPU that loads the library holds the array until the process exits.
+constexpr size_t LDA_NOALLOC_SCRATCH_BYTES = 1u << 20;   // 1 MiB
+static __device__ __align__(256) unsigned char g_lda_phi_scratch[LDA_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {nullptr};   // device address of the array, per device ordinal
+}  // namespace
+
+extern "C" int ab_lda_conj_phi_noalloc(int K, int V, const double* beta, int* cnt_kw, double* phiT,
+                                       int clear_counts, uint64_t seed, uint32_t iter, void* stream) {
+  int rc = check_lda_dims(1, K, V);
+  if (rc) return rc;
+  AB_REQUIRE(beta && cnt_kw && phiT, AB_ERR_ARG, "ab_lda_conj_phi_noalloc: null pointer");
+  const size_t need = lda_phi_scratch(K, V);
+  AB_REQUIRE(need <= LDA_NOALLOC_SCRATCH_BYTES, AB_ERR_ARG,
+             "ab_lda_conj_phi_noalloc: K=%d, V=%d need %zu bytes of scratch, above the built-in %zu; "
+             "use ab_lda_conj_phi with a caller buffer",
+             K, V, need, (size_t)LDA_NOALLOC_SCRATCH_BYTES);
+  int dev = 0;
+  AB_CUDA(cudaGetDevice(&dev));
+  AB_REQUIRE(dev >= 0 && dev < 64, AB_ERR_ARG, "ab_lda_conj_phi_noalloc: device ordinal %d >= 64", dev);
+  void* scratch = nullptr;
+  {
+    // First call on a device: look up the device address of the array (the
+    // host-side name is only a stand-in and must never reach a kernel).
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+      void* p = nullptr;
+      AB_CUDA(cudaGetSymbolAddress(&p, g_lda_phi_scratch));
+      g_noalloc_ptr[dev] = p;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  cudaStream_t st = as_stream(stream);
+  // the completion tickets must start at zero
+  AB_CUDA(cudaMemsetAsync(static_cast<char*>(scratch) + 256, 0, 4 * (size_t)K, st));
+  return launch_lda_phi(K, V, lda_kp(K), beta, cnt_kw, phiT, clear_counts, scratch, seed, nullptr, iter, st);
 }
 
 // ---- sweep runner with a captured CUDA graph -------------------------------

@@ -81,6 +81,21 @@ size_t ab_lda_phi_scratch_bytes(int K, int V);
 int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
                     int clear_counts, uint64_t seed, uint32_t iter, void* scratch, void* stream);
 
+/* Same draw as ab_lda_conj_phi for callers that cannot allocate device
+ * memory (a host framework that owns all device memory through its own pool,
+ * or a plugin that must not allocate while it runs).  This entry point has no
+ * counterpart in the reference.  It calls no cudaMalloc / cudaFree: its
+ * scratch is a 1 MiB array inside the library that every GPU loading the
+ * library keeps until the process exits, so it accepts only K, V with
+ * ab_lda_phi_scratch_bytes(K, V) <= 1 MiB (K = 50, V = 10,000 needs 17 KB)
+ * and rejects larger sizes with AB_ERR_ARG.  The first call on a device looks
+ * up the array's device address; make that first call before any stream
+ * capture.  All calls share the array: calls whose work overlaps on the GPU
+ * (other streams, other threads) race and must be serialised by the
+ * caller. */
+int ab_lda_conj_phi_noalloc(int K, int V, const double* beta, int* cnt_kw, double* phiT,
+                            int clear_counts, uint64_t seed, uint32_t iter, void* stream);
+
 /* z[t] ~ p(z | theta, phi) for every token: replaces the generated disc_z
  * (CgDisc.hs:122-156) over augur_unnorm_disc_samp (cbits/augur_dist.c:
  * 798-813); token t draws one uniform from substream (t, iter, 1).  If the
