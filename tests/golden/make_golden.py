@@ -205,7 +205,35 @@ def make_gmm(ref):
     np.savez_compressed(os.path.join(HERE, "hmvgmm_k4_d5.npz"), **rec)
 
 
+def make_models():
+    """The reference's model files (compiler/augur/test/*.rv) and the model
+    strings and schedules of its examples, as parser fixtures."""
+    import json
+    out = {"rv": {}, "examples": {}}
+    tdir = os.path.join(REF_ROOT, "compiler", "augur", "test")
+    for f in sorted(os.listdir(tdir)):
+        if f.endswith(".rv"):
+            out["rv"][f[:-3]] = open(os.path.join(tdir, f)).read()
+    for ex in ("hlr", "lda", "mvgmm"):
+        lines = [ln for ln in open(os.path.join(REF_ROOT, "examples", ex + ".py")).read().splitlines()
+                 if not ln.strip().startswith(("print ", "get_ipython"))]
+        tree = ast.parse("\n".join(lines))
+        rec = {"scheds": []}
+        for node in tree.body:
+            if isinstance(node, ast.Assign) and isinstance(node.targets[0], ast.Name) \
+                    and isinstance(node.value, ast.Constant) and isinstance(node.value.value, str):
+                name = node.targets[0].id
+                if name.startswith("augur_"):
+                    rec["model"] = node.value.value
+                elif name.startswith("sched"):
+                    rec["scheds"].append(node.value.value)
+        out["examples"][ex] = rec
+    with open(os.path.join(HERE, "models.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
+    make_models()
     O.build_oracle()
     ref = O.Oracle("ref")
     make_primitives(ref)
