@@ -80,6 +80,8 @@ _SIGS = {
     "ab_hlr_ll_grad": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp]),
     "ab_hlr_chain_scratch_bytes": (sz, [i32, i32]),
     "ab_hlr_run_chains": (i32, [vp, vp, vp, i32, vp, vp, i32, vp, i32, u32, u64, vp, vp, vp]),
+    # tensor-core GEMM core
+    "ab_tc_gemm_bf16": (i32, [i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp, vp]),
     # GMM
     "ab_gmm_table_doubles": (sz, [i32, i32]),
     "ab_gmm_prep": (i32, [i32, i32, vp, vp, vp, vp]),

@@ -1,0 +1,93 @@
+// Host side of the tensor-core GEMM core: tensor maps, launch helpers, and a
+// plain "store" epilogue exposed through the C ABI for checking the core
+// against a reference matrix product.
+#include <cudaTypedefs.h>
+#include <mutex>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+#include "tc_host.cuh"
+
+namespace ab {
+namespace tc {
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::mutex g_encode_mu;
+}  // namespace
+
+int encode_2d_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t cols, uint64_t ld_elems,
+                   uint32_t box_rows) {
+  {
+    std::lock_guard<std::mutex> lk(g_encode_mu);
+    if (!g_encode) {
+      cudaDriverEntryPointQueryResult q;
+      void* fn = nullptr;
+      AB_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q));
+      AB_REQUIRE(fn && q == cudaDriverEntryPointSuccess, AB_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+  }
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(ptr) & 15) == 0, AB_ERR_ARG, "tensor base must be 16-byte aligned");
+  AB_REQUIRE((ld_elems * 2) % 16 == 0, AB_ERR_ARG, "row stride must be a multiple of 16 bytes");
+  AB_REQUIRE(box_rows >= 1 && box_rows <= 256, AB_ERR_ARG, "box rows must be 1..256");
+  cuuint64_t dims[2] = {cols, rows};
+  cuuint64_t strides[1] = {ld_elems * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  AB_REQUIRE(r == CUDA_SUCCESS, AB_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return AB_OK;
+}
+
+// C (fp32, ldc) = A B^T, optionally split-K with atomic accumulation.
+struct StoreEpi {
+  static constexpr int kSmem = 0;
+  float* C;
+  int M, N, ldc;
+  int atomic;
+  __device__ void begin(int, int, int, char*) {}
+  __device__ void rows(int row, int col0, const float* v, bool ok) {
+    if (!ok) return;
+    float* out = C + (size_t)row * ldc;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int c = col0 + i;
+      if (c < N) {
+        if (atomic) atomicAdd(out + c, v[i]);
+        else out[c] = v[i];
+      }
+    }
+  }
+  __device__ void end(int, int, int) {}
+};
+
+}  // namespace tc
+}  // namespace ab
+
+using namespace ab;
+using namespace ab::tc;
+
+extern "C" int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C,
+                               int ldc, int splits, int* err, void* stream) {
+  AB_REQUIRE(M > 0 && N > 0 && K > 0 && splits >= 1, AB_ERR_ARG, "ab_tc_gemm_bf16: bad sizes");
+  AB_REQUIRE(A && B && C, AB_ERR_ARG, "ab_tc_gemm_bf16: null pointer");
+  AB_REQUIRE(lda >= K && ldb >= K && ldc >= N, AB_ERR_ARG, "ab_tc_gemm_bf16: leading dimension too small");
+  CUtensorMap ta, tb;
+  int rc = encode_2d_bf16(&ta, A, M, K, lda, BM);
+  if (rc) return rc;
+  const int BN = N >= 256 ? 256 : (N > 64 ? 128 : 64);
+  rc = encode_2d_bf16(&tb, B, N, K, ldb, BN);
+  if (rc) return rc;
+  StoreEpi epi{C, M, N, ldc, splits > 1};
+  const int ksplit = ((K + splits - 1) / splits + BK - 1) / BK * BK;
+  dim3 grid(ceil_div(M, BM), ceil_div(N, BN), splits);
+  cudaStream_t st = as_stream(stream);
+  if (splits > 1) AB_CUDA(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, st));
+  if (BN == 256) rc = launch_gemm<256>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
+  else if (BN == 128) rc = launch_gemm<128>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
+  else rc = launch_gemm<64>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
+  return rc;
+}

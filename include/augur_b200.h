@@ -244,6 +244,18 @@ int ab_gmm_mwg(int N, int d, int K, int shared_cov, const float* Y, const int* z
                const double* covp, const double* Linv, const double* hdet, int prior_slot, int prop_slot,
                int compat, double* mu, uint64_t seed, uint32_t iter, uint32_t comp, int* accepts, void* stream);
 
+/* ======================================================================= *
+ * Tensor-core building block (no counterpart in the reference, whose kernels
+ * are scalar FP64): C[M][N] (f32, ldc) = A[M][K] * B[N][K]^T with A, B
+ * row-major bf16, through tcgen05 MMAs fed by TMA.  splits > 1 splits K and
+ * accumulates atomically.  *err (device int, may be NULL) receives
+ * AB_ERR_TIMEOUT if a bounded wait inside the kernel expired.  Used by the
+ * batched HLR data passes and the gradient surrogate, and exported for
+ * checking the core on its own.
+ * ======================================================================= */
+int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
+                    int splits, int* err, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
