@@ -80,6 +80,24 @@ _SIGS = {
     "ab_hlr_ll_grad": (i32, [vp, vp, vp, i32, i32, vp, vp, vp, vp]),
     "ab_hlr_chain_scratch_bytes": (sz, [i32, i32]),
     "ab_hlr_run_chains": (i32, [vp, vp, vp, i32, vp, vp, i32, vp, i32, u32, u64, vp, vp, vp]),
+    # batched HLR, batched HMC, surrogate MLP
+    "ab_hlrb_xt_elems": (sz, [i32, i32]),
+    "ab_hlrb_transpose": (i32, [i32, i32, vp, i32, vp, vp]),
+    "ab_hlrb_workspace_bytes": (sz, [i32, i32, i32]),
+    "ab_hlrb_logp_grad": (i32, [vp, i32, vp, i32, vp, vp, i32, vp, vp, vp]),
+    "ab_hmcb_begin": (i32, [vp, vp]),
+    "ab_hmcb_step": (i32, [vp, vp, vp]),
+    "ab_hmcb_final": (i32, [vp, vp, vp, vp]),
+    "ab_mlp_param_count": (sz, [i32, i32, i32, i32]),
+    "ab_mlp_act_floats": (sz, [i32, i32, i32]),
+    "ab_mlp_backward_scratch_floats": (sz, [i32, i32, i32]),
+    "ab_mlp_forward": (i32, [vp, i32, vp, i32, vp, i32, vp, vp]),
+    "ab_mlp_mse": (i32, [i32, i32, vp, i32, vp, i32, vp, vp, vp]),
+    "ab_mlp_backward": (i32, [vp, i32, vp, i32, vp, vp, vp, vp, vp]),
+    "ab_mlp_adam": (i32, [vp, vp, vp, vp, i32, f32, f32, f32, f32, vp]),
+    "ab_mlp_sync_bf16": (i32, [vp, vp]),
+    "ab_sur_pre": (i32, [i32, i32, vp, vp, vp, vp, vp]),
+    "ab_sur_post": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
     # tensor-core GEMM core
     "ab_tc_gemm_bf16": (i32, [i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp, vp]),
     # GMM

@@ -1,0 +1,335 @@
+// Batched HLR log density and gradient on the tensor cores: C chains against
+// one data set, each chain's FP32 parameter vector theta[c][0..D-1].
+//
+//   logp(theta) = sum_n [ y_n t_n - softplus(t_n) ] + sum_d log prior(theta_d),
+//   t = X theta,   grad = X^T (y - sigmoid(t)) + d/dtheta log prior
+//
+// which is the reference's generated ll/grad pair for the HLR model
+// (compiler/augur/src/Comm/CgLike.hs:139-147 over augur_bernoulli_ll,
+// augur_dist.c:59-66, and CgGrad.hs:345-376 with augur_bernoulli_dotarg1 x
+// augur_expit_grad_0, augur_dist.c:68-71, augur_math.c:56-59) evaluated for
+// all chains at once:
+//
+//   forward  T^T[C x N] = Theta3[C x 3D] . X[N x D]^T   (theta split hi+mid+lo
+//            into bf16, so the FP32 product is exact to FP32 rounding); the
+//            epilogue turns each t into its log-likelihood term (summed per
+//            chain and 256-row tile, Kahan-compensated) and the residual
+//            r = y - sigmoid(t), stored as three bf16 parts R3[C][3][Np];
+//   backward G[C x D] = R3[C x 3Np] . Xt[D x Np]^T, split over rows into
+//            deterministic FP32 partial tiles;
+//   finish   one block per chain: FP64 sums of the per-tile log-likelihood
+//            partials and of the gradient partials in a fixed order, plus
+//            the FP64 prior and its gradient.
+// X is bf16 [N][ldx]; Xt is its transpose [D][Np] with Np = N rounded up to
+// 64 and zero padding, built once by ab_hlrb_transpose.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+#include "tc_host.cuh"
+
+namespace ab {
+namespace {
+
+constexpr int FWD_BN = 128;   // data rows per forward tile
+constexpr int BWD_BN = 128;   // gradient columns per backward tile
+
+inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+inline size_t align256(size_t a) { return (a + 255) & ~size_t(255); }
+
+struct Layout {
+  int Np, Dp, fwd_tiles, splits, ldw;
+  size_t off_t3, off_r3, off_ll, off_w, total;
+};
+
+Layout layout(int N, int D, int C) {
+  Layout L;
+  L.Np = round_up(N, 64);
+  L.Dp = round_up(D, 64);
+  L.fwd_tiles = (N + FWD_BN - 1) / FWD_BN;
+  const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + BWD_BN - 1) / BWD_BN);
+  const int kb = L.Np / tc::BK;
+  int sp = tc::sm_count() / tiles;
+  if (sp < 1) sp = 1;
+  if (sp > kb) sp = kb;
+  // the kernel's own split arithmetic (whole K steps per split)
+  const int per = (kb + sp - 1) / sp;
+  L.splits = (kb + per - 1) / per;
+  L.ldw = round_up(D, 32);
+  size_t o = 0;
+  L.off_t3 = o;
+  o = align256(o + (size_t)C * 3 * L.Dp * 2);
+  L.off_r3 = o;
+  o = align256(o + (size_t)C * 3 * L.Np * 2);
+  L.off_ll = o;
+  o = align256(o + (size_t)L.fwd_tiles * C * 4);
+  L.off_w = o;
+  o = align256(o + (size_t)L.splits * C * L.ldw * 4);
+  L.total = o;
+  return L;
+}
+
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+  h = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h);   // exact in FP32
+  m = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(m);  // exact in FP32
+  l = __float2bfloat16_rn(r2);
+}
+
+// theta [C][ldt] f32 -> Theta3 [C][3][Dp] bf16 (hi, mid, lo; zero padding).
+__global__ void hlrb_split_kernel(int C, int D, int Dp, const float* __restrict__ theta, int ldt,
+                                  __nv_bfloat16* __restrict__ t3) {
+  const int c = blockIdx.y;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < Dp; d += gridDim.x * blockDim.x) {
+    __nv_bfloat16 h, m, l;
+    if (d < D) {
+      split3(theta[(size_t)c * ldt + d], h, m, l);
+    } else {
+      h = m = l = __float2bfloat16_rn(0.0f);
+    }
+    __nv_bfloat16* row = t3 + (size_t)c * 3 * Dp;
+    row[d] = h;
+    row[Dp + d] = m;
+    row[2 * Dp + d] = l;
+  }
+}
+
+// X [N][ldx] -> Xt [D][Np], zero for n >= N.  32x32 tiles through shared memory.
+__global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16* __restrict__ X, int ldx,
+                                      __nv_bfloat16* __restrict__ Xt) {
+  __shared__ __nv_bfloat16 tile[32][33];
+  const int n0 = blockIdx.x * 32, d0 = blockIdx.y * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;   // 32 x 8
+  for (int j = ty; j < 32; j += 8) {
+    const int n = n0 + j, d = d0 + tx;
+    tile[j][tx] = (n < N && d < D) ? X[(size_t)n * ldx + d] : __float2bfloat16_rn(0.0f);
+  }
+  __syncthreads();
+  for (int j = ty; j < 32; j += 8) {
+    const int d = d0 + j, n = n0 + tx;
+    if (d < D && n < Np) Xt[(size_t)d * Np + n] = tile[tx][j];
+  }
+}
+
+// Forward epilogue: rows are chains, columns are data rows.
+struct FwdEpi {
+  static constexpr int kSmem = FWD_BN * 4;
+  const int* y;
+  __nv_bfloat16* r3;   // NULL: log density only
+  float* llpart;       // [fwd_tiles][C]
+  int N, Np, C;
+  // per-thread state
+  const int* ys;
+  int n0;
+  float acc, comp;
+
+  __device__ void begin(int, int nt, int, char* smem, int etid) {
+    int* s = reinterpret_cast<int*>(smem);
+    n0 = nt * FWD_BN;
+    for (int j = etid; j < FWD_BN; j += 128) {
+      const int n = n0 + j;
+      s[j] = n < N ? y[n] : -1;
+    }
+    ys = s;
+    acc = 0.0f;
+    comp = 0.0f;
+  }
+
+  __device__ void rows(int c, int col0, const float* v, bool ok) {
+    if (!ok) return;
+    float rv[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      const int yv = ys[col0 - n0 + i];
+      const float t = v[i];
+      float term = 0.0f, r = 0.0f;
+      if (yv >= 0) {
+        const float e = expf(-fabsf(t));
+        const float sp = fmaxf(t, 0.0f) + log1pf(e);   // softplus(t)
+        term = yv ? t - sp : -sp;
+        const float inv = __frcp_rn(1.0f + e);
+        const float sig = t >= 0.0f ? inv : e * inv;
+        r = (float)yv - sig;
+        // Kahan-compensated running sum of this chain's terms
+        const float yk = term - comp;
+        const float tk = acc + yk;
+        comp = (tk - acc) - yk;
+        acc = tk;
+      }
+      rv[i] = r;
+    }
+    if (r3 && col0 < Np) {
+      __nv_bfloat16* base = r3 + (size_t)c * 3 * Np + col0;
+      uint32_t ph[16], pm[16], pl[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        __nv_bfloat16 h0, m0, l0, h1, m1, l1;
+        split3(rv[2 * i], h0, m0, l0);
+        split3(rv[2 * i + 1], h1, m1, l1);
+        ph[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        pm[i] = (uint32_t)__bfloat16_as_ushort(m0) | ((uint32_t)__bfloat16_as_ushort(m1) << 16);
+        pl[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+      }
+      uint4* dh = reinterpret_cast<uint4*>(base);
+      uint4* dm = reinterpret_cast<uint4*>(base + Np);
+      uint4* dl = reinterpret_cast<uint4*>(base + 2 * (size_t)Np);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        dh[i] = make_uint4(ph[4 * i], ph[4 * i + 1], ph[4 * i + 2], ph[4 * i + 3]);
+        dm[i] = make_uint4(pm[4 * i], pm[4 * i + 1], pm[4 * i + 2], pm[4 * i + 3]);
+        dl[i] = make_uint4(pl[4 * i], pl[4 * i + 1], pl[4 * i + 2], pl[4 * i + 3]);
+      }
+    }
+  }
+
+  __device__ void end(int, int nt, int, int c, bool ok) {
+    if (ok) llpart[(size_t)nt * C + c] = acc;
+  }
+};
+
+// Backward epilogue: rows are chains, columns are features; one FP32 partial
+// tile per split.
+struct GradEpi {
+  static constexpr int kSmem = 0;
+  float* w;   // [splits][C][ldw]
+  int C, D, ldw;
+  int sp;
+  __device__ void begin(int, int, int split, char*, int) { sp = split; }
+  __device__ void rows(int c, int col0, const float* v, bool ok) {
+    if (!ok || col0 >= D) return;
+    float* out = w + ((size_t)sp * C + c) * ldw + col0;
+    if (col0 + 32 <= ldw) {
+      float4* o4 = reinterpret_cast<float4*>(out);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) o4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    }
+  }
+  __device__ void end(int, int, int, int, bool) {}
+};
+
+__device__ __forceinline__ void prior_term(int kind, double a, double b, double x, double& ll, double& g) {
+  if (kind == AB_PRIOR_NORMAL) {
+    // Normal(0, a): log density and derivative
+    ll = -0.5 * log(2.0 * M_PI * a) - 0.5 * x * x / a;
+    g = -x / a;
+  } else {
+    // Student-t(nu = a, scale = b)
+    const double nu = a, z = x / b;
+    ll = lgamma(0.5 * (nu + 1.0)) - lgamma(0.5 * nu) - 0.5 * log(nu * M_PI) - log(b) -
+         0.5 * (nu + 1.0) * log1p(z * z / nu);
+    g = -(nu + 1.0) * x / (nu * b * b + x * x);
+  }
+}
+
+// One block per chain: logp[c] (FP64) and grad[c][0..D-1] (FP32) from the
+// partials, in a fixed order.
+__global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_tiles, int splits, int ldw,
+                                                          const float* __restrict__ llpart,
+                                                          const float* __restrict__ w, const float* __restrict__ theta,
+                                                          int ldt, int prior, double pa, double pb,
+                                                          double* __restrict__ logp, float* __restrict__ grad,
+                                                          int ldg) {
+  __shared__ double red[33];
+  const int c = blockIdx.x;
+  double s = 0.0;
+  for (int t = threadIdx.x; t < fwd_tiles; t += blockDim.x) s += (double)llpart[(size_t)t * C + c];
+  for (int d = threadIdx.x; d < D; d += blockDim.x) {
+    double pl, pg;
+    prior_term(prior, pa, pb, (double)theta[(size_t)c * ldt + d], pl, pg);
+    s += pl;
+    if (grad) {
+      double g = pg;
+      for (int k = 0; k < splits; ++k) g += (double)w[((size_t)k * C + c) * ldw + d];
+      grad[(size_t)c * ldg + d] = (float)g;
+    }
+  }
+  s = block_sum_f64(s, red);
+  if (threadIdx.x == 0) logp[c] = s;
+}
+
+}  // namespace
+
+int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad, int ldg,
+                   void* work, int* err, cudaStream_t st) {
+  const int N = m->N, D = m->D;
+  const Layout L = layout(N, D, C);
+  char* wb = static_cast<char*>(work);
+  __nv_bfloat16* t3 = reinterpret_cast<__nv_bfloat16*>(wb + L.off_t3);
+  __nv_bfloat16* r3 = reinterpret_cast<__nv_bfloat16*>(wb + L.off_r3);
+  float* llp = reinterpret_cast<float*>(wb + L.off_ll);
+  float* w = reinterpret_cast<float*>(wb + L.off_w);
+
+  hlrb_split_kernel<<<dim3(ceil_div(L.Dp, 256), C), 256, 0, st>>>(C, D, L.Dp, theta, ldt, t3);
+  AB_LAUNCH_CHECK("hlrb_split_kernel");
+
+  int rc;
+  CUtensorMap ma, mb;
+  if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
+  if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
+  FwdEpi fe{m->y, grad ? r3 : nullptr, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
+  const tc::Shape fs = tc::make_shape(C, N, D, 1, L.Dp, 0, FWD_BN);
+  if ((rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st))) return rc;
+
+  if (grad) {
+    if ((rc = tc::encode_2d_bf16(&ma, r3, C, 3 * L.Np, 3 * L.Np, tc::BM))) return rc;
+    if ((rc = tc::encode_2d_bf16(&mb, m->Xt, D, L.Np, L.Np, BWD_BN))) return rc;
+    GradEpi ge{w, C, D, L.ldw, 0};
+    const tc::Shape bs = tc::make_shape(C, D, N, L.splits, L.Np, 0, BWD_BN);
+    AB_REQUIRE(bs.splits == L.splits, AB_ERR_STATE, "hlrb: split arithmetic mismatch");
+    if ((rc = tc::launch_gemm<BWD_BN, 3, 1>(ma, mb, bs, ge, err, st))) return rc;
+  }
+  hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
+                                        m->prior_a, m->prior_b, logp, grad, ldg);
+  AB_LAUNCH_CHECK("hlrb_finish_kernel");
+  return AB_OK;
+}
+
+int hlrb_check_model(const ab_hlrb_model* m) {
+  AB_REQUIRE(m, AB_ERR_ARG, "hlrb: null model");
+  AB_REQUIRE(m->N > 0 && m->D > 0 && m->D <= 65536, AB_ERR_ARG, "hlrb: bad sizes N=%d D=%d", m->N, m->D);
+  AB_REQUIRE(m->X && m->Xt && m->y, AB_ERR_ARG, "hlrb: null data pointer");
+  AB_REQUIRE(m->ldx >= m->D && m->ldx % 8 == 0, AB_ERR_ARG, "hlrb: ldx must be >= D and a multiple of 8");
+  AB_REQUIRE(m->prior == AB_PRIOR_NORMAL || m->prior == AB_PRIOR_STUDENT_T, AB_ERR_ARG, "hlrb: unknown prior");
+  AB_REQUIRE(m->prior_a > 0.0 && (m->prior == AB_PRIOR_NORMAL || m->prior_b > 0.0), AB_ERR_ARG,
+             "hlrb: prior parameters must be positive");
+  return AB_OK;
+}
+
+size_t hlrb_workspace_bytes(int N, int D, int C) { return layout(N, D, C).total; }
+
+}  // namespace ab
+
+using namespace ab;
+
+extern "C" size_t ab_hlrb_xt_elems(int N, int D) {
+  if (N <= 0 || D <= 0) return 0;
+  return (size_t)D * (size_t)((N + 63) / 64 * 64);
+}
+
+extern "C" int ab_hlrb_transpose(int N, int D, const void* X, int ldx, void* Xt, void* stream) {
+  AB_REQUIRE(N > 0 && D > 0 && ldx >= D, AB_ERR_ARG, "ab_hlrb_transpose: bad sizes");
+  AB_REQUIRE(X && Xt, AB_ERR_ARG, "ab_hlrb_transpose: null pointer");
+  const int Np = (N + 63) / 64 * 64;
+  hlrb_transpose_kernel<<<dim3(ceil_div(Np, 32), ceil_div(D, 32)), dim3(32, 8), 0, as_stream(stream)>>>(
+      N, D, Np, static_cast<const __nv_bfloat16*>(X), ldx, static_cast<__nv_bfloat16*>(Xt));
+  AB_LAUNCH_CHECK("hlrb_transpose_kernel");
+  return AB_OK;
+}
+
+extern "C" size_t ab_hlrb_workspace_bytes(int N, int D, int C) {
+  if (N <= 0 || D <= 0 || C <= 0) return 0;
+  return hlrb_workspace_bytes(N, D, C);
+}
+
+extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp,
+                                 float* grad, int ldg, void* work, int* err, void* stream) {
+  int rc = hlrb_check_model(m);
+  if (rc) return rc;
+  AB_REQUIRE(C > 0 && C <= 65535, AB_ERR_ARG, "ab_hlrb_logp_grad: C must be 1..65535");
+  AB_REQUIRE(theta && logp && work, AB_ERR_ARG, "ab_hlrb_logp_grad: null pointer");
+  AB_REQUIRE(ldt >= m->D && (!grad || ldg >= m->D), AB_ERR_ARG, "ab_hlrb_logp_grad: leading dimension too small");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(work) & 255) == 0, AB_ERR_ARG, "ab_hlrb_logp_grad: workspace must be 256-byte aligned");
+  return hlrb_logp_grad(m, C, theta, ldt, logp, grad, ldg, work, err, as_stream(stream));
+}

@@ -14,7 +14,19 @@ namespace tc {
 namespace {
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::mutex g_encode_mu;
+int g_sms[64] = {0};
 }  // namespace
+
+int sm_count() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (!g_sms[dev]) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    g_sms[dev] = n;
+  }
+  return g_sms[dev];
+}
 
 int encode_2d_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t cols, uint64_t ld_elems,
                    uint32_t box_rows) {
@@ -48,7 +60,7 @@ struct StoreEpi {
   float* C;
   int M, N, ldc;
   int atomic;
-  __device__ void begin(int, int, int, char*) {}
+  __device__ void begin(int, int, int, char*, int) {}
   __device__ void rows(int row, int col0, const float* v, bool ok) {
     if (!ok) return;
     float* out = C + (size_t)row * ldc;
@@ -61,7 +73,7 @@ struct StoreEpi {
       }
     }
   }
-  __device__ void end(int, int, int) {}
+  __device__ void end(int, int, int, int, bool) {}
 };
 
 }  // namespace tc
@@ -81,13 +93,12 @@ extern "C" int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, cons
   const int BN = N >= 256 ? 256 : (N > 64 ? 128 : 64);
   rc = encode_2d_bf16(&tb, B, N, K, ldb, BN);
   if (rc) return rc;
-  StoreEpi epi{C, M, N, ldc, splits > 1};
-  const int ksplit = ((K + splits - 1) / splits + BK - 1) / BK * BK;
-  dim3 grid(ceil_div(M, BM), ceil_div(N, BN), splits);
+  const Shape sh = make_shape(M, N, K, splits, 0, 0, BN);
+  StoreEpi epi{C, M, N, ldc, sh.splits > 1};
   cudaStream_t st = as_stream(stream);
-  if (splits > 1) AB_CUDA(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, st));
-  if (BN == 256) rc = launch_gemm<256>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
-  else if (BN == 128) rc = launch_gemm<128>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
-  else rc = launch_gemm<64>(ta, tb, M, N, K, ksplit, epi, err, grid, st);
+  if (sh.splits > 1) AB_CUDA(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, st));
+  if (BN == 256) rc = launch_gemm<256, 1, 1>(ta, tb, sh, epi, err, st);
+  else if (BN == 128) rc = launch_gemm<128, 1, 1>(ta, tb, sh, epi, err, st);
+  else rc = launch_gemm<64, 1, 1>(ta, tb, sh, epi, err, st);
   return rc;
 }

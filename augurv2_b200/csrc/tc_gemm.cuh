@@ -1,21 +1,29 @@
 // Tensor-core GEMM core for sm_100a (tcgen05 + TMA), shared by the batched
-// HLR data passes and the gradient-surrogate MLP:
+// HLR data passes and the plain checking entry point:
 //
-//   C[M x N] = A[M x K] * B[N x K]^T        A, B bf16, row-major (K-major)
+//   C[M x N] = sum_p A_p[M x K] * B_p[N x K]^T     A, B bf16, row-major (K-major)
 //
-// One CTA computes one 128 x BN output tile (BN <= 256) over a K range
-// (split-K via blockIdx.z).  Four warps:
-//   warp 0 lane 0  TMA producer: 128x64 A tiles and BNx64 B tiles, 128-byte
-//                  swizzled, into a STAGES-deep ring guarded by mbarriers;
-//   warp 1 lane 0  MMA issuer: tcgen05.mma.cta_group::1.kind::f16 (M=128,
-//                  N=BN, K=16) into an FP32 accumulator in tensor memory,
-//                  tcgen05.commit frees each stage and finally signals done;
-//   all 4 warps    epilogue: warp w reads TMEM lanes 32w..32w+31 (one output
+// "Parts" let one operand be a sum of bf16 slices of an FP32 matrix: with
+// PA = 3 the A operand is hi + mid + lo (three K-ranges of the same rows,
+// a_pstride elements apart) and B is shared by the three products, so an
+// FP32 matrix times a bf16 matrix is computed to FP32 accuracy on the bf16
+// tensor pipe.  At most one of PA, PB is above 1.
+//
+// Persistent kernel: one CTA per SM walks the 128 x BN output tiles
+// (tile = blockIdx.x + i * gridDim.x; tile -> (m fastest, n, split)).
+// Six warps:
+//   warp 0 lane 0  TMA producer: per K step PA 128x64 A tiles and PB BNx64 B
+//                  tiles, 128-byte swizzled, into a STAGES-deep ring;
+//   warp 1 lane 0  MMA issuer: tcgen05.mma.cta_group::1.kind::f16 (M = 128,
+//                  N = BN, K = 16) into one of two FP32 accumulators in
+//                  tensor memory, so the next tile's MMAs overlap the
+//                  previous tile's epilogue;
+//   warps 2..5     epilogue: warp w reads TMEM lanes 32(w%4)..+31 (one output
 //                  row per thread) 32 columns at a time with tcgen05.ld and
 //                  hands them to the epilogue functor.
 // Every mbarrier wait is bounded (clock-based); on expiry the kernel records
-// AB_ERR_TIMEOUT in *err, drains its outstanding copies, frees its tensor
-// memory and returns.
+// AB_ERR_TIMEOUT in *err, stops issuing, waits (bounded) for its outstanding
+// copies and MMAs, frees its tensor memory and returns.
 #pragma once
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -27,7 +35,9 @@ namespace tc {
 
 constexpr int BM = 128;
 constexpr int BK = 64;                      // 64 bf16 = one 128-byte swizzle row
+constexpr int THREADS = 192;
 constexpr long long WAIT_CYCLES = 4000000000LL;   // ~2 s at 2 GHz
+constexpr int SMEM_BUDGET = 232448;                // 227 KB opt-in per block
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -40,6 +50,10 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Bounded wait for the phase with the given parity; false on timeout.
@@ -96,6 +110,9 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// Named barrier over the four epilogue warps.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
 // 32 consecutive fp32 columns of this warp's 32 TMEM lanes.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   uint32_t r[32];
@@ -113,48 +130,73 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-template <int BN>
-struct Cfg {
-  static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "BN in {32, 64, ..., 256}");
-  static constexpr int A_BYTES = BM * BK * 2;
-  static constexpr int B_BYTES = BN * BK * 2;
-  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = (BN >= 256) ? 4 : (BN >= 128 ? 6 : 8);
-  static constexpr int TMEM_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
-  // ring + barriers + tmem slot, with 1024-byte alignment slack; the
-  // epilogue's own shared memory (Epi::kSmem) follows at EPI_OFFSET
-  static constexpr int EPI_OFFSET = STAGES * STAGE_BYTES + 256;
-  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+// Problem shape as the kernel sees it.  K is the reduction length of one
+// part; part p of A starts a_pstride elements after part 0 (likewise B).
+// Each split covers k_split elements of K (a multiple of BK); the host makes
+// every split non-empty.
+struct Shape {
+  int M, N, K;
+  int k_split;
+  int a_pstride, b_pstride;
+  int m_tiles, n_tiles, splits;
 };
 
-// The kernel.  Epi must provide:
-//   __device__ void begin(int m_tile, int n_tile, int split, char* smem_scratch)   (all threads)
-//   __device__ void rows(int row, int col0, const float* v32, bool row_ok)        (all threads, per 32 cols)
-//   __device__ void end(int m_tile, int n_tile, int split)                        (all threads)
-template <int BN, class Epi>
-__global__ void __launch_bounds__(128, 1)
-gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int M, int N, int K,
-            int k_split, Epi epi, int* __restrict__ err) {
-  using C = Cfg<BN>;
+template <int BN, int PA, int PB, int EPI_SMEM>
+struct Cfg {
+  static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "BN in {32, 64, ..., 256}");
+  static_assert(PA >= 1 && PB >= 1 && (PA == 1 || PB == 1), "one operand may have parts");
+  static constexpr int P = PA > PB ? PA : PB;
+  static constexpr int A_BYTES = BM * BK * 2;
+  static constexpr int B_BYTES = BN * BK * 2;
+  static constexpr int STAGE_BYTES = PA * A_BYTES + PB * B_BYTES;
+  static constexpr int FIXED = 1024 + 512 + EPI_SMEM;   // alignment slack, barriers, epilogue
+  static constexpr int FIT = (SMEM_BUDGET - FIXED) / STAGE_BYTES;
+  static constexpr int STAGES = FIT > 8 ? 8 : FIT;
+  static_assert(STAGES >= 2, "tile does not fit two stages in shared memory");
+  static constexpr int ACC_COLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+  static constexpr int TMEM_COLS = 2 * ACC_COLS;          // two accumulators
+  static constexpr int BAR_OFFSET = STAGES * STAGE_BYTES;
+  static constexpr int EPI_OFFSET = BAR_OFFSET + 512;
+  static constexpr int SMEM_BYTES = EPI_OFFSET + EPI_SMEM + 1024;
+};
+
+// The kernel.  Epi must provide (called by the 128 epilogue threads only;
+// etid = 0..127, row = this thread's output row):
+//   static constexpr int kSmem;
+//   __device__ void begin(int m_tile, int n_tile, int split, char* smem, int etid);
+//   __device__ void rows(int row, int col0, const float* v32, bool row_ok);
+//   __device__ void end(int m_tile, int n_tile, int split, int row, bool row_ok);
+// begin() may fill shared memory; a named barrier over the epilogue warps
+// separates begin() from rows() and end() from the next tile's begin().
+template <int BN, int PA, int PB, class Epi>
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, Shape sh, Epi epi,
+            int* __restrict__ err) {
+  using C = Cfg<BN, PA, PB, Epi::kSmem>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* ring = base;
-  uint64_t* full = reinterpret_cast<uint64_t*>(base + C::STAGES * C::STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + C::BAR_OFFSET);
   uint64_t* empty = full + C::STAGES;
-  uint64_t* done = empty + C::STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  uint64_t* acc_full = empty + C::STAGES;   // [2] MMA -> epilogue
+  uint64_t* acc_empty = acc_full + 2;       // [2] epilogue -> MMA
+  uint64_t* drain = acc_empty + 2;          // MMA issuer's final completion
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   int* fail = reinterpret_cast<int*>(tmem_slot + 1);
+  int* epi_fail = fail + 1;
+  char* epi_smem = reinterpret_cast<char*>(base + C::EPI_OFFSET);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  const int kb0 = (blockIdx.z * k_split) / BK;
-  const int kb1 = min((K + BK - 1) / BK, ((blockIdx.z + 1) * k_split) / BK);
-  const int nkb = max(0, kb1 - kb0);
+  const int total = sh.m_tiles * sh.n_tiles * sh.splits;
+  const int kb_all = (sh.K + BK - 1) / BK;
+  const int kb_per_split = sh.k_split / BK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    mbar_init(done, 1);
+    for (int b = 0; b < 2; ++b) { mbar_init(&acc_full[b], 1); mbar_init(&acc_empty[b], 4); }
+    mbar_init(drain, 1);
     *fail = 0;
+    *epi_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -167,61 +209,115 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
   __syncthreads();
   fence_after();
   const uint32_t tmem = *tmem_slot;
-  epi.begin(blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<char*>(base + C::EPI_OFFSET));
 
-  int issued = 0;   // TMA stages issued (producer)
-  if (threadIdx.x == 0) {
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % C::STAGES;
-      const uint32_t ph = (kb / C::STAGES) & 1;
-      if (kb >= C::STAGES && !mbar_wait(&empty[s], ph ^ 1)) { *fail = 1; break; }
-      if (*(volatile int*)fail) break;
-      unsigned char* a = ring + s * C::STAGE_BYTES;
-      unsigned char* b = a + C::A_BYTES;
-      mbar_expect_tx(&full[s], C::STAGE_BYTES);
-      tma_load_2d(a, &ta, &full[s], (kb0 + kb) * BK, m0);
-      tma_load_2d(b, &tb, &full[s], (kb0 + kb) * BK, n0);
-      ++issued;
-    }
-  } else if (threadIdx.x == 32) {
-    const uint32_t idesc = make_idesc(BN);
-    int kb = 0;
-    for (; kb < nkb; ++kb) {
-      const int s = kb % C::STAGES;
-      const uint32_t ph = (kb / C::STAGES) & 1;
-      if (!mbar_wait(&full[s], ph)) { *fail = 1; break; }
-      if (*(volatile int*)fail) break;
-      fence_after();
-      const uint64_t ad = make_desc(ring + s * C::STAGE_BYTES);
-      const uint64_t bd = make_desc(ring + s * C::STAGE_BYTES + C::A_BYTES);
+  int issued = 0;   // TMA stages issued (producer), for the drain on failure
+  if (warp == 0) {
+    if (lane == 0) {
+      int g = 0;   // global K-step counter across tiles (ring position)
+      for (int t = blockIdx.x; t < total && !*(volatile int*)fail; t += gridDim.x) {
+        const int mt = t % sh.m_tiles, nt = (t / sh.m_tiles) % sh.n_tiles, sp = t / (sh.m_tiles * sh.n_tiles);
+        const int kb0 = sp * kb_per_split, kb1 = min(kb_all, kb0 + kb_per_split);
+        for (int kb = kb0; kb < kb1; ++kb, ++g) {
+          const int s = g % C::STAGES;
+          const uint32_t ph = (g / C::STAGES) & 1;
+          if (g >= C::STAGES && !mbar_wait(&empty[s], ph ^ 1)) { *fail = 1; break; }
+          if (*(volatile int*)fail) break;
+          unsigned char* a = ring + s * C::STAGE_BYTES;
+          unsigned char* b = a + PA * C::A_BYTES;
+          mbar_expect_tx(&full[s], C::STAGE_BYTES);
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk)
-        mma_bf16(tmem, ad + 2 * kk, bd + 2 * kk, idesc, (kb > 0 || kk > 0) ? 1u : 0u);
-      mma_commit(&empty[s]);
+          for (int p = 0; p < PA; ++p)
+            tma_load_2d(a + p * C::A_BYTES, &ta, &full[s], kb * BK + p * sh.a_pstride, mt * BM);
+#pragma unroll
+          for (int p = 0; p < PB; ++p)
+            tma_load_2d(b + p * C::B_BYTES, &tb, &full[s], kb * BK + p * sh.b_pstride, nt * BN);
+          ++issued;
+        }
+      }
     }
-    mma_commit(done);   // arrives when every issued MMA has completed
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = make_idesc(BN);
+      int g = 0, i = 0;
+      for (int t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+        const int sp = t / (sh.m_tiles * sh.n_tiles);
+        const int kb0 = sp * kb_per_split, kb1 = min(kb_all, kb0 + kb_per_split);
+        const int ab = i & 1;
+        if (i >= 2 && !mbar_wait(&acc_empty[ab], ((i >> 1) - 1) & 1)) { *fail = 1; break; }
+        if (*(volatile int*)fail) break;
+        fence_after();
+        const uint32_t d = tmem + (uint32_t)(ab * C::ACC_COLS);
+        bool bad = false;
+        for (int kb = kb0; kb < kb1; ++kb, ++g) {
+          const int s = g % C::STAGES;
+          const uint32_t ph = (g / C::STAGES) & 1;
+          if (!mbar_wait(&full[s], ph)) { *fail = 1; bad = true; break; }
+          if (*(volatile int*)fail) { bad = true; break; }
+          fence_after();
+          unsigned char* a = ring + s * C::STAGE_BYTES;
+          unsigned char* b = a + PA * C::A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+#pragma unroll
+            for (int p = 0; p < C::P; ++p) {
+              const uint64_t ad = make_desc(a + (PA > 1 ? p : 0) * C::A_BYTES) + 2 * kk;
+              const uint64_t bd = make_desc(b + (PB > 1 ? p : 0) * C::B_BYTES) + 2 * kk;
+              mma_bf16(d, ad, bd, idesc, (kb > kb0 || kk > 0 || p > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit(&empty[s]);
+        }
+        if (bad) break;
+        mma_commit(&acc_full[ab]);   // arrives when this tile's MMAs have completed
+      }
+      // every MMA this thread issued has completed before tensor memory is freed
+      mma_commit(drain);
+      if (!mbar_wait(drain, 0)) *fail = 1;
+    }
+  } else {
+    // epilogue warps 2..5
+    const int q = warp & 3;                 // TMEM lane quarter this warp may access
+    const int etid = (warp - 2) * 32 + lane;
+    Epi e(epi);                             // per-thread copy: functors may keep running sums
+    int i = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+      const int mt = t % sh.m_tiles, nt = (t / sh.m_tiles) % sh.n_tiles, sp = t / (sh.m_tiles * sh.n_tiles);
+      const int kb0 = sp * kb_per_split, kb1 = min(kb_all, kb0 + kb_per_split);
+      const int ab = i & 1;
+      e.begin(mt, nt, sp, epi_smem, etid);
+      epi_sync();
+      // warp-uniform: tcgen05.ld is a warp-collective instruction
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[ab], (i >> 1) & 1));
+      fence_after();
+      const bool have = __all_sync(0xffffffffu, ok && kb1 > kb0 && !*(volatile int*)fail);
+      const int row = mt * BM + q * 32 + lane;
+      const bool row_ok = row < sh.M;
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        float v[32];
+        if (have) {
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * C::ACC_COLS + c0), v);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+        }
+        e.rows(row, nt * BN + c0, v, row_ok);
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acc_empty[ab]);
+      e.end(mt, nt, sp, row, row_ok);
+      if (!ok || *(volatile int*)fail) { *fail = 1; *(volatile int*)epi_fail = 1; }
+      epi_sync();
+      // uniform across the epilogue warps: written only before the barrier
+      if (*(volatile int*)epi_fail) break;
+    }
   }
   __syncwarp();
-  // epilogue
-  bool ok = mbar_wait(done, 0);
-  fence_after();
-  if (!ok) *fail = 1;
-  const bool have = nkb > 0 && ok && !*(volatile int*)fail;
-  const int row = m0 + warp * 32 + lane;
-  for (int c0 = 0; c0 < BN; c0 += 32) {
-    float v[32];
-    if (have) {
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-    } else {
-#pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = 0.0f;
-    }
-    epi.rows(row, n0 + c0, v, row < M);
-  }
-  epi.end(blockIdx.x, blockIdx.y, blockIdx.z);
-  // drain: a producer that stopped early still has copies in flight
+  // drain: a producer that stopped early may still have copies in flight;
+  // the last copy issued into each stage is the one still outstanding there
   if (threadIdx.x == 0 && *(volatile int*)fail) {
-    for (int kb = 0; kb < issued; ++kb) mbar_wait(&full[kb % C::STAGES], (kb / C::STAGES) & 1);
+    for (int g = max(0, issued - C::STAGES); g < issued; ++g)
+      mbar_wait(&full[g % C::STAGES], (g / C::STAGES) & 1);
   }
   fence_before();
   __syncthreads();

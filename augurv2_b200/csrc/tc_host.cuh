@@ -11,14 +11,39 @@ namespace tc {
 int encode_2d_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t cols, uint64_t ld_elems,
                    uint32_t box_rows);
 
-template <int BN, class Epi>
-int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int K, int ksplit, const Epi& epi,
-                int* err, dim3 grid, cudaStream_t st) {
-  using C = Cfg<BN>;
-  const int smem = C::SMEM_BYTES + Epi::kSmem;
-  AB_REQUIRE(smem <= 232448, AB_ERR_ARG, "GEMM tile needs %d bytes of shared memory", smem);
-  AB_CUDA(cudaFuncSetAttribute(gemm_kernel<BN, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  gemm_kernel<BN, Epi><<<grid, 128, smem, st>>>(ta, tb, M, N, K, ksplit, epi, err);
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Shape with K split into at most `splits` non-empty ranges of whole K steps.
+inline Shape make_shape(int M, int N, int K, int splits, int a_pstride, int b_pstride, int bn) {
+  Shape s;
+  s.M = M;
+  s.N = N;
+  s.K = K;
+  const int kb_all = (K + BK - 1) / BK;
+  if (splits < 1) splits = 1;
+  if (splits > kb_all) splits = kb_all;
+  const int per = (kb_all + splits - 1) / splits;
+  s.k_split = per * BK;
+  s.splits = (kb_all + per - 1) / per;
+  s.a_pstride = a_pstride;
+  s.b_pstride = b_pstride;
+  s.m_tiles = (M + BM - 1) / BM;
+  s.n_tiles = (N + bn - 1) / bn;
+  return s;
+}
+
+template <int BN, int PA, int PB, class Epi>
+int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, const Shape& sh, const Epi& epi, int* err,
+                cudaStream_t st) {
+  using C = Cfg<BN, PA, PB, Epi::kSmem>;
+  static_assert(C::SMEM_BYTES <= SMEM_BUDGET, "GEMM tile exceeds shared memory");
+  AB_CUDA(cudaFuncSetAttribute(gemm_kernel<BN, PA, PB, Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               C::SMEM_BYTES));
+  const long long total = (long long)sh.m_tiles * sh.n_tiles * sh.splits;
+  AB_REQUIRE(total > 0 && total < (1LL << 31), AB_ERR_ARG, "GEMM tile count out of range");
+  const int grid = (int)(total < sm_count() ? total : sm_count());
+  gemm_kernel<BN, PA, PB, Epi><<<grid, THREADS, C::SMEM_BYTES, st>>>(ta, tb, sh, epi, err);
   AB_LAUNCH_CHECK("tc gemm_kernel");
   return AB_OK;
 }

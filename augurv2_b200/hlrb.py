@@ -1,0 +1,433 @@
+"""Batched HLR sampling on the tensor cores: host side of ab_hlrb_*, ab_hmcb_*
+and the gradient surrogate (ab_mlp_*, ab_sur_*).
+
+Model (compiler/augur/test/hlr.rv with the coefficient prior fixed):
+    theta[d] ~ Normal(0, var)  or  StudentT(nu, scale)      d < D
+    y[n] ~ Bernoulli(sigmoid(dotprod(theta, x[n])))
+C chains share one bf16 design matrix; each chain is one FP32 row of
+`theta` [C, D].  `BatchedHmc` runs the reference's HMC transition
+(cbits/augur_mcmclib.h:343-424) for all chains with the exact gradient;
+`SurrogateHmc` runs the same transition with the leapfrog driven by a small
+MLP trained online on (theta, exact gradient) pairs that the sampler itself
+produces, while the exact log density decides every accept.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+PRIOR_NORMAL, PRIOR_STUDENT_T = 0, 1
+
+
+class HlrbModelC(C.Structure):
+    _fields_ = [("N", C.c_int), ("D", C.c_int), ("ldx", C.c_int), ("X", C.c_void_p), ("Xt", C.c_void_p),
+                ("y", C.c_void_p), ("prior", C.c_int), ("prior_a", C.c_double), ("prior_b", C.c_double)]
+
+
+class HmcbStateC(C.Structure):
+    _fields_ = [("C", C.c_int), ("D", C.c_int), ("seed", C.c_ulonglong), ("iter", C.c_void_p),
+                ("eps0", C.c_void_p), ("jitter", C.c_float), ("theta", C.c_void_p), ("p", C.c_void_p),
+                ("g_cur", C.c_void_p), ("logp_cur", C.c_void_p), ("theta0", C.c_void_p), ("g0", C.c_void_p),
+                ("logp0", C.c_void_p), ("H0", C.c_void_p), ("eps_c", C.c_void_p), ("stats", C.c_void_p)]
+
+
+class MlpDescC(C.Structure):
+    _fields_ = [("d_in", C.c_int), ("h1", C.c_int), ("h2", C.c_int), ("d_out", C.c_int), ("w", C.c_void_p),
+                ("wb", C.c_void_p)]
+
+
+class HlrbData:
+    """Design matrix (bf16, device), its transpose, labels and the prior."""
+
+    def __init__(self, X, y, prior="student_t", nu=3.0, scale=1.0, var=1.0, device="cuda"):
+        X = torch.as_tensor(X)
+        if X.dtype != torch.bfloat16:
+            X = X.to(torch.float32).to(torch.bfloat16)
+        self.X = X.to(device).contiguous()
+        self.N, self.D = self.X.shape
+        if self.D % 8:
+            raise ValueError("D must be a multiple of 8 (16-byte rows for the tensor maps)")
+        self.y = torch.as_tensor(y).to(device=device, dtype=torch.int32).contiguous()
+        n_xt = int(N.lib().ab_hlrb_xt_elems(self.N, self.D))
+        self.Xt = torch.empty(n_xt, dtype=torch.bfloat16, device=device)
+        N.check(N.lib().ab_hlrb_transpose(self.N, self.D, N.ptr(self.X), self.D, N.ptr(self.Xt), N.stream_ptr()),
+                "ab_hlrb_transpose")
+        if prior == "student_t":
+            self.prior, self.pa, self.pb = PRIOR_STUDENT_T, float(nu), float(scale)
+        elif prior == "normal":
+            self.prior, self.pa, self.pb = PRIOR_NORMAL, float(var), 0.0
+        else:
+            raise ValueError("prior must be 'student_t' or 'normal'")
+        self.c = HlrbModelC(self.N, self.D, self.D, self.X.data_ptr(), self.Xt.data_ptr(), self.y.data_ptr(),
+                            self.prior, self.pa, self.pb)
+        self.device = self.X.device
+
+    def workspace(self, C_):
+        nb = int(N.lib().ab_hlrb_workspace_bytes(self.N, self.D, C_))
+        return torch.empty(nb, dtype=torch.uint8, device=self.device)
+
+    def logp_grad(self, theta, grad=True, logp_out=None, grad_out=None, work=None, err=None, stream=None):
+        """(logp [C] f64, grad [C, D] f32 or None) at theta [C, D] f32 (device)."""
+        C_ = theta.shape[0]
+        if logp_out is None:
+            logp_out = torch.empty(C_, dtype=torch.float64, device=self.device)
+        if grad and grad_out is None:
+            grad_out = torch.empty((C_, self.D), dtype=torch.float32, device=self.device)
+        if work is None:
+            work = self.workspace(C_)
+        N.check(N.lib().ab_hlrb_logp_grad(C.byref(self.c), C_, N.ptr(theta), theta.stride(0), N.ptr(logp_out),
+                                          N.ptr(grad_out) if grad else None, self.D, N.ptr(work),
+                                          N.ptr(err) if err is not None else None, N.stream_ptr(stream)),
+                "ab_hlrb_logp_grad")
+        return logp_out, (grad_out if grad else None)
+
+
+def synthetic(N_, D, seed=0, nu=3.0, device="cuda", chunk=1 << 18):
+    """X ~ N(0,1) (bf16), beta ~ StudentT(nu), y ~ Bernoulli(sigmoid(X beta))."""
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    rs = np.random.default_rng(seed)
+    beta = rs.standard_t(nu, size=D).astype(np.float32)
+    X = torch.empty((N_, D), dtype=torch.bfloat16, device=device)
+    y = torch.empty(N_, dtype=torch.int32, device=device)
+    bt = torch.as_tensor(beta, device=device)
+    for s in range(0, N_, chunk):
+        e = min(N_, s + chunk)
+        xs = torch.randn((e - s, D), generator=g, device=device)
+        X[s:e] = xs.to(torch.bfloat16)
+        t = X[s:e].float() @ bt
+        y[s:e] = (torch.rand(e - s, generator=g, device=device) < torch.sigmoid(t)).to(torch.int32)
+    return X, y, beta
+
+
+class _ChainState:
+    """Device buffers of ab_hmcb_state."""
+
+    def __init__(self, C_, D, seed, eps, jitter, init, device):
+        f32, f64 = torch.float32, torch.float64
+        self.C, self.D = C_, D
+        self.theta = torch.as_tensor(np.asarray(init, np.float32)).to(device).reshape(C_, D).contiguous()
+        z = lambda *s, dt=f32: torch.zeros(*s, dtype=dt, device=device)
+        self.p, self.g_cur, self.theta0, self.g0 = z(C_, D), z(C_, D), z(C_, D), z(C_, D)
+        self.logp_cur, self.logp0, self.H0 = z(C_, dt=f64), z(C_, dt=f64), z(C_, dt=f64)
+        self.eps_c = z(C_)
+        self.stats = z(C_, 2, dt=f64)
+        self.iter = torch.zeros(1, dtype=torch.int64, device=device)
+        self.eps0 = torch.full((1,), float(eps), dtype=f32, device=device)
+        self.c = HmcbStateC(C_, D, int(seed), self.iter.data_ptr(), self.eps0.data_ptr(), float(jitter),
+                            self.theta.data_ptr(), self.p.data_ptr(), self.g_cur.data_ptr(),
+                            self.logp_cur.data_ptr(), self.theta0.data_ptr(), self.g0.data_ptr(),
+                            self.logp0.data_ptr(), self.H0.data_ptr(), self.eps_c.data_ptr(), self.stats.data_ptr())
+
+    def begin(self, stream=None):
+        N.check(N.lib().ab_hmcb_begin(C.byref(self.c), N.stream_ptr(stream)), "ab_hmcb_begin")
+
+    def step(self, g, stream=None):
+        N.check(N.lib().ab_hmcb_step(C.byref(self.c), N.ptr(g), N.stream_ptr(stream)), "ab_hmcb_step")
+
+    def final(self, g_new, logp_new, stream=None):
+        N.check(N.lib().ab_hmcb_final(C.byref(self.c), N.ptr(g_new), N.ptr(logp_new), N.stream_ptr(stream)),
+                "ab_hmcb_final")
+
+
+class BatchedHmc:
+    """C chains of exact-gradient HMC on an HlrbData: L leapfrog steps of size
+    eps (jittered per chain by +-jitter), FP64 energies, one exact log density
+    and gradient per step."""
+
+    def __init__(self, data, C_, L=10, eps=0.01, jitter=0.1, seed=0, init=None):
+        self.data, self.C, self.L = data, int(C_), int(L)
+        D = data.D
+        if init is None:
+            init = np.zeros((self.C, D), np.float32)
+        init = np.broadcast_to(np.asarray(init, np.float32), (self.C, D)).copy()
+        self.s = _ChainState(self.C, D, seed, eps, jitter, init, data.device)
+        self.work = data.workspace(self.C)
+        self.err = torch.zeros(1, dtype=torch.int32, device=data.device)
+        self.logp_new = torch.zeros(self.C, dtype=torch.float64, device=data.device)
+        self.g_new = torch.zeros((self.C, D), dtype=torch.float32, device=data.device)
+        self.n_grad = 0
+        data.logp_grad(self.s.theta, True, self.s.logp_cur, self.s.g_cur, self.work, self.err)
+        self.graph = None
+
+    @property
+    def theta(self):
+        return self.s.theta
+
+    def set_eps(self, eps):
+        self.s.eps0.fill_(float(eps))
+
+    def _iteration(self, stream=None):
+        s, d = self.s, self.data
+        s.begin(stream)
+        for l in range(self.L):
+            d.logp_grad(s.theta, True, self.logp_new, self.g_new, self.work, self.err, stream)
+            if l < self.L - 1:
+                s.step(self.g_new, stream)
+        s.final(self.g_new, self.logp_new, stream)
+
+    def capture(self):
+        """Capture one iteration (L exact passes) as a CUDA graph."""
+        side = torch.cuda.Stream(device=self.data.device)
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            self._iteration(side)          # warm (sets kernel attributes outside capture)
+        torch.cuda.current_stream().wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._iteration(torch.cuda.current_stream())
+        self.n_grad += self.L
+
+    def run(self, n=1, record=None):
+        for _ in range(int(n)):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._iteration()
+            self.n_grad += self.L
+            if record is not None:
+                record.append(self.s.theta.clone())
+
+    def accept_rate(self):
+        st = self.s.stats.cpu().numpy()
+        it = int(self.s.iter.item())
+        return st[:, 0].sum() / max(1, it * self.C), st[:, 1].sum() / max(1, it * self.C)
+
+    def reset_stats(self):
+        self.s.stats.zero_()
+        self.s.iter.zero_()
+
+
+class MlpSurrogate:
+    """Gradient surrogate g(theta) ~ a + h (theta - mu) + o * MLP((theta - mu) / s).
+
+    The diagonal linear part (a, h per coordinate) is a least-squares fit of
+    each gradient coordinate on its own parameter; the MLP d-h1-h2-d (GELU,
+    bf16 weights, FP32 accumulation) learns the rest in units of the
+    residual's per-coordinate scale o.  Trained by Adam on (theta, gradient)
+    pairs from a replay buffer."""
+
+    def __init__(self, D, h1=256, h2=256, seed=0, device="cuda", capacity=8192, batch=512, lr=1e-3):
+        self.D, self.h1, self.h2 = D, h1, h2
+        self.device = device
+        n = int(N.lib().ab_mlp_param_count(D, h1, h2, D))
+        rs = np.random.default_rng(seed)
+        w = np.zeros(n, np.float32)
+        off = 0
+        for fan_in, fan_out in ((D, h1), (h1, h2), (h2, D)):
+            lim = math.sqrt(6.0 / (fan_in + fan_out))
+            w[off:off + fan_in * fan_out] = rs.uniform(-lim, lim, fan_in * fan_out)
+            off += fan_in * fan_out + fan_out
+        # last layer starts at zero output: the surrogate begins as the linear fit
+        w3 = n - D - h2 * D
+        w[w3:w3 + h2 * D] *= 0.1
+        self.w = torch.as_tensor(w).to(device)
+        self.wb = torch.empty(n, dtype=torch.bfloat16, device=device)
+        self.m = torch.zeros_like(self.w)
+        self.v = torch.zeros_like(self.w)
+        self.gw = torch.zeros_like(self.w)
+        self.desc = MlpDescC(D, h1, h2, D, self.w.data_ptr(), self.wb.data_ptr())
+        N.check(N.lib().ab_mlp_sync_bf16(C.byref(self.desc), N.stream_ptr()), "ab_mlp_sync_bf16")
+        self.step_count = 0
+        self.lr, self.batch = lr, int(batch)
+        f = lambda: torch.zeros(D, dtype=torch.float32, device=device)
+        self.mu, self.inv_s, self.a, self.h, self.o = f(), f() + 1.0, f(), f(), f() + 1.0
+        self.cap = int(capacity)
+        self.buf_theta = torch.zeros((self.cap, D), dtype=torch.float32, device=device)
+        self.buf_grad = torch.zeros((self.cap, D), dtype=torch.float32, device=device)
+        self.n_buf, self.pos = 0, 0
+        self._bufs = {}
+        self.gen = torch.Generator(device=device)
+        self.gen.manual_seed(int(seed) + 1)
+        self.use_net = True
+
+    def _scratch(self, B):
+        if B not in self._bufs:
+            D, dev = self.D, self.device
+            self._bufs[B] = dict(
+                z=torch.empty((B, D), dtype=torch.float32, device=dev),
+                out=torch.empty((B, D), dtype=torch.float32, device=dev),
+                act=torch.empty(int(N.lib().ab_mlp_act_floats(B, self.h1, self.h2)), dtype=torch.float32,
+                                device=dev),
+                bsc=torch.empty(int(N.lib().ab_mlp_backward_scratch_floats(B, self.h1, self.h2)),
+                                dtype=torch.float32, device=dev),
+                dy=torch.empty((B, D), dtype=torch.float32, device=dev),
+                tgt=torch.empty((B, D), dtype=torch.float32, device=dev),
+                rsq=torch.empty(B, dtype=torch.float64, device=dev),
+            )
+        return self._bufs[B]
+
+    def add(self, theta, grad):
+        """Append pairs (rows of theta, grad) to the replay ring."""
+        n = theta.shape[0]
+        idx = (torch.arange(n, device=self.device) + self.pos) % self.cap
+        self.buf_theta[idx] = theta
+        self.buf_grad[idx] = grad
+        self.pos = (self.pos + n) % self.cap
+        self.n_buf = min(self.cap, self.n_buf + n)
+
+    def refit(self):
+        """Input scaling and the diagonal linear part from the replay buffer."""
+        th, g = self.buf_theta[:self.n_buf], self.buf_grad[:self.n_buf]
+        mu = th.mean(0)
+        dt = th - mu
+        var = (dt * dt).mean(0).clamp_min(1e-30)
+        gm = g.mean(0)
+        h = ((g - gm) * dt).mean(0) / var
+        self.mu.copy_(mu)
+        self.inv_s.copy_(var.rsqrt())
+        self.a.copy_(gm)
+        self.h.copy_(h)
+        res = g - gm - h * dt
+        self.o.copy_((res * res).mean(0).sqrt().clamp_min(1e-12))
+
+    def predict(self, theta, out_grad, stream=None):
+        B = theta.shape[0]
+        sc = self._scratch(B)
+        L, st = N.lib(), N.stream_ptr(stream)
+        N.check(L.ab_sur_pre(B, self.D, N.ptr(theta), N.ptr(self.mu), N.ptr(self.inv_s), N.ptr(sc["z"]), st),
+                "ab_sur_pre")
+        if self.use_net:
+            N.check(L.ab_mlp_forward(C.byref(self.desc), B, N.ptr(sc["z"]), self.D, N.ptr(sc["out"]), self.D,
+                                     N.ptr(sc["act"]), st), "ab_mlp_forward")
+        else:
+            sc["out"].zero_()
+        N.check(L.ab_sur_post(B, self.D, N.ptr(theta), N.ptr(sc["out"]), N.ptr(self.mu), N.ptr(self.a),
+                              N.ptr(self.h), N.ptr(self.o), N.ptr(out_grad), st), "ab_sur_post")
+        return out_grad
+
+    def train(self, steps):
+        """Adam steps on minibatches of the replay buffer; returns the last
+        minibatch's mean squared error in output units."""
+        if self.n_buf == 0 or not self.use_net:
+            return float("nan")
+        B = min(self.batch, self.n_buf)
+        sc = self._scratch(B)
+        L, st = N.lib(), N.stream_ptr()
+        loss = None
+        for _ in range(int(steps)):
+            idx = torch.randint(0, self.n_buf, (B,), generator=self.gen, device=self.device)
+            th = self.buf_theta[idx]
+            g = self.buf_grad[idx]
+            dt = th - self.mu
+            torch.mul(dt, self.inv_s, out=sc["z"])
+            torch.div(g - self.a - self.h * dt, self.o, out=sc["tgt"])
+            N.check(L.ab_mlp_forward(C.byref(self.desc), B, N.ptr(sc["z"]), self.D, N.ptr(sc["out"]), self.D,
+                                     N.ptr(sc["act"]), st), "ab_mlp_forward")
+            N.check(L.ab_mlp_mse(B, self.D, N.ptr(sc["out"]), self.D, N.ptr(sc["tgt"]), self.D, N.ptr(sc["dy"]),
+                                 N.ptr(sc["rsq"]), st), "ab_mlp_mse")
+            N.check(L.ab_mlp_backward(C.byref(self.desc), B, N.ptr(sc["z"]), self.D, N.ptr(sc["dy"]),
+                                      N.ptr(sc["act"]), N.ptr(self.gw), N.ptr(sc["bsc"]), st), "ab_mlp_backward")
+            self.step_count += 1
+            N.check(L.ab_mlp_adam(C.byref(self.desc), N.ptr(self.gw), N.ptr(self.m), N.ptr(self.v),
+                                  self.step_count, self.lr, 0.9, 0.999, 1e-8, st), "ab_mlp_adam")
+            loss = sc["rsq"]
+        return float(loss.sum().item()) / (B * self.D)
+
+    def rel_error(self, theta, grad):
+        """Relative error |g_hat - g| / |g| (Frobenius) on given pairs."""
+        gh = torch.empty_like(grad)
+        self.predict(theta, gh)
+        return float(torch.linalg.vector_norm(gh - grad) / torch.linalg.vector_norm(grad).clamp_min(1e-30))
+
+
+class SurrogateHmc:
+    """HMC whose leapfrog uses the surrogate gradient; the exact log density
+    (tensor-core forward pass) decides every accept, so each chain targets the
+    exact posterior.  Every `train_every` iterations the exact gradient at the
+    proposals is computed too and joins the replay buffer; if the surrogate's
+    relative error on those fresh pairs exceeds `max_rel_err`, the sampler
+    falls back to exact-gradient HMC until a later check passes."""
+
+    def __init__(self, data, C_, L=10, eps=0.01, jitter=0.1, seed=0, init=None, surrogate=None,
+                 train_every=4, train_steps=20, max_rel_err=0.5):
+        self.data, self.C, self.L = data, int(C_), int(L)
+        D = data.D
+        if init is None:
+            init = np.zeros((self.C, D), np.float32)
+        init = np.broadcast_to(np.asarray(init, np.float32), (self.C, D)).copy()
+        self.s = _ChainState(self.C, D, seed, eps, jitter, init, data.device)
+        self.sur = surrogate if surrogate is not None else MlpSurrogate(D, seed=seed, device=data.device)
+        self.work = data.workspace(self.C)
+        self.err = torch.zeros(1, dtype=torch.int32, device=data.device)
+        self.logp_new = torch.zeros(self.C, dtype=torch.float64, device=data.device)
+        self.g_new = torch.zeros((self.C, D), dtype=torch.float32, device=data.device)
+        self.g_exact = torch.zeros((self.C, D), dtype=torch.float32, device=data.device)
+        self.train_every, self.train_steps, self.max_rel_err = int(train_every), int(train_steps), max_rel_err
+        self.n_grad = 0          # exact gradient passes (forward + backward)
+        self.n_logp = 0          # exact log-density-only passes
+        self.it = 0
+        self.fallback = False
+        self.last_rel_err = float("nan")
+        data.logp_grad(self.s.theta, True, self.s.logp_cur, self.g_exact, self.work, self.err)
+        self.n_grad += 1
+        self.sur.add(self.s.theta, self.g_exact)
+        self.sur.refit()
+        self.sur.predict(self.s.theta, self.s.g_cur)
+
+    @property
+    def theta(self):
+        return self.s.theta
+
+    def set_eps(self, eps):
+        self.s.eps0.fill_(float(eps))
+
+    def _refresh_current(self):
+        """After the surrogate changes, the gradient at the current points is
+        re-evaluated so that every trajectory uses one force field."""
+        if self.fallback:
+            self.data.logp_grad(self.s.theta, True, self.s.logp_cur, self.s.g_cur, self.work, self.err)
+            self.n_grad += 1
+        else:
+            self.sur.predict(self.s.theta, self.s.g_cur)
+
+    def iteration(self, learn=True):
+        s, d = self.s, self.data
+        check = learn and (self.it % self.train_every == 0)
+        s.begin()
+        for l in range(self.L):
+            last = l == self.L - 1
+            if self.fallback or (last and check):
+                d.logp_grad(s.theta, True, self.logp_new, self.g_exact, self.work, self.err)
+                self.n_grad += 1
+                if self.fallback:
+                    self.g_new.copy_(self.g_exact)
+                else:
+                    self.sur.predict(s.theta, self.g_new)
+            elif last:
+                d.logp_grad(s.theta, False, self.logp_new, None, self.work, self.err)
+                self.n_logp += 1
+                self.sur.predict(s.theta, self.g_new)
+            else:
+                self.sur.predict(s.theta, self.g_new)
+            if not last:
+                s.step(self.g_new)
+        if check:
+            # fresh exact pairs at the proposals: error check, then training
+            self.last_rel_err = self.sur.rel_error(s.theta, self.g_exact)
+            self.sur.add(s.theta, self.g_exact)
+        s.final(self.g_new, self.logp_new)
+        self.it += 1
+        if check:
+            self.fallback = not (self.last_rel_err <= self.max_rel_err)
+            if self.train_steps > 0:
+                self.sur.train(self.train_steps)
+            self._refresh_current()
+
+    def run(self, n=1, learn=True, record=None):
+        for _ in range(int(n)):
+            self.iteration(learn)
+            if record is not None:
+                record.append(self.s.theta.clone())
+
+    def accept_rate(self):
+        st = self.s.stats.cpu().numpy()
+        it = int(self.s.iter.item())
+        return st[:, 0].sum() / max(1, it * self.C), st[:, 1].sum() / max(1, it * self.C)
+
+    def reset_stats(self):
+        self.s.stats.zero_()
+        self.s.iter.zero_()

@@ -245,6 +245,100 @@ int ab_gmm_mwg(int N, int d, int K, int shared_cov, const float* Y, const int* z
                int compat, double* mu, uint64_t seed, uint32_t iter, uint32_t comp, int* accepts, void* stream);
 
 /* ======================================================================= *
+ * Batched HLR on the tensor cores: C chains against one data set.
+ * The reference evaluates one chain's block log density and gradient with
+ * its generated ll_/grad_ functions (compiler/augur/src/Comm/CgLike.hs:
+ * 139-147, CgGrad.hs:345-376) over augur_bernoulli_ll / augur_dotprod
+ * (cbits/augur_dist.c:59-71, cbits/augur_math.c:52-59,119-163); these entry
+ * points compute the same quantities for every chain in two bf16 tensor-core
+ * passes over the data (FP32-exact products by three-way bf16 splitting).
+ * The prior on each coefficient is Normal(0, prior_a) or Student-t with
+ * prior_a degrees of freedom and scale prior_b (no reference counterpart:
+ * the reference's modelling language has no Student-t).
+ * ======================================================================= */
+enum { AB_PRIOR_NORMAL = 0, AB_PRIOR_STUDENT_T = 1 };
+
+typedef struct ab_hlrb_model {
+  int N, D, ldx;        /* rows, features, row stride of X (multiple of 8)    */
+  const void* X;        /* bf16 [N][ldx], device                              */
+  const void* Xt;       /* bf16 [D][Np] from ab_hlrb_transpose, device        */
+  const int* y;         /* int32 [N] labels 0/1, device                       */
+  int prior;            /* AB_PRIOR_NORMAL or AB_PRIOR_STUDENT_T              */
+  double prior_a, prior_b;
+} ab_hlrb_model;
+
+/* Elements of the transposed copy Xt (D x Np, Np = N rounded up to 64). */
+size_t ab_hlrb_xt_elems(int N, int D);
+int ab_hlrb_transpose(int N, int D, const void* X, int ldx, void* Xt, void* stream);
+/* Device workspace (256-byte aligned) for ab_hlrb_logp_grad with C chains. */
+size_t ab_hlrb_workspace_bytes(int N, int D, int C);
+/* logp[c] (FP64) and, unless grad is NULL, grad[c][0..D-1] (FP32, row stride
+ * ldg) at theta[c][0..D-1] (FP32, row stride ldt), for c < C. */
+int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad,
+                      int ldg, void* work, int* err, void* stream);
+
+/* ======================================================================= *
+ * Batched HMC driver (h_augur_mcmc_hmc / h_augur_mcmc_leapfrog,
+ * cbits/augur_mcmclib.h:343-424, for C chains at once).  All pointers are
+ * device memory with row stride D; the caller evaluates the gradient (exact
+ * or surrogate) between the calls:
+ *   begin; { gradient at theta; step } x (L-1); exact logp + gradient; final
+ * ======================================================================= */
+typedef struct ab_hmcb_state {
+  int C, D;
+  unsigned long long seed;
+  long long* iter;      /* iteration counter, advanced by ab_hmcb_final       */
+  const float* eps0;    /* base step size                                     */
+  float jitter;         /* eps_c = eps0 * (1 + jitter * (2u - 1)), in [0, 1)  */
+  float* theta;         /* [C][D] current position                            */
+  float* p;             /* [C][D] momentum                                    */
+  float* g_cur;         /* [C][D] gradient used at the current position       */
+  double* logp_cur;     /* [C] exact log density at the current position      */
+  float* theta0;        /* [C][D] trajectory start (restored on reject)       */
+  float* g0;            /* [C][D]                                             */
+  double* logp0;        /* [C]                                                */
+  double* H0;           /* [C] starting energy                                */
+  float* eps_c;         /* [C] this iteration's step size                     */
+  double* stats;        /* [C][2] accepted count, summed acceptance prob.     */
+} ab_hmcb_state;
+
+int ab_hmcb_begin(const ab_hmcb_state* s, void* stream);
+int ab_hmcb_step(const ab_hmcb_state* s, const float* g, void* stream);
+int ab_hmcb_final(const ab_hmcb_state* s, const float* g_new, const double* logp_new, void* stream);
+
+/* ======================================================================= *
+ * Gradient-surrogate MLP (no counterpart in the reference): d_in -> h1 ->
+ * h2 -> d_out, GELU hidden layers, flat FP32 master parameters w with a bf16
+ * copy wb of the same layout [W1, b1, W2, b2, W3, b3]; forward passes use
+ * the bf16 weights with FP32 accumulation.
+ * ======================================================================= */
+typedef struct ab_mlp_desc {
+  int d_in, h1, h2, d_out;
+  float* w;             /* FP32 master parameters, device                     */
+  void* wb;             /* bf16 copy, device                                  */
+} ab_mlp_desc;
+
+size_t ab_mlp_param_count(int d_in, int h1, int h2, int d_out);
+/* activation buffer (P1, A1, P2, A2) for a batch of B rows, in floats */
+size_t ab_mlp_act_floats(int B, int h1, int h2);
+size_t ab_mlp_backward_scratch_floats(int B, int h1, int h2);
+int ab_mlp_forward(const ab_mlp_desc* d, int B, const float* x, int ldx, float* y, int ldy, float* act, void* stream);
+/* dy = 2 (y - target) / (B D) (row stride D); row_sq[b] = squared error of row b */
+int ab_mlp_mse(int B, int D, const float* y, int ldy, const float* target, int ldt, float* dy, double* row_sq,
+               void* stream);
+/* grad (flat, parameter layout) of the loss whose output gradient is dy */
+int ab_mlp_backward(const ab_mlp_desc* d, int B, const float* x, int ldx, const float* dy, const float* act,
+                    float* grad, float* scratch, void* stream);
+int ab_mlp_adam(const ab_mlp_desc* d, const float* grad, float* m, float* v, int step, float lr, float b1, float b2,
+                float eps, void* stream);
+int ab_mlp_sync_bf16(const ab_mlp_desc* d, void* stream);
+/* Surrogate input/output maps around the network, per coordinate d:
+ *   z = (theta - mu) * inv_s;   g = a + h (theta - mu) + o * out          */
+int ab_sur_pre(int C, int D, const float* theta, const float* mu, const float* inv_s, float* z, void* stream);
+int ab_sur_post(int C, int D, const float* theta, const float* out, const float* mu, const float* a, const float* h,
+                const float* o, float* g, void* stream);
+
+/* ======================================================================= *
  * Tensor-core building block (no counterpart in the reference, whose kernels
  * are scalar FP64): C[M][N] (f32, ldc) = A[M][K] * B[N][K]^T with A, B
  * row-major bf16, through tcgen05 MMAs fed by TMA.  splits > 1 splits K and

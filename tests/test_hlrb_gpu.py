@@ -1,0 +1,136 @@
+"""Batched HLR on the tensor cores against the FP64 oracle.
+
+Tolerances (written here, per the FP32 data-pass contract):
+  log density   |logp - logp64| <= 1e-5 * sum_n |term_n| (relative to the sum's scale)
+  gradient      |g - g64| <= 1e-5 * (|g64| + sum_n |r_n x_nd|) per coordinate
+Transitions: the same accept decisions as the FP64 oracle fed the same Philox
+draws, and end points within 1e-4 relative."""
+import numpy as np
+import pytest
+import torch
+
+from augurv2_b200 import hlrb as H
+from oracle import batched as B
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(N, D, seed, prior="student_t", scale=0.3):
+    rs = np.random.default_rng(seed)
+    X = torch.as_tensor(rs.standard_normal((N, D)), dtype=torch.float32).to(torch.bfloat16)
+    beta = rs.standard_normal(D) * scale
+    t = X.double().numpy() @ beta
+    y = (rs.random(N) < 1 / (1 + np.exp(-t))).astype(np.int32)
+    d = H.HlrbData(X, y, prior=prior, nu=3.0, scale=1.0, var=2.0)
+    return d, X.double().numpy(), y
+
+
+def _check(d, X64, y, theta):
+    th = torch.as_tensor(theta, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lp, g = d.logp_grad(th, err=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    lp64, g64, scale = B.hlr_logp_grad(X64, y, th.double().cpu().numpy(), d.prior, d.pa, d.pb)
+    t = th.double().cpu().numpy() @ X64.T
+    term_scale = (np.abs(y * t) + np.logaddexp(0, t)).sum(-1)
+    assert np.all(np.abs(lp.cpu().numpy() - lp64) <= 1e-5 * term_scale), np.max(np.abs(lp.cpu().numpy() - lp64) / term_scale)
+    gd = g.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(gd - g64) <= 1e-5 * (np.abs(g64) + scale)), np.max(np.abs(gd - g64) / (np.abs(g64) + scale))
+    # the log-density-only pass gives the same numbers
+    lp2, _ = d.logp_grad(th, grad=False)
+    np.testing.assert_array_equal(lp2.cpu().numpy(), lp.cpu().numpy())
+    return lp, g
+
+
+@pytest.mark.parametrize("N,D,C,prior", [(3000, 64, 40, "student_t"), (1000, 16, 3, "normal"),
+                                         (2500, 200, 130, "student_t"), (777, 520, 9, "normal"),
+                                         (64, 8, 1, "student_t"), (20000, 128, 256, "student_t")])
+def test_logp_grad_matches_fp64(N, D, C, prior):
+    d, X64, y = _data(N, D, seed=N + D + C, prior=prior)
+    rs = np.random.default_rng(C)
+    _check(d, X64, y, rs.standard_normal((C, D)) * 0.3)
+
+
+def test_deterministic_repeat():
+    d, X64, y = _data(5000, 96, seed=1)
+    th = torch.randn(50, 96, device="cuda") * 0.2
+    a = d.logp_grad(th)
+    b = d.logp_grad(th)
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+
+
+def test_full_size_against_fp64_on_device():
+    # N = 2,000,000 rows, D = 512, C = 256 chains: checked for 4 chains
+    # against an FP64 product of the same bf16 data on the device.
+    X, y, beta = H.synthetic(2_000_000, 512, seed=7)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    th = torch.as_tensor(beta, device="cuda").repeat(256, 1)
+    th += 0.01 * torch.randn(256, 512, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lp, g = d.logp_grad(th, err=err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    pick = [0, 77, 128, 255]
+    th64 = th[pick].double()
+    ll = torch.zeros(4, dtype=torch.float64, device="cuda")
+    gg = torch.zeros(4, 512, dtype=torch.float64, device="cuda")
+    sc = torch.zeros(4, 512, dtype=torch.float64, device="cuda")
+    tscale = torch.zeros(4, dtype=torch.float64, device="cuda")
+    for s in range(0, 2_000_000, 250_000):
+        xs = X[s:s + 250_000].double()
+        ys = y[s:s + 250_000].double()
+        t = xs @ th64.T
+        sp = torch.logaddexp(torch.zeros_like(t), t)
+        ll += (ys[:, None] * t - sp).sum(0)
+        tscale += (torch.abs(ys[:, None] * t) + sp).sum(0)
+        r = ys[:, None] - torch.sigmoid(t)
+        gg += r.T @ xs
+        sc += r.abs().T @ xs.abs()
+    pl, pg = B.prior_terms(th64.cpu().numpy(), 1, 3.0, 1.0)
+    ll = ll.cpu().numpy() + pl
+    gg = gg.cpu().numpy() + pg
+    sc = sc.cpu().numpy()
+    lpd = lp[pick].cpu().numpy()
+    gd = g[pick].double().cpu().numpy()
+    assert np.all(np.abs(lpd - ll) <= 1e-5 * tscale.cpu().numpy())
+    assert np.all(np.abs(gd - gg) <= 1e-5 * (np.abs(gg) + sc))
+
+
+def test_hmc_transitions_match_fp64_oracle():
+    o = O.Oracle("oracle")
+    d, X64, y = _data(600, 16, seed=11, prior="student_t")
+    C, L, eps, jit, seed = 6, 4, 0.05, 0.2, 9
+    rs = np.random.default_rng(3)
+    init = rs.standard_normal((C, 16)) * 0.2
+    hmc = H.BatchedHmc(d, C, L=L, eps=eps, jitter=jit, seed=seed, init=init)
+    th = hmc.theta.double().cpu().numpy()
+    lp64, g64, _ = B.hlr_logp_grad(X64, y, th, d.prior, d.pa, d.pb)
+    n_acc = 0
+    for it in range(4):
+        hmc.run(1)
+        th, g64, lp64, acc, dH = B.hmc_iteration(o, X64, y, th, g64, lp64, float(np.float32(eps)), float(np.float32(jit)),
+                                                 L, seed, it, d.prior, d.pa, d.pb)
+        n_acc += acc.sum()
+        got = hmc.theta.double().cpu().numpy()
+        np.testing.assert_allclose(got, th, rtol=1e-4, atol=1e-5)
+    st = hmc.s.stats.cpu().numpy()
+    assert int(st[:, 0].sum()) == n_acc
+    assert n_acc > 0
+
+
+def test_graph_replay_equals_eager():
+    d, X64, y = _data(4000, 64, seed=5)
+    init = np.random.default_rng(0).standard_normal((16, 64)) * 0.1
+    a = H.BatchedHmc(d, 16, L=3, eps=0.02, seed=4, init=init)
+    b = H.BatchedHmc(d, 16, L=3, eps=0.02, seed=4, init=init)
+    a.run(3)
+    b.capture()
+    b.s.iter.zero_()
+    b.s.theta.copy_(torch.as_tensor(init, dtype=torch.float32, device="cuda"))
+    b.s.stats.zero_()
+    d.logp_grad(b.s.theta, True, b.s.logp_cur, b.s.g_cur)
+    b.run(3)
+    torch.cuda.synchronize()
+    assert torch.equal(a.theta, b.theta)

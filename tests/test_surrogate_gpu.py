@@ -1,0 +1,95 @@
+"""The gradient-surrogate network: its device forward/backward against the
+FP64 oracle from the same bf16 weights, and what the trained network gains
+over the sampler without it."""
+import numpy as np
+import pytest
+import torch
+
+from augurv2_b200 import hlrb as H
+from augurv2_b200.diagnostics import ess
+from oracle import batched as B
+
+pytestmark = pytest.mark.gpu
+
+
+def test_mlp_forward_backward_match_fp64():
+    D, h1, h2, Bn = 512, 256, 256, 64
+    sur = H.MlpSurrogate(D, h1, h2, seed=3)
+    gen = torch.Generator("cuda").manual_seed(0)
+    x = torch.randn(Bn, D, device="cuda", generator=gen)
+    tgt = torch.randn(Bn, D, device="cuda", generator=gen)
+    sc = sur._scratch(Bn)
+    L = H.N.lib()
+    H.N.check(L.ab_mlp_forward(H.C.byref(sur.desc), Bn, H.N.ptr(x), D, H.N.ptr(sc["out"]), D, H.N.ptr(sc["act"]), None))
+    H.N.check(L.ab_mlp_mse(Bn, D, H.N.ptr(sc["out"]), D, H.N.ptr(tgt), D, H.N.ptr(sc["dy"]), H.N.ptr(sc["rsq"]), None))
+    H.N.check(L.ab_mlp_backward(H.C.byref(sur.desc), Bn, H.N.ptr(x), D, H.N.ptr(sc["dy"]), H.N.ptr(sc["act"]),
+                                H.N.ptr(sur.gw), H.N.ptr(sc["bsc"]), None))
+    torch.cuda.synchronize()
+    wmat = sur.wb.float().double().cpu().numpy()
+    wb = sur.w.double().cpu().numpy()
+    Y, _ = B.mlp_forward(wmat, wb, x.double().cpu().numpy(), D, h1, h2, D)
+    out = sc["out"].double().cpu().numpy()
+    assert np.max(np.abs(out - Y)) <= 1e-4 * max(1.0, np.max(np.abs(Y)))
+    loss, g = B.mlp_loss_grad(wmat, wb, x.double().cpu().numpy(), tgt.double().cpu().numpy(), D, h1, h2, D)
+    gd = sur.gw.double().cpu().numpy()
+    # FP32 accumulation against FP64: relative to the largest gradient entry of each block
+    n1, n2 = h1 * D, h2 * h1
+    offs = [0, n1, n1 + h1, n1 + h1 + n2, n1 + h1 + n2 + h2, n1 + h1 + n2 + h2 + D * h2, len(g)]
+    for a, b in zip(offs[:-1], offs[1:]):
+        s = np.max(np.abs(g[a:b]))
+        assert np.max(np.abs(gd[a:b] - g[a:b])) <= 1e-4 * s, (a, b)
+    assert abs(sc["rsq"].sum().item() / (Bn * D) - loss) <= 1e-5 * loss
+
+
+def test_training_reduces_loss():
+    D = 64
+    sur = H.MlpSurrogate(D, 128, 128, seed=1, batch=256, lr=2e-3)
+    gen = torch.Generator("cuda").manual_seed(2)
+    th = torch.randn(4096, D, device="cuda", generator=gen)
+    A = torch.randn(D, D, device="cuda", generator=gen) / D ** 0.5
+    g = -th @ A - 0.3 * torch.tanh(th)
+    sur.add(th, g)
+    sur.refit()
+    e0 = sur.rel_error(th[:512], g[:512])
+    sur.train(300)
+    e1 = sur.rel_error(th[:512], g[:512])
+    assert e1 < 0.5 * e0
+
+
+def _run(sampler, n, record):
+    draws = []
+    sampler.run(n, record=draws) if record else sampler.run(n)
+    return draws
+
+
+def test_surrogate_gains_over_plain_hmc():
+    # N = 100,000 rows, D = 64; 64 chains started at the generating
+    # coefficients; both samplers tuned to the same step size.  Cost is
+    # counted in exact data passes (a log-density-only pass counts one half
+    # of a gradient pass: it is the forward half).
+    N_, D, C = 100_000, 64, 64
+    X, y, beta = H.synthetic(N_, D, seed=3)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    init = np.asarray(beta, np.float32)[None] + 1e-3 * np.random.default_rng(0).standard_normal((C, D)).astype(np.float32)
+    eps, L = 0.004, 10
+    plain = H.BatchedHmc(d, C, L=L, eps=eps, jitter=0.1, seed=1, init=init)
+    plain.run(30)
+    plain.reset_stats()
+    rec_p = []
+    plain.run(120, record=rec_p)
+    ess_p = ess(torch.stack(rec_p).cpu().numpy()).min()
+    cost_p = 120 * L
+
+    sur = H.SurrogateHmc(d, C, L=L, eps=eps, jitter=0.1, seed=2, init=init, train_every=4, train_steps=40)
+    sur.run(60)                        # warm-up: collect pairs and train
+    sur.reset_stats()
+    g0, l0 = sur.n_grad, sur.n_logp
+    rec_s = []
+    sur.run(120, record=rec_s)
+    ess_s = ess(torch.stack(rec_s).cpu().numpy()).min()
+    cost_s = (sur.n_grad - g0) + 0.5 * (sur.n_logp - l0)
+    gain = (ess_s / cost_s) / (ess_p / cost_p)
+    print("plain ESS %.1f cost %d acc %s | surrogate ESS %.1f cost %.1f acc %s err %.3f fallback %s gain %.2f" % (
+        ess_p, cost_p, plain.accept_rate(), ess_s, cost_s, sur.accept_rate(), sur.last_rel_err, sur.fallback, gain))
+    assert not sur.fallback
+    assert gain > 2.0
