@@ -170,16 +170,20 @@ class BatchedHmc:
         s.final(self.g_new, self.logp_new, stream)
 
     def capture(self):
-        """Capture one iteration (L exact passes) as a CUDA graph."""
+        """Capture one iteration (L exact passes) as a CUDA graph; the chain
+        state is left as it was."""
+        keep = (self.s.theta, self.s.g_cur, self.s.logp_cur, self.s.stats, self.s.iter)
+        saved = [t.clone() for t in keep]
         side = torch.cuda.Stream(device=self.data.device)
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
-            self._iteration(side)          # warm (sets kernel attributes outside capture)
+            self._iteration(side)          # warm-up launch outside capture
         torch.cuda.current_stream().wait_stream(side)
         self.graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(self.graph):
             self._iteration(torch.cuda.current_stream())
-        self.n_grad += self.L
+        for t, v in zip(keep, saved):
+            t.copy_(v)
 
     def run(self, n=1, record=None):
         for _ in range(int(n)):
@@ -417,9 +421,41 @@ class SurrogateHmc:
                 self.sur.train(self.train_steps)
             self._refresh_current()
 
+    def _plain_iteration(self, stream=None):
+        """A surrogate trajectory without the exact gradient check."""
+        s, d = self.s, self.data
+        s.begin(stream)
+        for l in range(self.L):
+            if l == self.L - 1:
+                d.logp_grad(s.theta, False, self.logp_new, None, self.work, self.err, stream)
+            self.sur.predict(s.theta, self.g_new, stream)
+            if l < self.L - 1:
+                s.step(self.g_new, stream)
+        s.final(self.g_new, self.logp_new, stream)
+
+    def capture(self):
+        """Capture a surrogate trajectory (no check, no training) as a CUDA graph."""
+        side = torch.cuda.Stream(device=self.data.device)
+        side.wait_stream(torch.cuda.current_stream())
+        saved = [t.clone() for t in (self.s.theta, self.s.g_cur, self.s.logp_cur, self.s.stats, self.s.iter)]
+        with torch.cuda.stream(side):
+            self._plain_iteration(side)      # warm-up launch outside capture
+        torch.cuda.current_stream().wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._plain_iteration(torch.cuda.current_stream())
+        for t, v in zip((self.s.theta, self.s.g_cur, self.s.logp_cur, self.s.stats, self.s.iter), saved):
+            t.copy_(v)
+
     def run(self, n=1, learn=True, record=None):
         for _ in range(int(n)):
-            self.iteration(learn)
+            check = learn and (self.it % self.train_every == 0)
+            if (not check) and (not self.fallback) and getattr(self, "graph", None) is not None:
+                self.graph.replay()
+                self.n_logp += 1
+                self.it += 1
+            else:
+                self.iteration(learn)
             if record is not None:
                 record.append(self.s.theta.clone())
 
@@ -431,3 +467,18 @@ class SurrogateHmc:
     def reset_stats(self):
         self.s.stats.zero_()
         self.s.iter.zero_()
+
+
+def adapt_step_size(sampler, n, target=0.8, rate=1.5, lo=1e-6, hi=10.0, run_kw=None):
+    """Warm-up: after each iteration multiply the base step size by
+    exp(rate * (mean acceptance probability - target)).  Returns the final
+    step size."""
+    run_kw = run_kw or {}
+    eps = float(sampler.s.eps0.item())
+    for _ in range(int(n)):
+        before = sampler.s.stats[:, 1].sum().item()
+        sampler.run(1, **run_kw)
+        a = (sampler.s.stats[:, 1].sum().item() - before) / sampler.C
+        eps = float(min(hi, max(lo, eps * math.exp(rate * (a - target)))))
+        sampler.set_eps(eps)
+    return eps

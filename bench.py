@@ -7,6 +7,13 @@ One step = one augur_step of the schedule
 ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z].
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload lda|hlr_surrogate]
+
+The default line also carries, under "hlr_surrogate", the surrogate-gradient
+HMC measurement on HLR (N=2,000,000 rows, D=512, X ~ N(0,1) stored bf16,
+beta ~ Student-t(3), 256 chains, L=10): min-ESS/s of the learned sampler and
+of plain exact-gradient HMC on the same GPU, and their ratio
+(`--workload hlr_surrogate` prints that measurement as its own line).
 
 N > 1 (launched by torch.distributed.run) runs one independent chain per GPU
 (replicas; LDA chains share nothing), value = all tokens / max-over-ranks time.
@@ -108,6 +115,150 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def measured_tensor_peak(sustained=False):
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    key = "bf16_tflops_sustained" if sustained else "bf16_tflops"
+    if os.path.exists(p):
+        d = json.load(open(p))
+        if key in d:
+            return d[key], "measured"
+    return (1400.0 if sustained else 1590.0), "fallback"
+
+
+HLR_N, HLR_D, HLR_C, HLR_L, HLR_SEED = 2_000_000, 512, 256, 10, 5
+
+
+def run_hlr_pass(n_rows, steps, warmup):
+    """Exact batched HLR passes alone (log density + gradient for 256 chains
+    at D=512 over n_rows bf16 rows): device time per pass and tensor-pipe
+    throughput."""
+    import torch
+    from augurv2_b200 import hlrb as H
+    X, y, beta = H.synthetic(n_rows, HLR_D, seed=HLR_SEED)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    th = torch.as_tensor(beta, device="cuda").repeat(HLR_C, 1).contiguous()
+    work = d.workspace(HLR_C)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    out = {}
+    for grad in (False, True):
+        for _ in range(warmup):
+            d.logp_grad(th, grad, work=work, err=err)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            d.logp_grad(th, grad, work=work, err=err)
+        e1.record()
+        torch.cuda.synchronize()
+        out["grad" if grad else "logp"] = e0.elapsed_time(e1) / steps
+    if int(err.item()) != 0:
+        raise RuntimeError("device wait timed out in the HLR pass")
+    fwd = 2.0 * 3 * n_rows * HLR_D * HLR_C
+    peak, kind = measured_tensor_peak(sustained=False)
+    return {"metric": "batched HLR exact pass (logp + grad, 256 chains)", "value": out["grad"], "unit": "ms",
+            "higher_is_better": False, "logp_only_ms": out["logp"],
+            "tflops": {"forward": fwd / (out["logp"] / 1e3) / 1e12, "forward+backward": 2 * fwd / (out["grad"] / 1e3) / 1e12},
+            "peak": peak, "peak_source": kind,
+            "config": {"workload": "hlr_pass_n%d_d%d_c%d" % (n_rows, HLR_D, HLR_C), "N": n_rows, "D": HLR_D,
+                       "chains": HLR_C}}
+
+
+def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
+    """Surrogate-gradient HMC vs plain exact-gradient HMC on the same data,
+    chains, step-size rule and iteration count; min-ESS/s of each (ESS over
+    all D coefficients, Geyer initial monotone, 256 chains), device time by
+    CUDA events around every iteration (Python gaps included)."""
+    import torch
+    from augurv2_b200 import hlrb as H
+    from augurv2_b200.diagnostics import ess
+
+    X, y, beta = H.synthetic(HLR_N, HLR_D, seed=HLR_SEED)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    rs = np.random.default_rng(HLR_SEED)
+    init = np.asarray(beta, np.float32)[None] + 1e-3 * rs.standard_normal((HLR_C, HLR_D)).astype(np.float32)
+
+    # exact pass timing (forward = log density only; forward + backward)
+    th = torch.as_tensor(init, device="cuda")
+    work = d.workspace(HLR_C)
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    pass_ms = {}
+    for grad in (False, True):
+        for _ in range(3):
+            d.logp_grad(th, grad, work=work, err=err)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            d.logp_grad(th, grad, work=work, err=err)
+        e1.record()
+        torch.cuda.synchronize()
+        pass_ms["grad" if grad else "logp"] = e0.elapsed_time(e1) / 10
+    fwd_flops = 2.0 * 3 * HLR_N * HLR_D * HLR_C
+    peak, peak_kind = measured_tensor_peak(sustained=True)
+    ach = 2 * fwd_flops / (pass_ms["grad"] / 1e3) / 1e12
+
+    def timed(sampler, n):
+        rec = torch.empty((n, HLR_C, HLR_D), dtype=torch.float32, device="cuda")
+        ms = 0.0
+        for i in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            sampler.run(1)
+            b.record()
+            rec[i].copy_(sampler.theta)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+        return rec, ms
+
+    plain = H.BatchedHmc(d, HLR_C, L=HLR_L, eps=2e-4, jitter=0.1, seed=11, init=init)
+    eps = H.adapt_step_size(plain, warm)
+    plain.capture()
+    plain.reset_stats()
+    rec_p, ms_p = timed(plain, iters)
+    draws_p = rec_p.cpu().numpy()
+    ess_p = ess(draws_p)
+    acc_p = plain.accept_rate()[0]
+    del plain
+
+    sur = H.SurrogateHmc(d, HLR_C, L=HLR_L, eps=eps, jitter=0.1, seed=12, init=init, train_every=4,
+                         train_steps=20)
+    sur.run(sur_warm)
+    H.adapt_step_size(sur, warm // 2)
+    sur.capture()
+    sur.reset_stats()
+    g0, l0 = sur.n_grad, sur.n_logp
+    rec_s, ms_s = timed(sur, iters)
+    draws_s = rec_s.cpu().numpy()
+    ess_s = ess(draws_s)
+    acc_s = sur.accept_rate()[0]
+
+    # posterior moments: both chains target the same posterior
+    mp, ms_ = draws_p.reshape(-1, HLR_D).mean(0), draws_s.reshape(-1, HLR_D).mean(0)
+    sd = draws_p.reshape(-1, HLR_D).std(0)
+    z = (ms_ - mp) / np.sqrt(sd ** 2 / ess_p + sd ** 2 / ess_s)
+    v_p = ess_p.min() / (ms_p / 1e3)
+    v_s = ess_s.min() / (ms_s / 1e3)
+    return {
+        "metric": "min-ESS/sec (surrogate-gradient HMC, HLR)", "value": v_s, "unit": "min-ESS/s",
+        "plain_hmc_value": v_p, "gain_vs_plain": v_s / v_p,
+        "iterations": iters, "chains": HLR_C, "leapfrog_steps": HLR_L, "step_size": eps,
+        "ms_per_iteration": {"surrogate": ms_s / iters, "plain": ms_p / iters},
+        "min_ess": {"surrogate": float(ess_s.min()), "plain": float(ess_p.min())},
+        "accept": {"surrogate": float(acc_s), "plain": float(acc_p)},
+        "surrogate_rel_err": sur.last_rel_err, "fallback": sur.fallback,
+        "exact_passes": {"grad": sur.n_grad - g0, "logp_only": sur.n_logp - l0, "plain_grad": iters * HLR_L},
+        "posterior_mean_diff_in_sd": float(np.max(np.abs(ms_ - mp) / sd)),
+        "posterior_mean_z_max": float(np.max(np.abs(z))),
+        "exact_pass_ms": pass_ms,
+        "roofline": {"bound": "tensor", "kernel": "gemm_kernel (forward + backward data passes)",
+                     "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                     "peak_source": peak_kind + " (sustained)",
+                     "algorithmic_flops_per_pass": 2 * fwd_flops,
+                     "note": "2 x 3 x 2 N D C: three bf16 parts of the FP32 operand, forward and backward"},
+        "config": {"workload": "hlr_surrogate_n2000000_d512_c256", "N": HLR_N, "D": HLR_D, "chains": HLR_C,
+                   "x_dtype": "bf16", "prior": "student_t(3)", "mlp": "512-256-256-512 gelu, bf16 weights",
+                   "init": "generating coefficients + N(0, 1e-6)", "warmup": warm, "surrogate_warmup": sur_warm},
+    }
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from augurv2_b200 import _native as N
@@ -186,6 +337,11 @@ def run_ours(args, rank, world, local_rank):
         }
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(off, w, budget_s=args.cpu_seconds)
+        if world == 1 and not args.no_secondary:
+            try:
+                line["hlr_surrogate"] = run_hlr_surrogate(iters=args.hlr_iters)
+            except Exception as e:   # the LDA line stands on its own
+                line["hlr_surrogate"] = {"error": repr(e)[:300]}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -312,6 +468,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-secondary", action="store_true", help="skip the surrogate HLR measurement")
+    ap.add_argument("--workload", default="lda", choices=["lda", "hlr_surrogate", "hlr_pass"])
+    ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
+    ap.add_argument("--hlr-iters", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", 0))
@@ -319,6 +479,18 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
+    elif args.workload == "hlr_pass":
+        import torch
+        torch.cuda.set_device(local_rank)
+        line = run_hlr_pass(args.hlr_n, args.steps, args.warmup) if rank == 0 else None
+    elif args.workload == "hlr_surrogate":
+        import torch
+        torch.cuda.set_device(local_rank)
+        line = run_hlr_surrogate(iters=args.hlr_iters) if rank == 0 else None
+        if line is not None:
+            line.update({"n_gpus": 1, "steps": args.hlr_iters, "warmup": 30, "higher_is_better": True,
+                         "scaling": "weak", "vs_baseline": None, "dtype": "bf16 x3 parts, f32 accum, f64 energy",
+                         "data": "synthetic (X ~ N(0,1) bf16, beta ~ Student-t(3), seed 5)"})
     else:
         line = run_ours(args, rank, world, local_rank)
     if rank == 0 and line is not None:
