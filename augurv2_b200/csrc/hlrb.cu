@@ -13,15 +13,21 @@
 //   forward  T^T[C x N] = Theta3[C x 3D] . X[N x D]^T   (theta split hi+mid+lo
 //            into bf16, so the FP32 product is exact to FP32 rounding); the
 //            epilogue turns each t into its log-likelihood term (summed per
-//            chain and 256-row tile, Kahan-compensated) and the residual
-//            r = y - sigmoid(t), stored as three bf16 parts R3[C][3][Np];
-//   backward G[C x D] = R3[C x 3Np] . Xt[D x Np]^T, split over rows into
+//            chain, 128-row tile and column group, Kahan-compensated) and the
+//            residual r = y - sigmoid(t), stored as three bf16 parts;
+//   backward G[C x D] = sum_p R_p[C x N] . Xt[D x N]^T, split over rows into
 //            deterministic FP32 partial tiles;
 //   finish   one block per chain: FP64 sums of the per-tile log-likelihood
 //            partials and of the gradient partials in a fixed order, plus
 //            the FP64 prior and its gradient.
-// X is bf16 [N][ldx]; Xt is its transpose [D][Np] with Np = N rounded up to
-// 64 and zero padding, built once by ab_hlrb_transpose.
+// X is bf16 [N][ldx].  The backward operands are stored K-blocked so that
+// every 128 x 64 tile the tensor memory accelerator fetches is one
+// contiguous 16 KB box (row-major [rows][N] tiles would touch 128 rows that
+// lie megabytes apart):
+//   Xt  [Np/64][D][64]     the transpose of X in 64-row blocks, zero padded
+//                          (Np = N rounded up to 64), built once by
+//                          ab_hlrb_transpose;
+//   R3  [Np/64][3][C][64]  the residual parts, written by the forward pass.
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -33,6 +39,8 @@ namespace ab {
 namespace {
 
 constexpr int FWD_BN = 128;   // data rows per forward tile
+constexpr int FWD_WARPS = 8;  // epilogue warps of the forward pass (two column groups)
+constexpr int FWD_GROUPS = FWD_WARPS / 4;
 constexpr int BWD_BN = 128;   // gradient columns per backward tile
 
 inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
@@ -63,7 +71,7 @@ Layout layout(int N, int D, int C) {
   L.off_r3 = o;
   o = align256(o + (size_t)C * 3 * L.Np * 2);
   L.off_ll = o;
-  o = align256(o + (size_t)L.fwd_tiles * C * 4);
+  o = align256(o + (size_t)L.fwd_tiles * FWD_GROUPS * C * 4);
   L.off_w = o;
   o = align256(o + (size_t)L.splits * C * L.ldw * 4);
   L.total = o;
@@ -96,7 +104,8 @@ __global__ void hlrb_split_kernel(int C, int D, int Dp, const float* __restrict_
   }
 }
 
-// X [N][ldx] -> Xt [D][Np], zero for n >= N.  32x32 tiles through shared memory.
+// X [N][ldx] -> Xt [Np/64][D][64], zero for n >= N.  32x32 tiles through
+// shared memory.
 __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16* __restrict__ X, int ldx,
                                       __nv_bfloat16* __restrict__ Xt) {
   __shared__ __nv_bfloat16 tile[32][33];
@@ -109,16 +118,17 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
   __syncthreads();
   for (int j = ty; j < 32; j += 8) {
     const int d = d0 + j, n = n0 + tx;
-    if (d < D && n < Np) Xt[(size_t)d * Np + n] = tile[tx][j];
+    if (d < D && n < Np) Xt[((size_t)(n >> 6) * D + d) * 64 + (n & 63)] = tile[tx][j];
   }
 }
 
 // Forward epilogue: rows are chains, columns are data rows.
 struct FwdEpi {
   static constexpr int kSmem = FWD_BN * 4;
+  static constexpr int kWarps = FWD_WARPS;
   const int* y;
   __nv_bfloat16* r3;   // NULL: log density only
-  float* llpart;       // [fwd_tiles][C]
+  float* llpart;       // [fwd_tiles][FWD_GROUPS][C]
   int N, Np, C;
   // per-thread state
   const int* ys;
@@ -128,7 +138,7 @@ struct FwdEpi {
   __device__ void begin(int, int nt, int, char* smem, int etid) {
     int* s = reinterpret_cast<int*>(smem);
     n0 = nt * FWD_BN;
-    for (int j = etid; j < FWD_BN; j += 128) {
+    for (int j = etid; j < FWD_BN; j += 32 * FWD_WARPS) {
       const int n = n0 + j;
       s[j] = n < N ? y[n] : -1;
     }
@@ -149,7 +159,7 @@ struct FwdEpi {
         const float e = expf(-fabsf(t));
         const float sp = fmaxf(t, 0.0f) + log1pf(e);   // softplus(t)
         term = yv ? t - sp : -sp;
-        const float inv = __frcp_rn(1.0f + e);
+        const float inv = __fdividef(1.0f, 1.0f + e);   // 1/(1+e), 1+e in (1, 2]
         const float sig = t >= 0.0f ? inv : e * inv;
         r = (float)yv - sig;
         // Kahan-compensated running sum of this chain's terms
@@ -161,7 +171,8 @@ struct FwdEpi {
       rv[i] = r;
     }
     if (r3 && col0 < Np) {
-      __nv_bfloat16* base = r3 + (size_t)c * 3 * Np + col0;
+      // K-blocked [Np/64][3][C][64]: part p of chain c for rows col0..col0+31
+      __nv_bfloat16* base = r3 + ((size_t)(col0 >> 6) * 3 * C + c) * 64 + (col0 & 63);
       uint32_t ph[16], pm[16], pl[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
@@ -173,8 +184,8 @@ struct FwdEpi {
         pl[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
       }
       uint4* dh = reinterpret_cast<uint4*>(base);
-      uint4* dm = reinterpret_cast<uint4*>(base + Np);
-      uint4* dl = reinterpret_cast<uint4*>(base + 2 * (size_t)Np);
+      uint4* dm = reinterpret_cast<uint4*>(base + (size_t)C * 64);
+      uint4* dl = reinterpret_cast<uint4*>(base + (size_t)2 * C * 64);
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         dh[i] = make_uint4(ph[4 * i], ph[4 * i + 1], ph[4 * i + 2], ph[4 * i + 3]);
@@ -184,8 +195,8 @@ struct FwdEpi {
     }
   }
 
-  __device__ void end(int, int nt, int, int c, bool ok) {
-    if (ok) llpart[(size_t)nt * C + c] = acc;
+  __device__ void end(int, int nt, int, int c, bool ok, int cg) {
+    if (ok) llpart[((size_t)nt * FWD_GROUPS + cg) * C + c] = acc;
   }
 };
 
@@ -193,6 +204,7 @@ struct FwdEpi {
 // tile per split.
 struct GradEpi {
   static constexpr int kSmem = 0;
+  static constexpr int kWarps = 4;
   float* w;   // [splits][C][ldw]
   int C, D, ldw;
   int sp;
@@ -206,7 +218,7 @@ struct GradEpi {
       for (int i = 0; i < 8; ++i) o4[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
     }
   }
-  __device__ void end(int, int, int, int, bool) {}
+  __device__ void end(int, int, int, int, bool, int) {}
 };
 
 __device__ __forceinline__ void prior_term(int kind, double a, double b, double x, double& ll, double& g) {
@@ -269,18 +281,19 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
   if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
   FwdEpi fe{m->y, grad ? r3 : nullptr, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
-  const tc::Shape fs = tc::make_shape(C, N, D, 1, L.Dp, 0, FWD_BN);
+  const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), FWD_BN);
   if ((rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st))) return rc;
 
   if (grad) {
-    if ((rc = tc::encode_2d_bf16(&ma, r3, C, 3 * L.Np, 3 * L.Np, tc::BM))) return rc;
-    if ((rc = tc::encode_2d_bf16(&mb, m->Xt, D, L.Np, L.Np, BWD_BN))) return rc;
+    const int nb = L.Np / 64;
+    if ((rc = tc::encode_2d_bf16(&ma, r3, (uint64_t)nb * 3 * C, 64, 64, tc::BM))) return rc;
+    if ((rc = tc::encode_2d_bf16(&mb, m->Xt, (uint64_t)nb * D, 64, 64, BWD_BN))) return rc;
     GradEpi ge{w, C, D, L.ldw, 0};
-    const tc::Shape bs = tc::make_shape(C, D, N, L.splits, L.Np, 0, BWD_BN);
+    const tc::Shape bs = tc::make_shape(C, D, N, L.splits, tc::k_blocked(3, C), tc::k_blocked(1, D), BWD_BN);
     AB_REQUIRE(bs.splits == L.splits, AB_ERR_STATE, "hlrb: split arithmetic mismatch");
     if ((rc = tc::launch_gemm<BWD_BN, 3, 1>(ma, mb, bs, ge, err, st))) return rc;
   }
-  hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
+  hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles * FWD_GROUPS, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
                                         m->prior_a, m->prior_b, logp, grad, ldg);
   AB_LAUNCH_CHECK("hlrb_finish_kernel");
   return AB_OK;

@@ -57,6 +57,7 @@ int encode_2d_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t co
 // C (fp32, ldc) = A B^T, optionally split-K with atomic accumulation.
 struct StoreEpi {
   static constexpr int kSmem = 0;
+  static constexpr int kWarps = 4;
   float* C;
   int M, N, ldc;
   int atomic;
@@ -73,7 +74,7 @@ struct StoreEpi {
       }
     }
   }
-  __device__ void end(int, int, int, int, bool) {}
+  __device__ void end(int, int, int, int, bool, int) {}
 };
 
 }  // namespace tc
@@ -93,7 +94,7 @@ extern "C" int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, cons
   const int BN = N >= 256 ? 256 : (N > 64 ? 128 : 64);
   rc = encode_2d_bf16(&tb, B, N, K, ldb, BN);
   if (rc) return rc;
-  const Shape sh = make_shape(M, N, K, splits, 0, 0, BN);
+  const Shape sh = make_shape(M, N, K, splits, row_major(0), row_major(0), BN);
   StoreEpi epi{C, M, N, ldc, sh.splits > 1};
   cudaStream_t st = as_stream(stream);
   if (sh.splits > 1) AB_CUDA(cudaMemsetAsync(C, 0, sizeof(float) * (size_t)M * ldc, st));

@@ -4,10 +4,16 @@
 //   C[M x N] = sum_p A_p[M x K] * B_p[N x K]^T     A, B bf16, row-major (K-major)
 //
 // "Parts" let one operand be a sum of bf16 slices of an FP32 matrix: with
-// PA = 3 the A operand is hi + mid + lo (three K-ranges of the same rows,
-// a_pstride elements apart) and B is shared by the three products, so an
-// FP32 matrix times a bf16 matrix is computed to FP32 accuracy on the bf16
-// tensor pipe.  At most one of PA, PB is above 1.
+// PA = 3 the A operand is hi + mid + lo and B is shared by the three
+// products, so an FP32 matrix times a bf16 matrix is computed to FP32
+// accuracy on the bf16 tensor pipe.  At most one of PA, PB is above 1.
+//
+// Where each 64-wide K step of an operand lives is given by an Addr: the
+// tensor-map coordinate of (K step kb, part p, tile start r) is
+//   x = kb * x_kb + p * x_p,   y = r + kb * y_kb + p * y_p.
+// Row-major [rows][K] operands use x_kb = 64 (parts x_p elements apart);
+// K-blocked operands ([K/64][parts][rows][64], one contiguous 16 KB box per
+// tile) use x = 0 and y_kb, y_p row offsets.
 //
 // Persistent kernel: one CTA per SM walks the 128 x BN output tiles
 // (tile = blockIdx.x + i * gridDim.x; tile -> (m fastest, n, split)).
@@ -18,9 +24,11 @@
 //                  N = BN, K = 16) into one of two FP32 accumulators in
 //                  tensor memory, so the next tile's MMAs overlap the
 //                  previous tile's epilogue;
-//   warps 2..5     epilogue: warp w reads TMEM lanes 32(w%4)..+31 (one output
-//                  row per thread) 32 columns at a time with tcgen05.ld and
-//                  hands them to the epilogue functor.
+//   warps 2..      epilogue (Epi::kWarps warps, a multiple of 4): warp w reads
+//                  TMEM lanes 32(w%4)..+31 (one output row per thread); the
+//                  kWarps/4 warps of one lane quarter split the columns into
+//                  groups; 32 columns at a time come out with tcgen05.ld and
+//                  go to the epilogue functor.
 // Every mbarrier wait is bounded (clock-based); on expiry the kernel records
 // AB_ERR_TIMEOUT in *err, stops issuing, waits (bounded) for its outstanding
 // copies and MMAs, frees its tensor memory and returns.
@@ -35,7 +43,8 @@ namespace tc {
 
 constexpr int BM = 128;
 constexpr int BK = 64;                      // 64 bf16 = one 128-byte swizzle row
-constexpr int THREADS = 192;
+// threads of a launch whose epilogue has `epi_warps` warps (a multiple of 4)
+__host__ __device__ constexpr int threads_for(int epi_warps) { return 64 + 32 * epi_warps; }
 constexpr long long WAIT_CYCLES = 4000000000LL;   // ~2 s at 2 GHz
 constexpr int SMEM_BUDGET = 232448;                // 227 KB opt-in per block
 
@@ -110,8 +119,8 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Named barrier over the four epilogue warps.
-__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+// Named barrier over the epilogue warps.
+__device__ __forceinline__ void epi_sync(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
 
 // 32 consecutive fp32 columns of this warp's 32 TMEM lanes.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
@@ -130,14 +139,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+struct Addr {
+  int x_kb, x_p, y_kb, y_p;
+};
+
 // Problem shape as the kernel sees it.  K is the reduction length of one
-// part; part p of A starts a_pstride elements after part 0 (likewise B).
-// Each split covers k_split elements of K (a multiple of BK); the host makes
-// every split non-empty.
+// part.  Each split covers k_split elements of K (a multiple of BK); the
+// host makes every split non-empty.
 struct Shape {
   int M, N, K;
   int k_split;
-  int a_pstride, b_pstride;
+  Addr a, b;
   int m_tiles, n_tiles, splits;
 };
 
@@ -160,16 +172,17 @@ struct Cfg {
   static constexpr int SMEM_BYTES = EPI_OFFSET + EPI_SMEM + 1024;
 };
 
-// The kernel.  Epi must provide (called by the 128 epilogue threads only;
-// etid = 0..127, row = this thread's output row):
-//   static constexpr int kSmem;
+// The kernel.  Epi must provide (called by the epilogue threads only;
+// etid = 0..32*kWarps-1, row = this thread's output row, cg = its column
+// group, 0..kWarps/4-1):
+//   static constexpr int kSmem, kWarps;
 //   __device__ void begin(int m_tile, int n_tile, int split, char* smem, int etid);
 //   __device__ void rows(int row, int col0, const float* v32, bool row_ok);
-//   __device__ void end(int m_tile, int n_tile, int split, int row, bool row_ok);
+//   __device__ void end(int m_tile, int n_tile, int split, int row, bool row_ok, int cg);
 // begin() may fill shared memory; a named barrier over the epilogue warps
 // separates begin() from rows() and end() from the next tile's begin().
 template <int BN, int PA, int PB, class Epi>
-__global__ void __launch_bounds__(THREADS, 1)
+__global__ void __launch_bounds__(threads_for(Epi::kWarps), 1)
 gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, Shape sh, Epi epi,
             int* __restrict__ err) {
   using C = Cfg<BN, PA, PB, Epi::kSmem>;
@@ -193,7 +206,7 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < C::STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
-    for (int b = 0; b < 2; ++b) { mbar_init(&acc_full[b], 1); mbar_init(&acc_empty[b], 4); }
+    for (int b = 0; b < 2; ++b) { mbar_init(&acc_full[b], 1); mbar_init(&acc_empty[b], Epi::kWarps); }
     mbar_init(drain, 1);
     *fail = 0;
     *epi_fail = 0;
@@ -227,10 +240,12 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
           mbar_expect_tx(&full[s], C::STAGE_BYTES);
 #pragma unroll
           for (int p = 0; p < PA; ++p)
-            tma_load_2d(a + p * C::A_BYTES, &ta, &full[s], kb * BK + p * sh.a_pstride, mt * BM);
+            tma_load_2d(a + p * C::A_BYTES, &ta, &full[s], kb * sh.a.x_kb + p * sh.a.x_p,
+                        mt * BM + kb * sh.a.y_kb + p * sh.a.y_p);
 #pragma unroll
           for (int p = 0; p < PB; ++p)
-            tma_load_2d(b + p * C::B_BYTES, &tb, &full[s], kb * BK + p * sh.b_pstride, nt * BN);
+            tma_load_2d(b + p * C::B_BYTES, &tb, &full[s], kb * sh.b.x_kb + p * sh.b.x_p,
+                        nt * BN + kb * sh.b.y_kb + p * sh.b.y_p);
           ++issued;
         }
       }
@@ -275,8 +290,14 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
       if (!mbar_wait(drain, 0)) *fail = 1;
     }
   } else {
-    // epilogue warps 2..5
+    // epilogue warps 2 .. 2+kWarps-1
+    constexpr int EW = Epi::kWarps;
+    static_assert(EW % 4 == 0 && EW >= 4, "epilogue warps: a multiple of 4");
+    constexpr int GROUPS = EW / 4;
+    static_assert(BN % (32 * GROUPS) == 0, "column groups of whole 32-column chunks");
+    constexpr int GCOLS = BN / GROUPS;
     const int q = warp & 3;                 // TMEM lane quarter this warp may access
+    const int cg = (warp - 2) >> 2;         // column group
     const int etid = (warp - 2) * 32 + lane;
     Epi e(epi);                             // per-thread copy: functors may keep running sums
     int i = 0;
@@ -285,14 +306,14 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
       const int kb0 = sp * kb_per_split, kb1 = min(kb_all, kb0 + kb_per_split);
       const int ab = i & 1;
       e.begin(mt, nt, sp, epi_smem, etid);
-      epi_sync();
+      epi_sync(32 * EW);
       // warp-uniform: tcgen05.ld is a warp-collective instruction
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&acc_full[ab], (i >> 1) & 1));
       fence_after();
       const bool have = __all_sync(0xffffffffu, ok && kb1 > kb0 && !*(volatile int*)fail);
       const int row = mt * BM + q * 32 + lane;
       const bool row_ok = row < sh.M;
-      for (int c0 = 0; c0 < BN; c0 += 32) {
+      for (int c0 = cg * GCOLS; c0 < (cg + 1) * GCOLS; c0 += 32) {
         float v[32];
         if (have) {
           tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * C::ACC_COLS + c0), v);
@@ -305,9 +326,9 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
       fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[ab]);
-      e.end(mt, nt, sp, row, row_ok);
+      e.end(mt, nt, sp, row, row_ok, cg);
       if (!ok || *(volatile int*)fail) { *fail = 1; *(volatile int*)epi_fail = 1; }
-      epi_sync();
+      epi_sync(32 * EW);
       // uniform across the epilogue warps: written only before the barrier
       if (*(volatile int*)epi_fail) break;
     }

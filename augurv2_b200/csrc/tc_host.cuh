@@ -14,8 +14,13 @@ int encode_2d_bf16(CUtensorMap* map, const void* ptr, uint64_t rows, uint64_t co
 // Number of SMs of the current device (cached per device).
 int sm_count();
 
+// Operand addressing: row-major [rows][K] with parts `pstride` elements
+// apart, or K-blocked [K/64][parts][blk_rows][64].
+inline Addr row_major(int pstride) { return Addr{BK, pstride, 0, 0}; }
+inline Addr k_blocked(int parts, int blk_rows) { return Addr{0, 0, parts * blk_rows, blk_rows}; }
+
 // Shape with K split into at most `splits` non-empty ranges of whole K steps.
-inline Shape make_shape(int M, int N, int K, int splits, int a_pstride, int b_pstride, int bn) {
+inline Shape make_shape(int M, int N, int K, int splits, Addr a, Addr b, int bn) {
   Shape s;
   s.M = M;
   s.N = N;
@@ -26,8 +31,8 @@ inline Shape make_shape(int M, int N, int K, int splits, int a_pstride, int b_ps
   const int per = (kb_all + splits - 1) / splits;
   s.k_split = per * BK;
   s.splits = (kb_all + per - 1) / per;
-  s.a_pstride = a_pstride;
-  s.b_pstride = b_pstride;
+  s.a = a;
+  s.b = b;
   s.m_tiles = (M + BM - 1) / BM;
   s.n_tiles = (N + bn - 1) / bn;
   return s;
@@ -43,7 +48,7 @@ int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, const Shape& sh, c
   const long long total = (long long)sh.m_tiles * sh.n_tiles * sh.splits;
   AB_REQUIRE(total > 0 && total < (1LL << 31), AB_ERR_ARG, "GEMM tile count out of range");
   const int grid = (int)(total < sm_count() ? total : sm_count());
-  gemm_kernel<BN, PA, PB, Epi><<<grid, THREADS, C::SMEM_BYTES, st>>>(ta, tb, sh, epi, err);
+  gemm_kernel<BN, PA, PB, Epi><<<grid, threads_for(Epi::kWarps), C::SMEM_BYTES, st>>>(ta, tb, sh, epi, err);
   AB_LAUNCH_CHECK("tc gemm_kernel");
   return AB_OK;
 }

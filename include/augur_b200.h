@@ -261,13 +261,14 @@ enum { AB_PRIOR_NORMAL = 0, AB_PRIOR_STUDENT_T = 1 };
 typedef struct ab_hlrb_model {
   int N, D, ldx;        /* rows, features, row stride of X (multiple of 8)    */
   const void* X;        /* bf16 [N][ldx], device                              */
-  const void* Xt;       /* bf16 [D][Np] from ab_hlrb_transpose, device        */
+  const void* Xt;       /* bf16 [Np/64][D][64] from ab_hlrb_transpose, device */
   const int* y;         /* int32 [N] labels 0/1, device                       */
   int prior;            /* AB_PRIOR_NORMAL or AB_PRIOR_STUDENT_T              */
   double prior_a, prior_b;
 } ab_hlrb_model;
 
-/* Elements of the transposed copy Xt (D x Np, Np = N rounded up to 64). */
+/* Elements of the transposed copy Xt: D x Np (Np = N rounded up to 64),
+ * stored in 64-row blocks [Np/64][D][64]. */
 size_t ab_hlrb_xt_elems(int N, int D);
 int ab_hlrb_transpose(int N, int D, const void* X, int ldx, void* Xt, void* stream);
 /* Device workspace (256-byte aligned) for ab_hlrb_logp_grad with C chains. */
