@@ -97,6 +97,7 @@ _SIGS = {
     "ab_mlp_adam": (i32, [vp, vp, vp, vp, i32, f32, f32, f32, f32, vp]),
     "ab_mlp_sync_bf16": (i32, [vp, vp]),
     "ab_sur_pre": (i32, [i32, i32, vp, vp, vp, vp, vp]),
+    "ab_sur_predict": (i32, [vp, i32, vp, i32, vp, vp, vp, vp, vp, vp, i32, vp]),
     "ab_sur_post": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
     # tensor-core GEMM core
     "ab_tc_gemm_bf16": (i32, [i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp, vp]),

@@ -122,7 +122,10 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
   }
 }
 
-// Forward epilogue: rows are chains, columns are data rows.
+// Forward epilogue: rows are chains, columns are data rows.  LL: sum the
+// log-likelihood terms; R: write the residual parts for the backward pass
+// (a leapfrog step that only needs the gradient skips the LL work).
+template <bool LL, bool R>
 struct FwdEpi {
   static constexpr int kSmem = FWD_BN * 4;
   static constexpr int kWarps = FWD_WARPS;
@@ -154,23 +157,27 @@ struct FwdEpi {
     for (int i = 0; i < 32; ++i) {
       const int yv = ys[col0 - n0 + i];
       const float t = v[i];
-      float term = 0.0f, r = 0.0f;
+      float r = 0.0f;
       if (yv >= 0) {
         const float e = expf(-fabsf(t));
-        const float sp = fmaxf(t, 0.0f) + log1pf(e);   // softplus(t)
-        term = yv ? t - sp : -sp;
-        const float inv = __fdividef(1.0f, 1.0f + e);   // 1/(1+e), 1+e in (1, 2]
-        const float sig = t >= 0.0f ? inv : e * inv;
-        r = (float)yv - sig;
-        // Kahan-compensated running sum of this chain's terms
-        const float yk = term - comp;
-        const float tk = acc + yk;
-        comp = (tk - acc) - yk;
-        acc = tk;
+        if (LL) {
+          const float sp = fmaxf(t, 0.0f) + log1pf(e);   // softplus(t)
+          const float term = yv ? t - sp : -sp;
+          // Kahan-compensated running sum of this chain's terms
+          const float yk = term - comp;
+          const float tk = acc + yk;
+          comp = (tk - acc) - yk;
+          acc = tk;
+        }
+        if (R) {
+          const float inv = __fdividef(1.0f, 1.0f + e);   // 1/(1+e), 1+e in (1, 2]
+          const float sig = t >= 0.0f ? inv : e * inv;
+          r = (float)yv - sig;
+        }
       }
       rv[i] = r;
     }
-    if (r3 && col0 < Np) {
+    if (R && col0 < Np) {
       // K-blocked [Np/64][3][C][64]: part p of chain c for rows col0..col0+31
       __nv_bfloat16* base = r3 + ((size_t)(col0 >> 6) * 3 * C + c) * 64 + (col0 & 63);
       uint32_t ph[16], pm[16], pl[16];
@@ -196,7 +203,7 @@ struct FwdEpi {
   }
 
   __device__ void end(int, int nt, int, int c, bool ok, int cg) {
-    if (ok) llpart[((size_t)nt * FWD_GROUPS + cg) * C + c] = acc;
+    if (LL && ok) llpart[((size_t)nt * FWD_GROUPS + cg) * C + c] = acc;
   }
 };
 
@@ -236,7 +243,7 @@ __device__ __forceinline__ void prior_term(int kind, double a, double b, double 
 }
 
 // One block per chain: logp[c] (FP64) and grad[c][0..D-1] (FP32) from the
-// partials, in a fixed order.
+// partials, in a fixed order; either output may be NULL.
 __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_tiles, int splits, int ldw,
                                                           const float* __restrict__ llpart,
                                                           const float* __restrict__ w, const float* __restrict__ theta,
@@ -246,7 +253,8 @@ __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_
   __shared__ double red[33];
   const int c = blockIdx.x;
   double s = 0.0;
-  for (int t = threadIdx.x; t < fwd_tiles; t += blockDim.x) s += (double)llpart[(size_t)t * C + c];
+  if (logp)
+    for (int t = threadIdx.x; t < fwd_tiles; t += blockDim.x) s += (double)llpart[(size_t)t * C + c];
   for (int d = threadIdx.x; d < D; d += blockDim.x) {
     double pl, pg;
     prior_term(prior, pa, pb, (double)theta[(size_t)c * ldt + d], pl, pg);
@@ -258,7 +266,7 @@ __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_
     }
   }
   s = block_sum_f64(s, red);
-  if (threadIdx.x == 0) logp[c] = s;
+  if (logp && threadIdx.x == 0) logp[c] = s;
 }
 
 }  // namespace
@@ -280,9 +288,18 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   CUtensorMap ma, mb;
   if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
   if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
-  FwdEpi fe{m->y, grad ? r3 : nullptr, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
   const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), FWD_BN);
-  if ((rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st))) return rc;
+  if (logp && grad) {
+    FwdEpi<true, true> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
+    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  } else if (logp) {
+    FwdEpi<true, false> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
+    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  } else {
+    FwdEpi<false, true> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
+    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  }
+  if (rc) return rc;
 
   if (grad) {
     const int nb = L.Np / 64;
@@ -341,7 +358,7 @@ extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* the
   int rc = hlrb_check_model(m);
   if (rc) return rc;
   AB_REQUIRE(C > 0 && C <= 65535, AB_ERR_ARG, "ab_hlrb_logp_grad: C must be 1..65535");
-  AB_REQUIRE(theta && logp && work, AB_ERR_ARG, "ab_hlrb_logp_grad: null pointer");
+  AB_REQUIRE(theta && work && (logp || grad), AB_ERR_ARG, "ab_hlrb_logp_grad: null pointer");
   AB_REQUIRE(ldt >= m->D && (!grad || ldg >= m->D), AB_ERR_ARG, "ab_hlrb_logp_grad: leading dimension too small");
   AB_REQUIRE((reinterpret_cast<uintptr_t>(work) & 255) == 0, AB_ERR_ARG, "ab_hlrb_logp_grad: workspace must be 256-byte aligned");
   return hlrb_logp_grad(m, C, theta, ldt, logp, grad, ldg, work, err, as_stream(stream));

@@ -12,7 +12,8 @@
 // small beside the exact HLR pass.
 //
 //   forward   P1 = X W1^T + b1, A1 = gelu(P1), P2 = A1 W2^T + b2,
-//             A2 = gelu(P2), Y = A2 W3^T + b3
+//             A2 = gelu(P2), Y = A2 W3^T + b3 — one fused launch, a few rows
+//             per block with the activations in shared memory
 //   loss      mean squared error against a target, dY = 2 (Y - T) / (B d_out)
 //   backward  dW3 = dY^T A2, db3 = colsum dY, dP2 = (dY W3) . gelu'(P2), ...
 //   Adam      on the master vector, refreshing the bf16 copy.
@@ -54,14 +55,16 @@ __global__ void __launch_bounds__(256) mlp_gemm_kernel(int M, int N, int K, cons
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  // consecutive threads walk the operand's unit-stride dimension
+  const bool a_k_unit = sak == 1, b_k_unit = sbk == 1;
   for (int k0 = 0; k0 < K; k0 += TK) {
     for (int e = threadIdx.x; e < TK * TM; e += 256) {
-      const int kk = e / TM, mm = e % TM;
+      const int kk = a_k_unit ? e % TK : e / TM, mm = a_k_unit ? e / TK : e % TM;
       const int m = m0 + mm, k = k0 + kk;
       As[kk][mm] = (m < M && k < K) ? A[(size_t)m * sam + (size_t)k * sak] : 0.0f;
     }
     for (int e = threadIdx.x; e < TK * TN; e += 256) {
-      const int kk = e / TN, nn = e % TN;
+      const int kk = b_k_unit ? e % TK : e / TN, nn = b_k_unit ? e / TK : e % TN;
       const int n = n0 + nn, k = k0 + kk;
       Bs[kk][nn] = (n < N && k < K) ? ld(B + (size_t)k * sbk + (size_t)n * sbn) : 0.0f;
     }
@@ -169,6 +172,145 @@ __global__ void sur_post_kernel(int C, int D, const float* __restrict__ theta, c
   }
 }
 
+// One dense layer for G rows held in shared memory: out[g][j] = act(b[j] +
+// sum_k W[j][k] in[g][k]).  One output feature j per thread: the thread
+// walks its bf16 weight row in 16-byte pieces (consecutive pieces share a
+// cache line) and reads the G input rows as shared-memory broadcasts, so no
+// cross-lane reduction is needed and the sum order is fixed.
+template <int G>
+__device__ __forceinline__ void dense_layer(const float* __restrict__ in, int din, const __nv_bfloat16* __restrict__ W,
+                                            const float* __restrict__ b, int dout, float* __restrict__ out,
+                                            float* __restrict__ pre, bool gelu_act) {
+  for (int j = threadIdx.x; j < dout; j += blockDim.x) {
+    float acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0.0f;
+    const uint4* row = reinterpret_cast<const uint4*>(W + (size_t)j * din);
+    const int n8 = din >> 3;
+#pragma unroll 4
+    for (int k8 = 0; k8 < n8; ++k8) {
+      const uint4 raw = __ldg(row + k8);
+      const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&raw);
+      float wv[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float2 f = __bfloat1622float2(h2[i]);
+        wv[2 * i] = f.x;
+        wv[2 * i + 1] = f.y;
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        const float4 x0 = *reinterpret_cast<const float4*>(in + g * din + 8 * k8);
+        const float4 x1 = *reinterpret_cast<const float4*>(in + g * din + 8 * k8 + 4);
+        acc[g] = fmaf(wv[0], x0.x, acc[g]);
+        acc[g] = fmaf(wv[1], x0.y, acc[g]);
+        acc[g] = fmaf(wv[2], x0.z, acc[g]);
+        acc[g] = fmaf(wv[3], x0.w, acc[g]);
+        acc[g] = fmaf(wv[4], x1.x, acc[g]);
+        acc[g] = fmaf(wv[5], x1.y, acc[g]);
+        acc[g] = fmaf(wv[6], x1.z, acc[g]);
+        acc[g] = fmaf(wv[7], x1.w, acc[g]);
+      }
+    }
+    const float bj = b[j];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const float v = acc[g] + bj;
+      if (pre) pre[g * dout + j] = v;
+      out[g * dout + j] = gelu_act ? gelu(v) : v;
+    }
+  }
+}
+
+// The whole network for G rows per block.  SUR: input theta with the
+// surrogate's input map z = (theta - mu) * inv_s, output the gradient
+// estimate a + h (theta - mu) + o * y; otherwise input x, output y, and the
+// activations (P1, A1, P2, A2 by rows) saved for the backward pass when act
+// is not NULL.
+template <int G, bool SUR>
+__global__ void __launch_bounds__(256) mlp_fused_kernel(int B, int din, int h1, int h2, int dout,
+                                                        const float* __restrict__ x, int ldx,
+                                                        const __nv_bfloat16* __restrict__ wb,
+                                                        const float* __restrict__ w, float* __restrict__ y, int ldy,
+                                                        float* __restrict__ act, const float* __restrict__ mu,
+                                                        const float* __restrict__ inv_s, const float* __restrict__ sa,
+                                                        const float* __restrict__ sh, const float* __restrict__ so) {
+  extern __shared__ float sm[];
+  float* z = sm;                       // [G][din]
+  float* a1 = z + G * din;             // [G][h1]
+  float* a2 = a1 + G * h1;             // [G][h2]
+  float* p1 = a2 + G * h2;             // [G][h1]
+  float* p2 = p1 + G * h1;             // [G][h2]
+  float* o3 = p2 + G * h2;             // [G][dout]
+  const int r0 = blockIdx.x * G;
+  const size_t ow1 = 0, ob1 = (size_t)h1 * din, ow2 = ob1 + h1, ob2 = ow2 + (size_t)h2 * h1, ow3 = ob2 + h2,
+               ob3 = ow3 + (size_t)dout * h2;
+  for (int i = threadIdx.x; i < G * din; i += blockDim.x) {
+    const int g = i / din, k = i % din, r = r0 + g;
+    float v = 0.0f;
+    if (r < B) {
+      v = x[(size_t)r * ldx + k];
+      if (SUR) v = (v - mu[k]) * inv_s[k];
+    }
+    z[i] = v;
+  }
+  __syncthreads();
+  const bool save = !SUR && act;
+  dense_layer<G>(z, din, wb + ow1, w + ob1, h1, a1, save ? p1 : nullptr, true);
+  __syncthreads();
+  dense_layer<G>(a1, h1, wb + ow2, w + ob2, h2, a2, save ? p2 : nullptr, true);
+  __syncthreads();
+  dense_layer<G>(a2, h2, wb + ow3, w + ob3, dout, o3, nullptr, false);
+  __syncthreads();
+  for (int i = threadIdx.x; i < G * dout; i += blockDim.x) {
+    const int g = i / dout, j = i % dout, r = r0 + g;
+    if (r >= B) continue;
+    float v = o3[i];
+    if (SUR) {
+      const float th = x[(size_t)r * ldx + j];
+      v = sa[j] + sh[j] * (th - mu[j]) + so[j] * v;
+    }
+    y[(size_t)r * ldy + j] = v;
+  }
+  if (save) {
+    float* P1 = act;
+    float* A1 = P1 + (size_t)B * h1;
+    float* P2 = A1 + (size_t)B * h1;
+    float* A2 = P2 + (size_t)B * h2;
+    for (int i = threadIdx.x; i < G * h1; i += blockDim.x) {
+      const int g = i / h1, j = i % h1, r = r0 + g;
+      if (r < B) {
+        P1[(size_t)r * h1 + j] = p1[i];
+        A1[(size_t)r * h1 + j] = a1[i];
+      }
+    }
+    for (int i = threadIdx.x; i < G * h2; i += blockDim.x) {
+      const int g = i / h2, j = i % h2, r = r0 + g;
+      if (r < B) {
+        P2[(size_t)r * h2 + j] = p2[i];
+        A2[(size_t)r * h2 + j] = a2[i];
+      }
+    }
+  }
+}
+
+constexpr int FUSED_G = 4;
+
+template <bool SUR>
+int launch_fused(const ab_mlp_desc* d, int B, const float* x, int ldx, float* y, int ldy, float* act,
+                 const float* mu, const float* inv_s, const float* a, const float* h, const float* o,
+                 cudaStream_t st) {
+  const size_t smem = sizeof(float) * FUSED_G * ((size_t)d->d_in + 2 * d->h1 + 2 * d->h2 + d->d_out);
+  AB_REQUIRE(smem <= 200 * 1024, AB_ERR_ARG, "mlp: layers too wide for the fused kernel");
+  AB_CUDA(cudaFuncSetAttribute(mlp_fused_kernel<FUSED_G, SUR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+  mlp_fused_kernel<FUSED_G, SUR><<<ceil_div(B, FUSED_G), 256, smem, st>>>(
+      B, d->d_in, d->h1, d->h2, d->d_out, x, ldx, static_cast<const __nv_bfloat16*>(d->wb), d->w, y, ldy, act, mu,
+      inv_s, a, h, o);
+  AB_LAUNCH_CHECK("mlp_fused_kernel");
+  return AB_OK;
+}
+
 struct Offsets {
   size_t w1, b1, w2, b2, w3, b3, total;
 };
@@ -198,6 +340,9 @@ int gemm(int M, int N, int K, const float* A, int sam, int sak, const TB* B, int
 int check(const ab_mlp_desc* d) {
   AB_REQUIRE(d, AB_ERR_ARG, "mlp: null descriptor");
   AB_REQUIRE(d->d_in > 0 && d->h1 > 0 && d->h2 > 0 && d->d_out > 0, AB_ERR_ARG, "mlp: bad layer sizes");
+  AB_REQUIRE(d->d_in % 8 == 0 && d->h1 % 8 == 0 && d->h2 % 8 == 0 && d->d_out % 8 == 0, AB_ERR_ARG,
+             "mlp: layer widths must be multiples of 8");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(d->wb) & 15) == 0, AB_ERR_ARG, "mlp: bf16 weights must be 16-byte aligned");
   AB_REQUIRE(d->w && d->wb, AB_ERR_ARG, "mlp: null parameters");
   return AB_OK;
 }
@@ -221,23 +366,21 @@ extern "C" int ab_mlp_forward(const ab_mlp_desc* d, int B, const float* x, int l
                               void* stream) {
   int rc = check(d);
   if (rc) return rc;
-  AB_REQUIRE(B > 0 && x && y && act && ldx >= d->d_in && ldy >= d->d_out, AB_ERR_ARG, "ab_mlp_forward: bad arguments");
-  const Offsets o = offsets(d);
-  const __nv_bfloat16* wb = static_cast<const __nv_bfloat16*>(d->wb);
-  const float* w = d->w;
-  cudaStream_t st = as_stream(stream);
-  float* P1 = act;
-  float* A1 = P1 + (size_t)B * d->h1;
-  float* P2 = A1 + (size_t)B * d->h1;
-  float* A2 = P2 + (size_t)B * d->h2;
-  if ((rc = gemm<__nv_bfloat16, EPI_GELU>(B, d->h1, d->d_in, x, ldx, 1, wb + o.w1, 1, d->d_in, w + o.b1, P1, d->h1,
-                                          A1, nullptr, 0, st)))
-    return rc;
-  if ((rc = gemm<__nv_bfloat16, EPI_GELU>(B, d->h2, d->h1, A1, d->h1, 1, wb + o.w2, 1, d->h1, w + o.b2, P2, d->h2,
-                                          A2, nullptr, 0, st)))
-    return rc;
-  return gemm<__nv_bfloat16, EPI_STORE>(B, d->d_out, d->h2, A2, d->h2, 1, wb + o.w3, 1, d->h2, w + o.b3, y, ldy,
-                                        nullptr, nullptr, 0, st);
+  AB_REQUIRE(B > 0 && x && y && ldx >= d->d_in && ldy >= d->d_out && ldx % 4 == 0, AB_ERR_ARG,
+             "ab_mlp_forward: bad arguments");
+  return launch_fused<false>(d, B, x, ldx, y, ldy, act, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             as_stream(stream));
+}
+
+extern "C" int ab_sur_predict(const ab_mlp_desc* d, int C, const float* theta, int ldt, const float* mu,
+                              const float* inv_s, const float* a, const float* h, const float* o, float* g, int ldg,
+                              void* stream) {
+  int rc = check(d);
+  if (rc) return rc;
+  AB_REQUIRE(d->d_in == d->d_out, AB_ERR_ARG, "ab_sur_predict: the network must map D to D");
+  AB_REQUIRE(C > 0 && theta && mu && inv_s && a && h && o && g && ldt >= d->d_in && ldg >= d->d_out, AB_ERR_ARG,
+             "ab_sur_predict: bad arguments");
+  return launch_fused<true>(d, C, theta, ldt, g, ldg, nullptr, mu, inv_s, a, h, o, as_stream(stream));
 }
 
 extern "C" int ab_mlp_mse(int B, int D, const float* y, int ldy, const float* target, int ldt, float* dy,

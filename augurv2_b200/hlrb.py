@@ -69,20 +69,25 @@ class HlrbData:
         nb = int(N.lib().ab_hlrb_workspace_bytes(self.N, self.D, C_))
         return torch.empty(nb, dtype=torch.uint8, device=self.device)
 
-    def logp_grad(self, theta, grad=True, logp_out=None, grad_out=None, work=None, err=None, stream=None):
-        """(logp [C] f64, grad [C, D] f32 or None) at theta [C, D] f32 (device)."""
+    def logp_grad(self, theta, grad=True, logp_out=None, grad_out=None, work=None, err=None, stream=None,
+                  logp=True):
+        """(logp [C] f64 or None, grad [C, D] f32 or None) at theta [C, D] f32
+        (device); logp=False skips the log-likelihood terms."""
         C_ = theta.shape[0]
-        if logp_out is None:
+        if not (grad or logp):
+            raise ValueError("nothing to compute")
+        if logp and logp_out is None:
             logp_out = torch.empty(C_, dtype=torch.float64, device=self.device)
         if grad and grad_out is None:
             grad_out = torch.empty((C_, self.D), dtype=torch.float32, device=self.device)
         if work is None:
             work = self.workspace(C_)
-        N.check(N.lib().ab_hlrb_logp_grad(C.byref(self.c), C_, N.ptr(theta), theta.stride(0), N.ptr(logp_out),
+        N.check(N.lib().ab_hlrb_logp_grad(C.byref(self.c), C_, N.ptr(theta), theta.stride(0),
+                                          N.ptr(logp_out) if logp else None,
                                           N.ptr(grad_out) if grad else None, self.D, N.ptr(work),
                                           N.ptr(err) if err is not None else None, N.stream_ptr(stream)),
                 "ab_hlrb_logp_grad")
-        return logp_out, (grad_out if grad else None)
+        return (logp_out if logp else None), (grad_out if grad else None)
 
 
 def synthetic(N_, D, seed=0, nu=3.0, device="cuda", chunk=1 << 18):
@@ -164,8 +169,10 @@ class BatchedHmc:
         s, d = self.s, self.data
         s.begin(stream)
         for l in range(self.L):
-            d.logp_grad(s.theta, True, self.logp_new, self.g_new, self.work, self.err, stream)
-            if l < self.L - 1:
+            last = l == self.L - 1
+            # the log density is needed only at the end point
+            d.logp_grad(s.theta, True, self.logp_new, self.g_new, self.work, self.err, stream, logp=last)
+            if not last:
                 s.step(self.g_new, stream)
         s.final(self.g_new, self.logp_new, stream)
 
@@ -290,8 +297,13 @@ class MlpSurrogate:
 
     def predict(self, theta, out_grad, stream=None):
         B = theta.shape[0]
-        sc = self._scratch(B)
         L, st = N.lib(), N.stream_ptr(stream)
+        if self.use_net:
+            N.check(L.ab_sur_predict(C.byref(self.desc), B, N.ptr(theta), theta.stride(0), N.ptr(self.mu),
+                                     N.ptr(self.inv_s), N.ptr(self.a), N.ptr(self.h), N.ptr(self.o),
+                                     N.ptr(out_grad), out_grad.stride(0), st), "ab_sur_predict")
+            return out_grad
+        sc = self._scratch(B)
         N.check(L.ab_sur_pre(B, self.D, N.ptr(theta), N.ptr(self.mu), N.ptr(self.inv_s), N.ptr(sc["z"]), st),
                 "ab_sur_pre")
         if self.use_net:
@@ -305,31 +317,37 @@ class MlpSurrogate:
 
     def train(self, steps):
         """Adam steps on minibatches of the replay buffer; returns the last
-        minibatch's mean squared error in output units."""
+        minibatch's mean squared error in output units.  The minibatches of
+        all steps are gathered and standardised in one pass."""
         if self.n_buf == 0 or not self.use_net:
             return float("nan")
+        steps = int(steps)
         B = min(self.batch, self.n_buf)
         sc = self._scratch(B)
+        key = ("train", steps, B)
+        if key not in self._bufs:
+            self._bufs[key] = (torch.empty((steps * B, self.D), dtype=torch.float32, device=self.device),
+                               torch.empty((steps * B, self.D), dtype=torch.float32, device=self.device))
+        zs, ts = self._bufs[key]
+        idx = torch.randint(0, self.n_buf, (steps * B,), generator=self.gen, device=self.device)
+        dt = torch.index_select(self.buf_theta, 0, idx).sub_(self.mu)
+        torch.mul(dt, self.inv_s, out=zs)
+        g = torch.index_select(self.buf_grad, 0, idx)
+        torch.div(g.sub_(self.a).sub_(dt.mul_(self.h)), self.o, out=ts)
         L, st = N.lib(), N.stream_ptr()
-        loss = None
-        for _ in range(int(steps)):
-            idx = torch.randint(0, self.n_buf, (B,), generator=self.gen, device=self.device)
-            th = self.buf_theta[idx]
-            g = self.buf_grad[idx]
-            dt = th - self.mu
-            torch.mul(dt, self.inv_s, out=sc["z"])
-            torch.div(g - self.a - self.h * dt, self.o, out=sc["tgt"])
-            N.check(L.ab_mlp_forward(C.byref(self.desc), B, N.ptr(sc["z"]), self.D, N.ptr(sc["out"]), self.D,
+        esz = zs.element_size() * B * self.D
+        for i in range(steps):
+            zp, tp = zs.data_ptr() + i * esz, ts.data_ptr() + i * esz
+            N.check(L.ab_mlp_forward(C.byref(self.desc), B, zp, self.D, N.ptr(sc["out"]), self.D,
                                      N.ptr(sc["act"]), st), "ab_mlp_forward")
-            N.check(L.ab_mlp_mse(B, self.D, N.ptr(sc["out"]), self.D, N.ptr(sc["tgt"]), self.D, N.ptr(sc["dy"]),
+            N.check(L.ab_mlp_mse(B, self.D, N.ptr(sc["out"]), self.D, tp, self.D, N.ptr(sc["dy"]),
                                  N.ptr(sc["rsq"]), st), "ab_mlp_mse")
-            N.check(L.ab_mlp_backward(C.byref(self.desc), B, N.ptr(sc["z"]), self.D, N.ptr(sc["dy"]),
+            N.check(L.ab_mlp_backward(C.byref(self.desc), B, zp, self.D, N.ptr(sc["dy"]),
                                       N.ptr(sc["act"]), N.ptr(self.gw), N.ptr(sc["bsc"]), st), "ab_mlp_backward")
             self.step_count += 1
             N.check(L.ab_mlp_adam(C.byref(self.desc), N.ptr(self.gw), N.ptr(self.m), N.ptr(self.v),
                                   self.step_count, self.lr, 0.9, 0.999, 1e-8, st), "ab_mlp_adam")
-            loss = sc["rsq"]
-        return float(loss.sum().item()) / (B * self.D)
+        return float(sc["rsq"].sum().item()) / (B * self.D)
 
     def rel_error(self, theta, grad):
         """Relative error |g_hat - g| / |g| (Frobenius) on given pairs."""
@@ -395,7 +413,7 @@ class SurrogateHmc:
         for l in range(self.L):
             last = l == self.L - 1
             if self.fallback or (last and check):
-                d.logp_grad(s.theta, True, self.logp_new, self.g_exact, self.work, self.err)
+                d.logp_grad(s.theta, True, self.logp_new, self.g_exact, self.work, self.err, logp=last)
                 self.n_grad += 1
                 if self.fallback:
                     self.g_new.copy_(self.g_exact)

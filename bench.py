@@ -162,7 +162,7 @@ def run_hlr_pass(n_rows, steps, warmup):
                        "chains": HLR_C}}
 
 
-def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
+def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_steps=10):
     """Surrogate-gradient HMC vs plain exact-gradient HMC on the same data,
     chains, step-size rule and iteration count; min-ESS/s of each (ESS over
     all D coefficients, Geyer initial monotone, 256 chains), device time by
@@ -210,6 +210,7 @@ def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
 
     plain = H.BatchedHmc(d, HLR_C, L=HLR_L, eps=2e-4, jitter=0.1, seed=11, init=init)
     eps = H.adapt_step_size(plain, warm)
+    init = plain.theta.cpu().numpy()      # both measured runs start from the warmed-up chains
     plain.capture()
     plain.reset_stats()
     rec_p, ms_p = timed(plain, iters)
@@ -218,8 +219,8 @@ def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
     acc_p = plain.accept_rate()[0]
     del plain
 
-    sur = H.SurrogateHmc(d, HLR_C, L=HLR_L, eps=eps, jitter=0.1, seed=12, init=init, train_every=4,
-                         train_steps=20)
+    sur = H.SurrogateHmc(d, HLR_C, L=HLR_L, eps=eps, jitter=0.1, seed=12, init=init, train_every=train_every,
+                         train_steps=train_steps)
     sur.run(sur_warm)
     H.adapt_step_size(sur, warm // 2)
     sur.capture()
@@ -247,6 +248,7 @@ def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
         "exact_passes": {"grad": sur.n_grad - g0, "logp_only": sur.n_logp - l0, "plain_grad": iters * HLR_L},
         "posterior_mean_diff_in_sd": float(np.max(np.abs(ms_ - mp) / sd)),
         "posterior_mean_z_max": float(np.max(np.abs(z))),
+        "posterior_mean_mc_sd": float(np.median(np.sqrt(1.0 / ess_p + 1.0 / ess_s))),
         "exact_pass_ms": pass_ms,
         "roofline": {"bound": "tensor", "kernel": "gemm_kernel (forward + backward data passes)",
                      "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
@@ -255,7 +257,9 @@ def run_hlr_surrogate(iters=100, warm=30, sur_warm=60):
                      "note": "2 x 3 x 2 N D C: three bf16 parts of the FP32 operand, forward and backward"},
         "config": {"workload": "hlr_surrogate_n2000000_d512_c256", "N": HLR_N, "D": HLR_D, "chains": HLR_C,
                    "x_dtype": "bf16", "prior": "student_t(3)", "mlp": "512-256-256-512 gelu, bf16 weights",
-                   "init": "generating coefficients + N(0, 1e-6)", "warmup": warm, "surrogate_warmup": sur_warm},
+                   "init": "generating coefficients + N(0, 1e-6), then the plain sampler's warm-up",
+                   "warmup": warm, "surrogate_warmup": sur_warm,
+                   "train_every": train_every, "train_steps": train_steps},
     }
 
 
@@ -339,7 +343,8 @@ def run_ours(args, rank, world, local_rank):
             line["cpu_baseline"] = cpu_baseline(off, w, budget_s=args.cpu_seconds)
         if world == 1 and not args.no_secondary:
             try:
-                line["hlr_surrogate"] = run_hlr_surrogate(iters=args.hlr_iters)
+                line["hlr_surrogate"] = run_hlr_surrogate(iters=args.hlr_iters, train_every=args.train_every,
+                                                          train_steps=args.train_steps)
             except Exception as e:   # the LDA line stands on its own
                 line["hlr_surrogate"] = {"error": repr(e)[:300]}
     if dist:
@@ -472,6 +477,8 @@ def main():
     ap.add_argument("--workload", default="lda", choices=["lda", "hlr_surrogate", "hlr_pass"])
     ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
     ap.add_argument("--hlr-iters", type=int, default=100)
+    ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
+    ap.add_argument("--train-steps", type=int, default=10, help="surrogate: Adam steps per check")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", 0))
@@ -486,7 +493,8 @@ def main():
     elif args.workload == "hlr_surrogate":
         import torch
         torch.cuda.set_device(local_rank)
-        line = run_hlr_surrogate(iters=args.hlr_iters) if rank == 0 else None
+        line = run_hlr_surrogate(iters=args.hlr_iters, train_every=args.train_every,
+                                 train_steps=args.train_steps) if rank == 0 else None
         if line is not None:
             line.update({"n_gpus": 1, "steps": args.hlr_iters, "warmup": 30, "higher_is_better": True,
                          "scaling": "weak", "vs_baseline": None, "dtype": "bf16 x3 parts, f32 accum, f64 energy",

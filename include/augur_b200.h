@@ -273,8 +273,10 @@ size_t ab_hlrb_xt_elems(int N, int D);
 int ab_hlrb_transpose(int N, int D, const void* X, int ldx, void* Xt, void* stream);
 /* Device workspace (256-byte aligned) for ab_hlrb_logp_grad with C chains. */
 size_t ab_hlrb_workspace_bytes(int N, int D, int C);
-/* logp[c] (FP64) and, unless grad is NULL, grad[c][0..D-1] (FP32, row stride
- * ldg) at theta[c][0..D-1] (FP32, row stride ldt), for c < C. */
+/* logp[c] (FP64) and grad[c][0..D-1] (FP32, row stride ldg) at
+ * theta[c][0..D-1] (FP32, row stride ldt), for c < C.  Either output may be
+ * NULL (not both): a NULL logp skips the log-likelihood terms (a leapfrog
+ * step needs only the gradient), a NULL grad skips the backward pass. */
 int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad,
                       int ldg, void* work, int* err, void* stream);
 
@@ -333,6 +335,10 @@ int ab_mlp_backward(const ab_mlp_desc* d, int B, const float* x, int ldx, const 
 int ab_mlp_adam(const ab_mlp_desc* d, const float* grad, float* m, float* v, int step, float lr, float b1, float b2,
                 float eps, void* stream);
 int ab_mlp_sync_bf16(const ab_mlp_desc* d, void* stream);
+/* The surrogate in one launch: g = a + h (theta - mu) + o * MLP((theta - mu) * inv_s),
+ * per coordinate, for C rows (d_in == d_out == D). */
+int ab_sur_predict(const ab_mlp_desc* d, int C, const float* theta, int ldt, const float* mu, const float* inv_s,
+                   const float* a, const float* h, const float* o, float* g, int ldg, void* stream);
 /* Surrogate input/output maps around the network, per coordinate d:
  *   z = (theta - mu) * inv_s;   g = a + h (theta - mu) + o * out          */
 int ab_sur_pre(int C, int D, const float* theta, const float* mu, const float* inv_s, float* z, void* stream);

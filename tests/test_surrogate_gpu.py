@@ -89,7 +89,55 @@ def test_surrogate_gains_over_plain_hmc():
     ess_s = ess(torch.stack(rec_s).cpu().numpy()).min()
     cost_s = (sur.n_grad - g0) + 0.5 * (sur.n_logp - l0)
     gain = (ess_s / cost_s) / (ess_p / cost_p)
-    print("plain ESS %.1f cost %d acc %s | surrogate ESS %.1f cost %.1f acc %s err %.3f fallback %s gain %.2f" % (
-        ess_p, cost_p, plain.accept_rate(), ess_s, cost_s, sur.accept_rate(), sur.last_rel_err, sur.fallback, gain))
+    acc_s = sur.accept_rate()[0]
+    # the same sampler without the network (its diagonal linear part only)
+    sur.sur.use_net = False
+    sur._refresh_current()
+    sur.reset_stats()
+    sur.run(40, learn=False)
+    acc_lin = sur.accept_rate()[0]
+    print("plain ESS %.1f cost %d acc %s | surrogate ESS %.1f cost %.1f acc %s err %.3f fallback %s gain %.2f"
+          " | without the network: acc %.3f" % (
+              ess_p, cost_p, plain.accept_rate(), ess_s, cost_s, acc_s, sur.last_rel_err, sur.fallback,
+              gain, acc_lin))
     assert not sur.fallback
     assert gain > 2.0
+    # the network is what makes the cheap trajectories acceptable
+    assert acc_s > 0.6 and acc_lin < 0.5 * acc_s
+
+
+def test_surrogate_chain_targets_the_exact_posterior():
+    # Small HLR (N = 20,000, D = 32, Student-t(3) prior), 256 chains.  The
+    # plain GPU sampler's transitions equal the FP64 oracle's
+    # (test_hlrb_gpu.test_hmc_transitions_match_fp64_oracle); the surrogate
+    # sampler, whose accept test uses the exact log density, must reach the
+    # same posterior: every posterior mean within 0.05 posterior sd, and
+    # within 5 Monte-Carlo standard errors.
+    N_, D, C = 20_000, 32, 256
+    X, y, beta = H.synthetic(N_, D, seed=8)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    init = np.asarray(beta, np.float32)[None] + 1e-3 * np.random.default_rng(1).standard_normal((C, D)).astype(np.float32)
+    plain = H.BatchedHmc(d, C, L=10, eps=0.01, jitter=0.1, seed=21, init=init)
+    eps = H.adapt_step_size(plain, 60)
+    plain.run(100)
+    start = plain.theta.cpu().numpy()
+    plain.capture()
+    rec_p = []
+    plain.run(400, record=rec_p)
+    sur = H.SurrogateHmc(d, C, L=10, eps=eps, jitter=0.1, seed=22, init=start, train_every=4, train_steps=10)
+    sur.run(100)
+    sur.capture()
+    rec_s = []
+    sur.run(400, record=rec_s)
+    dp = torch.stack(rec_p).cpu().numpy()
+    ds = torch.stack(rec_s).cpu().numpy()
+    ep, es = ess(dp), ess(ds)
+    mp, ms = dp.reshape(-1, D).mean(0), ds.reshape(-1, D).mean(0)
+    sd = dp.reshape(-1, D).std(0)
+    z = (ms - mp) / (sd * np.sqrt(1.0 / ep + 1.0 / es))
+    print("min ESS plain %.0f surrogate %.0f; max |diff|/sd %.4f; max |z| %.2f; accept %s %s" % (
+        ep.min(), es.min(), np.max(np.abs(ms - mp) / sd), np.max(np.abs(z)), plain.accept_rate(), sur.accept_rate()))
+    assert np.max(np.abs(ms - mp) / sd) < 0.05
+    assert np.max(np.abs(z)) < 5.0
+    sd_s = ds.reshape(-1, D).std(0)
+    assert np.all(np.abs(sd_s / sd - 1.0) < 0.1)
