@@ -91,11 +91,87 @@ struct Ws {
 
 __device__ __forceinline__ double cta_sum(double v, double* red) { return block_sum_f64(v, red); }
 
+constexpr int SMALL_COLS = 32;   // small-D pass: D gradient columns, the bias column, the log-likelihood
+
+// Sum over the warp's lanes of each of 32 per-lane values, transposed: on
+// return v[0] of lane L holds the warp sum of column L (31 shuffles; fixed
+// butterfly order, so deterministic).
+__device__ __forceinline__ void warp_transpose_sum(double (&v)[SMALL_COLS], int lane) {
+#pragma unroll
+  for (int sft = 16; sft >= 1; sft >>= 1) {
+    const bool up = (lane & sft) != 0;
+#pragma unroll
+    for (int i = 0; i < sft; ++i) {
+      const double send = up ? v[i] : v[i + sft];
+      const double keep = up ? v[i + sft] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
+    }
+  }
+}
+
+// Data pass for D + 2 <= 32: one row per thread (t, the log-likelihood term
+// and the residual's contributions to all D + 1 gradient columns in
+// registers, Kahan-compensated), then one transposed warp reduction and a
+// fixed-order sum over the warps, all in FP64.  The row-per-thread walk
+// keeps every thread busy at small N, where the segmented pass below is
+// bound by its per-row shuffle latency.
+__device__ double data_pass_small(const HlrModelDev& m, const double* par, Ws& ws, bool want_grad) {
+  const int D = m.D, N = m.N;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = tid; k < D; k += blockDim.x) ws.th[k] = (float)par[k];
+  const float bias = m.has_b ? (float)par[D] : 0.0f;
+  __syncthreads();
+  float th[SMALL_COLS - 2];
+#pragma unroll
+  for (int k = 0; k < SMALL_COLS - 2; ++k) th[k] = k < D ? ws.th[k] : 0.0f;
+  float s[SMALL_COLS], c[SMALL_COLS];
+#pragma unroll
+  for (int j = 0; j < SMALL_COLS; ++j) { s[j] = 0.0f; c[j] = 0.0f; }
+  for (int n = tid; n < N; n += blockDim.x) {
+    const size_t rb = (size_t)n * m.ldx;
+    float x[SMALL_COLS - 2];
+    float t = 0.0f;
+#pragma unroll
+    for (int k = 0; k < SMALL_COLS - 2; ++k) {
+      x[k] = k < D ? load_x(m, rb + k) : 0.0f;
+      t += x[k] * th[k];
+    }
+    float llv, rv;
+    bern_terms(m.y[n], t + bias, llv, rv);
+    kahan_add(s[SMALL_COLS - 1], c[SMALL_COLS - 1], llv);
+    if (want_grad) {
+#pragma unroll
+      for (int k = 0; k < SMALL_COLS - 2; ++k)
+        if (k < D) kahan_add(s[k], c[k], rv * x[k]);
+#pragma unroll
+      for (int k = 0; k < SMALL_COLS - 1; ++k)
+        if (k == D) kahan_add(s[k], c[k], rv);
+    }
+  }
+  double v[SMALL_COLS];
+#pragma unroll
+  for (int j = 0; j < SMALL_COLS; ++j) v[j] = (double)s[j] - (double)c[j];
+  warp_transpose_sum(v, lane);
+  __syncthreads();
+  ws.gpart[warp * 32 + lane] = v[0];
+  __syncthreads();
+  if (tid < 32) {
+    double acc = 0.0;
+    const int nw = blockDim.x >> 5;
+    for (int w = 0; w < nw; ++w) acc += ws.gpart[w * 32 + tid];
+    if (tid == SMALL_COLS - 1) ws.red[33] = acc;
+    else if (want_grad && tid <= D) ws.g[tid] = acc;
+  }
+  __syncthreads();
+  return ws.red[33];
+}
+
 // Data pass at `par` (theta in par[0..D-1], b = par[D] if has_b).  Writes
 // ll_data (returned, all threads) and, if want_grad, ws.g[0..D] (theta then
 // bias) — the full data gradient.
 __device__ double data_pass(const HlrModelDev& m, const double* par, Ws& ws, bool want_grad) {
   const int D = m.D, N = m.N;
+  if (D + 2 <= SMALL_COLS) return data_pass_small(m, par, ws, want_grad);
   const int tid = threadIdx.x;
   for (int k = tid; k < D; k += blockDim.x) ws.th[k] = (float)par[k];
   const float bias = m.has_b ? (float)par[D] : 0.0f;

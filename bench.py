@@ -162,6 +162,178 @@ def run_hlr_pass(n_rows, steps, warmup):
                        "chains": HLR_C}}
 
 
+# ---- config 1: small HLR, plain HMC (the reference's CPU case) -------------
+def hlr_small_data(N_=1000, D=10, seed=0):
+    """X ~ N(0,1), sigma^2 ~ InvGamma(1,1), beta ~ N(0, sigma^2 I), y ~ Bern(sigmoid(X beta))."""
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((N_, D))
+    s2 = 1.0 / rng.gamma(1.0, 1.0)
+    beta = rng.standard_normal(D) * np.sqrt(s2)
+    y = (rng.random(N_) < 1.0 / (1.0 + np.exp(-(X @ beta)))).astype(np.int32)
+    return X, y, beta, s2
+
+
+def hlr_small_cpu_baseline(X, y, init, iters, budget_s=10.0):
+    """The reference's own HMC (cbits h_augur_mcmc_hmc with the restated ll/grad,
+    oracle/_ref) for one chain on one host core: min-ESS/s over (beta, sigma^2)."""
+    from augurv2_b200.diagnostics import ess
+    from oracle import oracle as O
+    kind = "reference" if O.available("ref") else "port"
+    o = O.Oracle("ref" if kind == "reference" else "oracle")
+    m = O.HlrModel(X, y, has_b=False, vprior="invgamma", a0=1.0, s0=1.0)
+    D = X.shape[1]
+    idx = list(range(D)) + [D + 1]
+    par = np.array(init, np.float64)
+    draws = []
+    t0 = time.time()
+    for it in range(iters):
+        O.hlr_hmc(o, m, par, idx, 0.1, 0.01, 0, it, 0, 0)
+        draws.append(par[idx].copy())
+        if time.time() - t0 > budget_s:
+            break
+    wall = time.time() - t0
+    e = ess(np.asarray(draws)[:, None, :])
+    return {"value": float(e.min() / wall), "unit": "min-ESS/s", "cores": 1, "kind": kind,
+            "sample": "%d HMC iterations of one chain (10 leapfrog steps, eps 0.01), %.2f s" % (len(draws), wall)}
+
+
+def run_hlr_small(iters=1000, chains=256, cpu=True):
+    """HLR N=1000, D=10 (ighlr.rv: sigma^2 ~ InvGamma(1,1)), HMC over
+    (beta, sigma^2) with simulation length 0.1 and step 0.01 (10 leapfrog
+    steps), 1000 iterations, seed 0, on the per-chain engine: every chain's
+    whole run is one kernel launch.  min-ESS/s over the 11 parameters."""
+    import torch
+    from augurv2_b200 import hlr as G
+    from augurv2_b200.diagnostics import ess
+    X, y, beta, s2 = hlr_small_data()
+    D = X.shape[1]
+    data = G.HlrData(X, y, has_b=False, vprior="invgamma", a0=1.0, s0=1.0, compat=True, x_dtype="f32")
+    sched = [{"kind": "HMC", "block": ["theta", "v"], "simlen": 0.1, "eps": 0.01}]
+    init = np.zeros(D + 2)
+    init[:D] = beta
+    init[D + 1] = s2
+    idx = list(range(D)) + [D + 1]
+    out = {}
+    for C_ in (1, chains):
+        # draws (one launch per iteration, recorded) ...
+        ch = G.HlrChains(data, sched, C=C_, init=init, seed=0)
+        rec = np.empty((iters, C_, len(idx)))
+        for it in range(iters):
+            ch.run(1)
+            rec[it] = ch.pars[:, idx].cpu().numpy()
+        e = ess(rec)
+        # ... and the same iterations timed as one launch (identical states:
+        # the random streams are keyed by iteration)
+        ch2 = G.HlrChains(data, sched, C=C_, init=init, seed=0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ch2.run(iters)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        same = bool(np.array_equal(ch2.pars[:, idx].cpu().numpy(), rec[-1]))
+        out[C_] = {"min_ess": float(e.min()), "ms": ms, "min_ess_per_s": float(e.min() / (ms / 1e3)),
+                   "us_per_iteration": ms * 1e3 / iters, "replay_identical": same}
+    line = {"metric": "min-ESS/sec (HLR plain HMC, N=1000 D=10)", "value": out[chains]["min_ess_per_s"],
+            "unit": "min-ESS/s", "chains": chains, "single_chain": out[1], "batched": out[chains],
+            "config": {"workload": "hlr_hmc_n1000_d10", "N": 1000, "D": 10, "iterations": iters,
+                       "leapfrog_steps": 10, "eps": 0.01, "seed": 0, "x_dtype": "f32",
+                       "block": "theta, sigma^2"}}
+    if cpu:
+        line["cpu_baseline"] = hlr_small_cpu_baseline(X, y, init, iters)
+        line["gain_single_chain_vs_cpu"] = out[1]["min_ess_per_s"] / line["cpu_baseline"]["value"]
+    return line
+
+
+# ---- config 3: Gaussian mixture Gibbs ----------------------------------------
+GMM_N, GMM_K, GMM_D = 200_000, 16, 32
+
+
+def gmm_data(N_=GMM_N, K=GMM_K, d=GMM_D, seed=0):
+    """Means ~ N(0, 25 I), covariances ~ Wishart(d + 2, I) / (d + 2),
+    weights ~ Dirichlet(1); y stored as float32."""
+    rng = np.random.default_rng(seed)
+    mus = rng.standard_normal((K, d)) * 5.0
+    covs = []
+    for _ in range(K):
+        A = rng.standard_normal((d + 2, d))
+        covs.append(A.T @ A / (d + 2))
+    pis = rng.dirichlet(np.ones(K))
+    z = rng.choice(K, size=N_, p=pis)
+    Y = np.empty((N_, d))
+    for k in range(K):
+        m = z == k
+        if m.any():
+            Y[m] = mus[k] + rng.standard_normal((m.sum(), d)) @ np.linalg.cholesky(covs[k]).T
+    return Y.astype(np.float32), z.astype(np.int32), mus, np.array(covs), pis
+
+
+def gmm_cpu_baseline(Y, mus, covs, pis, n_points=1500):
+    """The reference's DiscGibbs z (cbits augur_mvnormal_ll, which factors the
+    covariance for every point and component) on a bounded sample of points."""
+    from oracle import oracle as O
+    kind = "reference" if O.available("ref") else "port"
+    o = O.Oracle("ref" if kind == "reference" else "oracle")
+    K, d = mus.shape
+    g = O.GmmModel(Y[:n_points].astype(np.float64), K, np.zeros(d), 25.0 * np.eye(d), shared_cov=False,
+                   alpha=np.ones(K), df=d + 2, scale0=np.eye(d))
+    t0 = time.time()
+    O.gmm_disc_z(o, g, pis, mus, covs, 0, 0)
+    wall = time.time() - t0
+    return {"value": n_points / wall, "unit": "points/s (assignment draw)", "cores": 1, "kind": kind,
+            "sample": "DiscGibbs z over %d of the %d points (K=%d, d=%d), %.2f s" % (n_points, len(Y), K, d, wall)}
+
+
+def run_gmm(steps=10, warmup=3, cpu=True):
+    """hmvgmm.rv, K=16, d=32, N=200,000: one sweep = ConjGibbs [pis] (*)
+    ConjGibbs [mu] (*) ConjGibbs [cov] (*) DiscGibbs [z] on the device."""
+    import torch
+    from augurv2_b200 import _native as Nn
+    from augurv2_b200.gmm import GmmGibbs
+    Y, z0, mus, covs, pis = gmm_data()
+    K, d = GMM_K, GMM_D
+    s = GmmGibbs(Y, K, np.zeros(d), 25.0 * np.eye(d), alpha=np.ones(K), df=d + 2, scale0=np.eye(d),
+                 mu=mus, cov=covs, pis=pis, z=z0, seed=3)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    s.sweep(warmup)
+    torch.cuda.synchronize()
+    ms = 0.0
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.sweep(1)
+        b.record()
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+    # the assignment kernel alone (its FP64 work is the sweep's bulk)
+    L = Nn.lib()
+    zs = s.z.clone()
+    zms = 0.0
+    for i in range(steps):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        Nn.check(L.ab_gmm_disc_z(GMM_N, d, K, 0, Nn.ptr(s.Y), Nn.ptr(s.pis), Nn.ptr(s.mu), Nn.ptr(s.Linv),
+                                 Nn.ptr(s.hdet), Nn.ptr(zs), s.seed, 10_000 + i, 0, Nn.stream_ptr()), "disc_z")
+        b.record()
+        torch.cuda.synchronize()
+        zms += a.elapsed_time(b)
+    zms /= steps
+    flops_pt = K * (d * d + 3 * d)     # triangular solve (d^2/2 FMAs) + centring and squares, per component
+    ach = GMM_N * flops_pt / (zms / 1e3) / 1e12
+    line = {"metric": "GMM Gibbs points/sec (hmvgmm, K=16 d=32)", "value": GMM_N * steps / (ms / 1e3),
+            "unit": "points/s", "ms_per_sweep": ms / steps, "steps": steps, "warmup": warmup,
+            "roofline": {"bound": "fp64", "kernel": "gmm_z_kernel", "achieved": ach, "peak": 37.0,
+                         "unit": "TFLOP/s", "frac": ach / 37.0, "peak_source": "nominal (no measured FP64 peak)",
+                         "launch_ms": zms, "algorithmic_flops_per_point": flops_pt},
+            "config": {"workload": "gmm_hmvgmm_n200000_k16_d32", "N": GMM_N, "K": K, "d": d,
+                       "y_dtype": "f32", "l2": "flushed between timed sweeps"}}
+    if cpu:
+        line["cpu_baseline"] = gmm_cpu_baseline(Y, mus, covs, pis)
+    return line
+
+
 def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_steps=10):
     """Surrogate-gradient HMC vs plain exact-gradient HMC on the same data,
     chains, step-size rule and iteration count; min-ESS/s of each (ESS over
@@ -342,11 +514,17 @@ def run_ours(args, rank, world, local_rank):
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(off, w, budget_s=args.cpu_seconds)
         if world == 1 and not args.no_secondary:
-            try:
-                line["hlr_surrogate"] = run_hlr_surrogate(iters=args.hlr_iters, train_every=args.train_every,
-                                                          train_steps=args.train_steps)
-            except Exception as e:   # the LDA line stands on its own
-                line["hlr_surrogate"] = {"error": repr(e)[:300]}
+            # the other configurations, each measured in the same run (the
+            # LDA line stands on its own if one of them fails)
+            for key, fn in (("hlr_surrogate", lambda: run_hlr_surrogate(iters=args.hlr_iters,
+                                                                         train_every=args.train_every,
+                                                                         train_steps=args.train_steps)),
+                            ("hlr_small", lambda: run_hlr_small(cpu=not args.no_cpu_baseline)),
+                            ("gmm", lambda: run_gmm(cpu=not args.no_cpu_baseline))):
+                try:
+                    line[key] = fn()
+                except Exception as e:
+                    line[key] = {"error": repr(e)[:300]}
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -474,7 +652,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the surrogate HLR measurement")
-    ap.add_argument("--workload", default="lda", choices=["lda", "hlr_surrogate", "hlr_pass"])
+    ap.add_argument("--workload", default="lda", choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm"])
     ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
     ap.add_argument("--hlr-iters", type=int, default=100)
     ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
@@ -486,6 +664,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
+    elif args.workload in ("hlr_small", "gmm"):
+        import torch
+        torch.cuda.set_device(local_rank)
+        fn = run_hlr_small if args.workload == "hlr_small" else run_gmm
+        line = fn(cpu=not args.no_cpu_baseline) if rank == 0 else None
     elif args.workload == "hlr_pass":
         import torch
         torch.cuda.set_device(local_rank)
