@@ -41,7 +41,9 @@ namespace {
 constexpr int FWD_BN = 128;   // data rows per forward tile
 constexpr int FWD_WARPS = 8;  // epilogue warps of the forward pass (two column groups)
 constexpr int FWD_GROUPS = FWD_WARPS / 4;
-constexpr int BWD_BN = 128;   // gradient columns per backward tile
+// gradient columns per backward tile: the narrowest of 32 / 64 / 128 that
+// covers D (wider D takes several 128-column tiles)
+inline int bwd_bn(int D) { return D <= 32 ? 32 : (D <= 64 ? 64 : 128); }
 
 inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 inline size_t align256(size_t a) { return (a + 255) & ~size_t(255); }
@@ -56,7 +58,8 @@ Layout layout(int N, int D, int C) {
   L.Np = round_up(N, 64);
   L.Dp = round_up(D, 64);
   L.fwd_tiles = (N + FWD_BN - 1) / FWD_BN;
-  const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + BWD_BN - 1) / BWD_BN);
+  const int bn = bwd_bn(D);
+  const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + bn - 1) / bn);
   const int kb = L.Np / tc::BK;
   int sp = tc::sm_count() / tiles;
   if (sp < 1) sp = 1;
@@ -304,11 +307,15 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   if (grad) {
     const int nb = L.Np / 64;
     if ((rc = tc::encode_2d_bf16(&ma, r3, (uint64_t)nb * 3 * C, 64, 64, tc::BM))) return rc;
-    if ((rc = tc::encode_2d_bf16(&mb, m->Xt, (uint64_t)nb * D, 64, 64, BWD_BN))) return rc;
+    const int bn = bwd_bn(D);
+    if ((rc = tc::encode_2d_bf16(&mb, m->Xt, (uint64_t)nb * D, 64, 64, bn))) return rc;
     GradEpi ge{w, C, D, L.ldw, 0};
-    const tc::Shape bs = tc::make_shape(C, D, N, L.splits, tc::k_blocked(3, C), tc::k_blocked(1, D), BWD_BN);
+    const tc::Shape bs = tc::make_shape(C, D, N, L.splits, tc::k_blocked(3, C), tc::k_blocked(1, D), bn);
     AB_REQUIRE(bs.splits == L.splits, AB_ERR_STATE, "hlrb: split arithmetic mismatch");
-    if ((rc = tc::launch_gemm<BWD_BN, 3, 1>(ma, mb, bs, ge, err, st))) return rc;
+    if (bn == 32) rc = tc::launch_gemm<32, 3, 1>(ma, mb, bs, ge, err, st);
+    else if (bn == 64) rc = tc::launch_gemm<64, 3, 1>(ma, mb, bs, ge, err, st);
+    else rc = tc::launch_gemm<128, 3, 1>(ma, mb, bs, ge, err, st);
+    if (rc) return rc;
   }
   hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles * FWD_GROUPS, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
                                         m->prior_a, m->prior_b, logp, grad, ldg);

@@ -500,3 +500,82 @@ def adapt_step_size(sampler, n, target=0.8, rate=1.5, lo=1e-6, hi=10.0, run_kw=N
         eps = float(min(hi, max(lo, eps * math.exp(rate * (a - target)))))
         sampler.set_eps(eps)
     return eps
+
+
+class BatchedNuts:
+    """C chains of the reference's NUTS (cbits/augur_mcmclib.h:575-776) on an
+    HlrbData, advanced together: each round every chain walks its tree to the
+    next leaf (ab_nutsb_advance) and one tensor-core pass evaluates the log
+    density and gradient at all chains' leaf positions.  Chains restart as
+    soon as their tree terminates, each recording its draws (up to
+    `hist_cap`).  One round can be captured as a CUDA graph."""
+
+    def __init__(self, data, C_, eps, max_depth=10, seed=0, init=None, hist_cap=256, comp=0, iter0=0):
+        self.data, self.C, self.D = data, int(C_), data.D
+        self.eps, self.max_depth, self.seed, self.comp = float(eps), int(max_depth), int(seed), int(comp)
+        self.hist_cap = int(hist_cap)
+        D, dev = self.D, data.device
+        if init is None:
+            init = np.zeros((self.C, D), np.float32)
+        init = np.broadcast_to(np.asarray(init, np.float32), (self.C, D)).copy()
+        nb = int(N.lib().ab_nutsb_state_bytes(self.C, D, self.hist_cap))
+        self.mem = torch.zeros(nb, dtype=torch.uint8, device=dev)
+        th = torch.as_tensor(init).to(dev).contiguous()
+        self.work = data.workspace(self.C)
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.logp_new = torch.zeros(self.C, dtype=torch.float64, device=dev)
+        self.g_new = torch.zeros((self.C, D), dtype=torch.float32, device=dev)
+        lp, g = data.logp_grad(th, True, work=self.work, err=self.err)
+        N.check(N.lib().ab_nutsb_init(N.ptr(self.mem), self.C, D, self.hist_cap, N.ptr(th), N.ptr(g), N.ptr(lp),
+                                      int(iter0), N.stream_ptr()), "ab_nutsb_init")
+        pt, ph, pd = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        N.check(N.lib().ab_nutsb_thprop(N.ptr(self.mem), self.C, D, self.hist_cap, C.byref(pt), C.byref(ph),
+                                        C.byref(pd)), "ab_nutsb_thprop")
+        base = self.mem.data_ptr()
+        f32 = self.mem.view(torch.float32) if nb % 4 == 0 else None
+        off_t, off_h, off_d = pt.value - base, ph.value - base, pd.value - base
+        self.thprop = self.mem[off_t:off_t + 4 * self.C * D].view(torch.float32).view(self.C, D)
+        self.hist = self.mem[off_h:off_h + 4 * self.C * self.hist_cap * D].view(torch.float32).view(
+            self.C, self.hist_cap, D)
+        self.hist_depth = self.mem[off_d:off_d + 4 * self.C * self.hist_cap].view(torch.int32).view(
+            self.C, self.hist_cap)
+        self.info_buf = torch.zeros((self.C, 6), dtype=torch.float64, device=dev)
+        self.rounds = 0
+        self.graph = None
+        del f32
+
+    def _round(self, stream=None):
+        N.check(N.lib().ab_nutsb_advance(N.ptr(self.mem), self.C, self.D, self.hist_cap, self.max_depth, self.eps,
+                                         self.seed, self.comp, N.ptr(self.logp_new), N.ptr(self.g_new),
+                                         N.stream_ptr(stream)), "ab_nutsb_advance")
+        self.data.logp_grad(self.thprop, True, self.logp_new, self.g_new, self.work, self.err, stream)
+
+    def capture(self, stream=None):
+        """Capture one round (advance + pass) as a CUDA graph.  The capture
+        itself does not run the round; a warm-up round runs first."""
+        self._round(stream)
+        self.rounds += 1
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=stream):
+            self._round(torch.cuda.current_stream())
+
+    def run(self, rounds):
+        for _ in range(int(rounds)):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._round()
+            self.rounds += 1
+
+    def info(self):
+        N.check(N.lib().ab_nutsb_info(N.ptr(self.mem), self.C, self.D, self.hist_cap, N.ptr(self.info_buf),
+                                      N.stream_ptr()), "ab_nutsb_info")
+        return self.info_buf.cpu().numpy()
+
+    def draws(self):
+        """[n, C, D]: the first n draws of every chain, n = the smallest count."""
+        inf = self.info()
+        if np.any(inf[:, 3] != 0):
+            raise N.AugurError("batched NUTS: a chain reported an error")
+        n = int(min(inf[:, 0].min(), self.hist_cap))
+        return self.hist[:, :n].permute(1, 0, 2).cpu().numpy()

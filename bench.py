@@ -245,6 +245,91 @@ def run_hlr_small(iters=1000, chains=256, cpu=True):
     return line
 
 
+# ---- config 4: many HLR instances, batched NUTS --------------------------------
+NUTS_INST, NUTS_C, NUTS_DEPTH = 64, 512, 10
+
+
+def nuts_instances(n_inst=NUTS_INST, seed=0):
+    """N_i log-uniform in [1e3, 1e6], D_i uniform over {16, 64, 256}."""
+    rng = np.random.default_rng(seed)
+    Ns = np.exp(rng.uniform(np.log(1e3), np.log(1e6), n_inst)).astype(np.int64)
+    Ds = rng.choice([16, 64, 256], n_inst)
+    return [(int(n), int(d)) for n, d in zip(Ns, Ds)]
+
+
+def run_hlr_nuts(rounds=600, n_inst=NUTS_INST, chains=NUTS_C, streams=8, hist_cap=128):
+    """64 HLR instances (X ~ N(0,1) bf16, sigma^2 ~ InvGamma(1,1),
+    beta ~ N(0, sigma^2 I), y ~ Bern(sigmoid(X beta)); sigma^2 held at its
+    generating value), 512 NUTS chains each, max tree depth 10.  Every round
+    each instance advances all its chains to their next leaf and evaluates
+    one batched tensor-core pass; an instance's round is one CUDA graph, the
+    instances' graphs are spread over `streams` streams.  min-ESS/s per
+    instance = min-ESS of its draws / the whole run's device time; the line
+    reports the minimum over instances."""
+    import torch
+    from augurv2_b200 import hlrb as H
+    from augurv2_b200.diagnostics import ess
+    specs = nuts_instances(n_inst)
+    rng = np.random.default_rng(42)
+    insts = []
+    flops_round = 0.0
+    for i, (Ni, Di) in enumerate(specs):
+        s2 = 1.0 / rng.gamma(1.0, 1.0)
+        beta = (rng.standard_normal(Di) * np.sqrt(s2)).astype(np.float32)
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1000 + i)
+        X = torch.randn((Ni, Di), generator=g, device="cuda").to(torch.bfloat16)
+        t = X.float() @ torch.as_tensor(beta, device="cuda")
+        y = (torch.rand(Ni, generator=g, device="cuda") < torch.sigmoid(t)).to(torch.int32)
+        w = (torch.sigmoid(t) * (1 - torch.sigmoid(t))).mean().item()
+        eps = 0.6 / np.sqrt(Ni * w + 1.0 / s2)       # ~ 0.6 of the posterior scale
+        d = H.HlrbData(X, y, prior="normal", var=s2)
+        init = beta[None] + (0.1 * eps) * rng.standard_normal((chains, Di)).astype(np.float32)
+        nuts = H.BatchedNuts(d, chains, eps=eps, max_depth=NUTS_DEPTH, seed=7 + i, init=init, hist_cap=hist_cap)
+        insts.append((d, nuts))
+        flops_round += 12.0 * Ni * Di * chains
+    sts = [torch.cuda.Stream() for _ in range(streams)]
+    for i, (_, nuts) in enumerate(insts):
+        with torch.cuda.stream(sts[i % streams]):
+            nuts.capture(sts[i % streams])
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for st in sts:
+        st.wait_stream(torch.cuda.current_stream())
+    for r in range(rounds):
+        for i, (_, nuts) in enumerate(insts):
+            with torch.cuda.stream(sts[i % streams]):
+                nuts.graph.replay()
+    for st in sts:
+        torch.cuda.current_stream().wait_stream(st)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    per = []
+    for i, (d, nuts) in enumerate(insts):
+        dr = nuts.draws()
+        inf = nuts.info()
+        e = ess(dr) if dr.shape[0] >= 4 else np.zeros(d.D)
+        per.append({"N": d.N, "D": d.D, "draws_per_chain": int(dr.shape[0]), "min_ess": float(e.min()),
+                    "mean_depth": float(inf[:, 5].mean()), "min_ess_per_s": float(e.min() / (ms / 1e3))})
+    worst = min(per, key=lambda q: q["min_ess_per_s"])
+    peak, kind = measured_tensor_peak(sustained=True)
+    ach = flops_round * rounds / (ms / 1e3) / 1e12
+    return {"metric": "min-ESS/sec per instance, min over 64 instances (batched NUTS, HLR)",
+            "value": worst["min_ess_per_s"], "unit": "min-ESS/s", "rounds": rounds, "seconds": ms / 1e3,
+            "worst_instance": worst, "median_instance_min_ess_per_s": float(np.median([q["min_ess_per_s"] for q in per])),
+            "total_draws": int(sum(q["draws_per_chain"] for q in per) * chains),
+            "roofline": {"bound": "tensor", "kernel": "gemm_kernel (batched passes, all instances)", "achieved": ach,
+                         "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "peak_source": kind + " (sustained)"},
+            "instances": per,
+            "config": {"workload": "hlr_nuts_64_instances_c512", "instances": n_inst, "chains": chains,
+                       "max_depth": NUTS_DEPTH, "x_dtype": "bf16", "N": "log-uniform [1e3, 1e6]",
+                       "D": "{16, 64, 256}", "prior": "normal(0, sigma^2), sigma^2 at its generating value",
+                       "step_size": "0.6 / sqrt(N E[w] + 1/sigma^2) at the generating coefficients",
+                       "streams": streams}}
+
+
 # ---- config 3: Gaussian mixture Gibbs ----------------------------------------
 GMM_N, GMM_K, GMM_D = 200_000, 16, 32
 
@@ -652,7 +737,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the surrogate HLR measurement")
-    ap.add_argument("--workload", default="lda", choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm"])
+    ap.add_argument("--workload", default="lda",
+                    choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm", "hlr_nuts"])
+    ap.add_argument("--nuts-rounds", type=int, default=600)
     ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
     ap.add_argument("--hlr-iters", type=int, default=100)
     ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
@@ -669,6 +756,10 @@ def main():
         torch.cuda.set_device(local_rank)
         fn = run_hlr_small if args.workload == "hlr_small" else run_gmm
         line = fn(cpu=not args.no_cpu_baseline) if rank == 0 else None
+    elif args.workload == "hlr_nuts":
+        import torch
+        torch.cuda.set_device(local_rank)
+        line = run_hlr_nuts(rounds=args.nuts_rounds) if rank == 0 else None
     elif args.workload == "hlr_pass":
         import torch
         torch.cuda.set_device(local_rank)

@@ -310,6 +310,25 @@ int ab_hmcb_step(const ab_hmcb_state* s, const float* g, void* stream);
 int ab_hmcb_final(const ab_hmcb_state* s, const float* g_new, const double* logp_new, void* stream);
 
 /* ======================================================================= *
+ * Batched NUTS (h_augur_mcmc_nuts / h_augur_nuts_build_tree,
+ * cbits/augur_mcmclib.h:575-776, for C chains of P parameters).  The chains'
+ * resumable tree walks live in one device buffer of ab_nutsb_state_bytes;
+ * each round is ab_nutsb_advance (every chain walks to its next leaf and
+ * leaves the leaf position in the thprop array) followed by the caller's
+ * evaluation of logp [C] and grad [C][P] at thprop, passed to the next
+ * advance.  Completed iterations append their draws to a per-chain history
+ * of hist_cap rows.  info[c][6] = draws, last tree depth, last leaves,
+ * error flag, iteration, mean depth.
+ * ======================================================================= */
+size_t ab_nutsb_state_bytes(int C, int P, int hist_cap);
+int ab_nutsb_init(void* state, int C, int P, int hist_cap, const float* theta, const float* grad, const double* logp,
+                  uint32_t iter0, void* stream);
+int ab_nutsb_thprop(void* state, int C, int P, int hist_cap, float** thprop, float** hist, int** hist_depth);
+int ab_nutsb_advance(void* state, int C, int P, int hist_cap, int max_depth, double eps, uint64_t seed, uint32_t comp,
+                     const double* logp_new, const float* g_new, void* stream);
+int ab_nutsb_info(void* state, int C, int P, int hist_cap, double* info, void* stream);
+
+/* ======================================================================= *
  * Gradient-surrogate MLP (no counterpart in the reference): d_in -> h1 ->
  * h2 -> d_out, GELU hidden layers, flat FP32 master parameters w with a bf16
  * copy wb of the same layout [W1, b1, W2, b2, W3, b3]; forward passes use

@@ -130,3 +130,30 @@ def test_graph_replay_equals_eager():
     b.run(3)
     torch.cuda.synchronize()
     assert torch.equal(a.theta, b.theta)
+
+
+def test_batched_nuts_matches_fp64_oracle_nuts():
+    # The reference's NUTS on the HLR block theta with v fixed (ighlr.rv's
+    # conditional), FP64 oracle, against the batched sampler fed the same
+    # Philox streams: same draws to FP32 accuracy and the same tree depths.
+    o = O.Oracle("oracle")
+    N_, D, C, v, eps, seed, depth = 400, 8, 5, 2.0, 0.05, 13, 6
+    d, X64, y = _data(N_, D, seed=31, prior="normal")
+    d = H.HlrbData(torch.as_tensor(X64, dtype=torch.float32).to(torch.bfloat16), y, prior="normal", var=v)
+    rs = np.random.default_rng(4)
+    init = (rs.standard_normal((C, D)) * 0.3).astype(np.float32)
+    nuts = H.BatchedNuts(d, C, eps=eps, max_depth=depth, seed=seed, init=init, hist_cap=32)
+    nuts.run(400)
+    got = nuts.draws()
+    depths = nuts.hist_depth.cpu().numpy()
+    assert got.shape[0] >= 4
+    m = O.HlrModel(X64, y, has_b=False, vprior="invgamma")
+    for c in range(C):
+        par = np.zeros(D + 2)
+        par[:D] = init[c]
+        par[D + 1] = v
+        for it in range(min(6, got.shape[0])):
+            dep, leaves, ovf = O.hlr_nuts(o, m, par, list(range(D)), float(np.float32(eps)), seed, it, chain=c,
+                                          comp=0, max_depth=depth)
+            assert dep == depths[c, it], (c, it, dep, depths[c, it])
+            np.testing.assert_allclose(got[it, c], par[:D], rtol=2e-4, atol=2e-5)
