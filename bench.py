@@ -9,11 +9,18 @@ ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z].
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload lda|hlr_surrogate]
 
-The default line also carries, under "hlr_surrogate", the surrogate-gradient
-HMC measurement on HLR (N=2,000,000 rows, D=512, X ~ N(0,1) stored bf16,
-beta ~ Student-t(3), 256 chains, L=10): min-ESS/s of the learned sampler and
-of plain exact-gradient HMC on the same GPU, and their ratio
-(`--workload hlr_surrogate` prints that measurement as its own line).
+The default line also carries the other configurations, each measured in the
+same run (and printable as its own line with --workload):
+  hlr_surrogate  surrogate-gradient HMC on HLR (N=2,000,000 rows, D=512,
+                 X ~ N(0,1) stored bf16, beta ~ Student-t(3), 256 chains,
+                 L=10): min-ESS/s of the learned sampler and of plain
+                 exact-gradient GPU HMC, and their ratio;
+  hlr_small      HLR N=1000, D=10 plain HMC (1000 iterations, 10 leapfrog
+                 steps of 0.01), min-ESS/s against the reference's cbits HMC;
+  gmm            hmvgmm K=16, d=32, N=200,000 Gibbs sweeps, points/s against
+                 the reference's assignment draw;
+  hlr_nuts       64 HLR instances x 512 NUTS chains (max depth 10), min over
+                 instances of min-ESS/s.
 
 N > 1 (launched by torch.distributed.run) runs one independent chain per GPU
 (replicas; LDA chains share nothing), value = all tokens / max-over-ranks time.
@@ -605,7 +612,8 @@ def run_ours(args, rank, world, local_rank):
                                                                          train_every=args.train_every,
                                                                          train_steps=args.train_steps)),
                             ("hlr_small", lambda: run_hlr_small(cpu=not args.no_cpu_baseline)),
-                            ("gmm", lambda: run_gmm(cpu=not args.no_cpu_baseline))):
+                            ("gmm", lambda: run_gmm(cpu=not args.no_cpu_baseline)),
+                            ("hlr_nuts", lambda: run_hlr_nuts(rounds=400))):
                 try:
                     line[key] = fn()
                 except Exception as e:
