@@ -19,7 +19,7 @@
 //                     phi[k]   ~ Dir(beta + cnt_kw[k])       (reads, then
 //                     clears cnt_kw); one draw per thread, then a parallel
 //                     normalisation pass
-//   lda_z_kernel      z ~ p(z | theta, phi), and the counts of the new z
+//   lda_zq_kernel     z ~ p(z | theta, phi), and the counts of the new z
 //                     (cnt_dk rows written whole, cnt_kw incremented)
 // The count statistics of the reference (conj_stat_*, rebuilt from zero each
 // step, CgKern.hs:103-107) are a function of z alone, so they are produced
@@ -30,6 +30,7 @@
 // (_rn intrinsics; this file is also compiled with -fmad=false), so given the
 // same theta, phi and Philox uniforms the assignments and counts equal the
 // reference's CPU sampler's bit for bit.
+#include <algorithm>
 #include <mutex>
 
 #include "common.cuh"
@@ -87,13 +88,13 @@ lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
 // ---------------------------------------------------------------------------
 // phi[k][v] = g[k][v] / sum_v g[k][v], g ~ Gamma(beta_v + cnt[k][v], 1),
 // stored word-major into phiT[v][k].  Two kernels:
-//  lda_phi_draw_kernel  one gamma draw per thread over K * B CTAs (B CTAs per
-//                       topic); writes g unnormalised into phiT, clears the
-//                       counts it read and stores the CTA's fixed-order
-//                       partial sum in scratch (partial[k][b]); the last CTA
-//                       of a topic (atomic ticket) adds the B partials in CTA
-//                       order into nrm[k];
-//  lda_phi_norm_kernel  divides phiT by nrm, row by row and coalesced.
+//  lda_phi_draw_kernel  one gamma draw per thread over K * B CTAs (B CTAs of
+//                       256 words per topic); writes g unnormalised into
+//                       phiT, clears the counts it read and stores the CTA's
+//                       fixed-order partial sum in scratch (partial[k][b]);
+//                       the last CTA of a topic (atomic ticket) adds the B
+//                       partials in CTA order into nrm[k];
+//  lda_phi_norm_kernel  divides phiT by nrm, one 16-byte pair per thread.
 // The sum is deterministic but not in the reference's sequential order, so
 // phi matches the reference to rounding, not bitwise.
 // ---------------------------------------------------------------------------
@@ -104,7 +105,6 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
                     double* __restrict__ nrm, uint64_t seed, const uint32_t* iter_dev,
                     uint32_t iter_fixed) {
   __shared__ double red[33];
-  __shared__ bool last;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
   const int k = blockIdx.x / B;
   const int b = blockIdx.x - k * B;
@@ -124,8 +124,7 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
   if (threadIdx.x == 0) {
     partial[(size_t)k * B + b] = bsum;
     __threadfence();
-    last = atomicAdd(ticket + k, 1u) == (unsigned)(B - 1);
-    if (last) {
+    if (atomicAdd(ticket + k, 1u) == (unsigned)(B - 1)) {
       __threadfence();
       double acc = 0.0;
       for (int i = 0; i < B; ++i) acc = __dadd_rn(acc, __ldcg(partial + (size_t)k * B + i));
@@ -135,50 +134,48 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
   }
 }
 
-constexpr int LDA_NORM_ROWS = 32;   // phiT rows per CTA of the normalisation
-
+// phiT [V][Kp] as V * Kp / 2 pairs of doubles; pair j holds topics 2j mod Kp
+// and the next one.  Padding topics (k >= K) are left untouched (zero).
 __global__ void __launch_bounds__(LDA_THREADS)
 lda_phi_norm_kernel(int K, int V, int Kp, const double* __restrict__ nrm_g,
                     double* __restrict__ phiT) {
   extern __shared__ double nrm[];   // [K]
   for (int k = threadIdx.x; k < K; k += blockDim.x) nrm[k] = nrm_g[k];
   __syncthreads();
-  // one warp per row, lanes over k
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const int v_end = min(V, (int)(blockIdx.x + 1) * LDA_NORM_ROWS);
-  for (int v = blockIdx.x * LDA_NORM_ROWS + warp; v < v_end; v += nw) {
-    double* rowp = phiT + (size_t)v * Kp;
-    for (int k = lane; k < K; k += 32) rowp[k] = __ddiv_rn(rowp[k], nrm[k]);
+  const int half_kp = Kp >> 1;
+  const size_t n2 = (size_t)V * half_kp;
+  double2* p2 = reinterpret_cast<double2*>(phiT);
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < n2; j += (size_t)gridDim.x * blockDim.x) {
+    const int k = 2 * (int)(j % half_kp);
+    if (k >= K) continue;
+    double2 x = p2[j];
+    x.x = __ddiv_rn(x.x, nrm[k]);
+    if (k + 1 < K) x.y = __ddiv_rn(x.y, nrm[k + 1]);
+    p2[j] = x;
   }
 }
 
 static inline int lda_phi_blocks(int V) { return (V + LDA_THREADS - 1) / LDA_THREADS; }
 
 // ---------------------------------------------------------------------------
-// z[t] for every token of document d (one CTA per document):
+// z[t] for every token of document d, K > 64 (one CTA per document; the
+// staged kernel below takes K <= 64):
 //   pmf_k  = (1 * theta[d][k]) * phi[k][w]                (CgDisc.hs:132-139)
 //   norm   = sum_k pmf_k  (sequential)                    (augur_dist.c:800-803)
 //   z      = first i with u < sum_{j<=i} pmf_j / norm      (:805-812)
-// Each warp takes 32 consecutive tokens.  With STAGED (K <= 64) the warp
-// copies the 32 phi rows into shared memory with asynchronous 16-byte copies,
-// one row per copy instruction (coalesced: a row is one contiguous segment,
-// and all 32 rows are in flight at once), with a row pitch
-// of an odd number of 16-byte units so that the per-lane row reads that
-// follow are bank-conflict free; otherwise each lane reads its own row from
-// global memory.  Each lane then computes its token.  The norm pass records
-// the running sum at 8 checkpoints; the reference's running quotient sum is
-// replaced by a division-free test (comment in token_draw) evaluated first
-// at the checkpoints and then inside the one block that contains the answer;
-// only a u within rounding distance of a boundary runs the reference loop
-// itself.  Products are recomputed where needed; they are the same binary64
-// values.
+// One lane per token, reading its phi row from global memory.  The norm pass
+// records the running sum at 8 checkpoints; the reference's running quotient
+// sum is replaced by a division-free test (comment in token_draw) evaluated
+// first at the checkpoints and then inside the one block that contains the
+// answer; only a u within rounding distance of a boundary runs the reference
+// loop itself.  Products are recomputed where needed; they are the same
+// binary64 values.
 // Counts of the new z: the document's row of cnt_dk is accumulated in shared
 // memory and stored whole; cnt_kw receives warp-aggregated atomic increments
 // (lanes with the same (z, w) key elect one leader that adds the group size).
 // ---------------------------------------------------------------------------
 constexpr int LDA_Z_THREADS = 128;
 constexpr int LDA_Z_CP = 8;            // checkpoints of the running sum
-constexpr int LDA_Z_STAGE_MAX_K = 64;
 
 __device__ __forceinline__ int token_draw(int K, int half_kp, int nsuper, int R, int S,
                                           const double* __restrict__ th, const double* row,
@@ -257,7 +254,6 @@ __device__ __forceinline__ int token_draw(int K, int half_kp, int nsuper, int R,
   return zk;
 }
 
-template <bool STAGED>
 __global__ void __launch_bounds__(LDA_Z_THREADS, 4)
 lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
              const int* __restrict__ w, const double* __restrict__ theta,
@@ -269,9 +265,6 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
   double* th = smem;                                    // [KT] (zero padded)
   int* hist = reinterpret_cast<int*>(smem + KT);        // [K]
   const int half_kp = Kp / 2;
-  const int pitch2 = half_kp | 1;                       // row pitch in 16-byte units (odd)
-  double2* stage = reinterpret_cast<double2*>(smem + KT + ((K + 3) & ~3) / 2 + 2) +
-                   (size_t)(threadIdx.x >> 5) * 32 * pitch2;
   const int lane = threadIdx.x & 31;
   const int d = blockIdx.x;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
@@ -292,27 +285,7 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
     const int t = tb + lane;
     const bool active = t < t1;
     const int wt = active ? w[t] : 0;
-    const double* row;
-    if (STAGED) {
-      // Asynchronous 16-byte copies global -> shared (cp.async, L2 only):
-      // all 32 rows are in flight at once and no registers hold them.
-      const int nrow = min(32, t1 - tb);
-#pragma unroll
-      for (int r = 0; r < 32; ++r) {
-        const int wr = __shfl_sync(0xffffffffu, wt, r);
-        if (r < nrow && lane < half_kp) {
-          const double2* src = reinterpret_cast<const double2*>(phiT + (size_t)wr * Kp) + lane;
-          const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + r * pitch2 + lane);
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-        }
-      }
-      asm volatile("cp.async.commit_group;\n" ::: "memory");
-      asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-      __syncwarp();
-      row = reinterpret_cast<const double*>(stage + lane * pitch2);
-    } else {
-      row = phiT + (size_t)wt * Kp;
-    }
+    const double* row = phiT + (size_t)wt * Kp;
     int zk = 0;
     if (active) {
       Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
@@ -330,7 +303,6 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
         if (lane == leader) atomicAdd(cnt_kw + key, __popc(peers));
       }
     }
-    if (STAGED) __syncwarp();   // the stage is rewritten by the next chunk
   }
   __syncthreads();
   if (cnt_dk != nullptr)
@@ -349,6 +321,171 @@ lda_z_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
       }
     }
   }
+}
+
+// The reference's draw itself (augur_unnorm_disc_samp, augur_dist.c:798-813,
+// with pmf_k = (1 * theta_k) * phi_k of CgDisc.hs:132-139): a sequential norm,
+// then the running sum of quotients.  Used where the division-free test of
+// the grouped kernel cannot decide (u within rounding of a boundary, or a
+// norm that is zero, subnormal, infinite or NaN).
+__device__ __noinline__ int lda_reference_draw(int K, const double* __restrict__ th,
+                                               const double* __restrict__ row, double u) {
+  double norm = 0.0;
+  for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, __dmul_rn(th[k], row[k]));
+  double acc = __ddiv_rn(__dmul_rn(th[0], row[0]), norm);
+  int zk = K - 1;
+  for (int i = 1; i < K; ++i) {
+    if (u < acc) { zk = i - 1; break; }
+    acc = __dadd_rn(acc, __ddiv_rn(__dmul_rn(th[i], row[i]), norm));
+  }
+  return zk;
+}
+
+// ---------------------------------------------------------------------------
+// z[t] for every token of document d, K <= 64 (one CTA of 128 threads per
+// document; NQ = Kp / 4 quads of topics, a compile-time constant).
+// Each warp takes 32 consecutive tokens, one per lane.  The warp copies the
+// 32 phi rows into shared memory with asynchronous 16-byte copies, one row
+// per copy instruction (a row is one contiguous segment, and all 32 rows are
+// in flight at once); the row pitch is an odd number of 16-byte units so
+// that the per-lane row reads that follow are bank-conflict free.  Each lane
+// then makes one pass over its row: p_k = theta_k * phi_k and the
+// sequential running sum c_k = c_{k-1} + p_k, written back over the row, so
+// c_{K-1} is the reference's norm bit for bit.  The draw is the first
+// k <= K - 2 with u < acc_k (acc_k the reference's running sum of p_j / norm);
+// it is found without divisions by a binary search over the nondecreasing
+// c_k for the first k with u norm <= c_k (1 + m), and is decided when also
+// u norm < c_k (1 - m).  m = (6K + 32) 2^-53 bounds the rounding of the
+// products, sums and quotients on both sides, so a decided draw equals the
+// reference's; a u within m of a boundary (or a zero, subnormal, infinite or
+// NaN norm) runs the reference's loop itself (lda_reference_draw).  theta and
+// phi are probabilities (nonnegative), which keeps c_k monotone.
+// Counts of the new z: the document's row of cnt_dk is accumulated in shared
+// memory and stored whole; cnt_kw receives warp-aggregated atomic increments
+// (lanes with the same (z, w) key elect one leader that adds the group size).
+// ---------------------------------------------------------------------------
+constexpr int LDA_ZQ_MAX_K = 64;
+
+template <int NQ>
+__global__ void __launch_bounds__(LDA_Z_THREADS, 4)
+lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
+              const int* __restrict__ w, const double* __restrict__ theta,
+              const double* __restrict__ phiT, int* __restrict__ z,
+              int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
+              uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
+  constexpr int KP = 4 * NQ;          // row length in doubles (= the phiT stride)
+  constexpr int H2 = 2 * NQ;          // row length in 16-byte units
+  constexpr int P2 = H2 + 1;          // row pitch in 16-byte units (odd)
+  constexpr int STEP0 = KP > 32 ? 32 : (KP > 16 ? 16 : (KP > 8 ? 8 : (KP > 4 ? 4 : 2)));
+  extern __shared__ double2 smem2[];
+  double2* th2 = smem2;                                        // [H2] theta, zero padded
+  int* hist = reinterpret_cast<int*>(smem2 + H2);              // [KP]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double2* stage = smem2 + H2 + NQ + warp * 32 * P2;           // [32][P2] this warp's rows
+  const int d = blockIdx.x;
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  double* th = reinterpret_cast<double*>(th2);
+  for (int k = threadIdx.x; k < KP; k += blockDim.x) {
+    th[k] = k < K ? theta[(size_t)d * K + k] : 0.0;
+    hist[k] = 0;
+  }
+  __syncthreads();
+  const int t0 = doc_off[d], t1 = doc_off[d + 1];
+  const double m = (6.0 * K + 32.0) * 1.1102230246251565e-16;
+  const double lo = 1.0 - m, hi = 1.0 + m;
+  const double2* __restrict__ phi2 = reinterpret_cast<const double2*>(phiT);
+  for (int tb = t0 + warp * 32; tb < t1; tb += (LDA_Z_THREADS / 32) * 32) {
+    const int t = tb + lane;
+    const bool active = t < t1;
+    const int wt = active ? w[t] : 0;
+    const int nrow = min(32, t1 - tb);
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const int wr = __shfl_sync(0xffffffffu, wt, r);
+      if (r < nrow && lane < H2) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + r * P2 + lane);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                     "l"(phi2 + (size_t)wr * H2 + lane) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    int zk = 0;
+    double u = 0.0;
+    if (active) {
+      Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+      u = s.uniform();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    if (active) {
+      double2* row = stage + lane * P2;
+      double c = 0.0;
+#pragma unroll
+      for (int q = 0; q < H2; ++q) {
+        const double2 f = row[q], g = th2[q];
+        const double c0 = __dadd_rn(c, __dmul_rn(g.x, f.x));
+        c = __dadd_rn(c0, __dmul_rn(g.y, f.y));
+        row[q] = make_double2(c0, c);
+      }
+      const double norm = c;              // padding topics add exact zeros
+      bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
+      zk = K - 1;
+      if (!exact) {
+        const double un = __dmul_rn(u, norm);
+        const double* cs = reinterpret_cast<const double*>(row);
+        // pos = number of k in [0, K-2] with c_k (1 + m) < u norm (a prefix)
+        int pos = 0;
+#pragma unroll
+        for (int step = STEP0; step >= 1; step >>= 1)
+          if (pos + step <= K - 1 && __dmul_rn(cs[pos + step - 1], hi) < un) pos += step;
+        if (pos < K - 1) {
+          if (un < __dmul_rn(cs[pos], lo)) zk = pos;
+          else exact = true;
+        }
+      }
+      if (exact) zk = lda_reference_draw(K, th, phiT + (size_t)wt * KP, u);
+      z[t] = zk;
+      atomicAdd(&hist[zk], 1);
+    }
+    if (cnt_kw != nullptr) {
+      const unsigned mask = __ballot_sync(0xffffffffu, active);
+      if (active) {
+        const long long key = (long long)zk * V + wt;
+        const unsigned peers = __match_any_sync(mask, key);
+        if (lane == __ffs(peers) - 1) atomicAdd(cnt_kw + key, __popc(peers));
+      }
+    }
+    __syncwarp();   // the stage is rewritten by the next chunk
+  }
+  __syncthreads();
+  if (cnt_dk != nullptr)
+    for (int k = threadIdx.x; k < K; k += blockDim.x) cnt_dk[(size_t)d * K + k] = hist[k];
+  // The last CTA to finish advances the device iteration counter, so a
+  // captured sweep can be replayed without host updates.
+  if (iter_dev != nullptr && done_ctr != nullptr) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(done_ctr, 1u);
+      if (prev == (unsigned)(D - 1)) {
+        *done_ctr = 0u;
+        *iter_dev = iter + 1u;
+        __threadfence();
+      }
+    }
+  }
+}
+
+template <int NQ>
+static int launch_lda_zq(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                         const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                         uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
+  const size_t smem = 16 * (size_t)(2 * NQ + NQ + (LDA_Z_THREADS / 32) * 32 * (2 * NQ + 1));
+  AB_CUDA(cudaFuncSetAttribute(lda_zq_kernel<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  lda_zq_kernel<NQ><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed,
+                                                    iter_dev, iter, done_ctr);
+  AB_LAUNCH_CHECK("lda_zq_kernel");
+  return AB_OK;
 }
 
 // Count statistics of a given z (conj_stat_theta / conj_stat_phi of
@@ -409,8 +546,9 @@ int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double
   lda_phi_draw_kernel<<<K * B, LDA_THREADS, 0, st>>>(K, V, Kp, B, beta, cnt_kw, phiT, clear, partial,
                                                      ticket, nrm, seed, iter_dev, iter);
   AB_LAUNCH_CHECK("lda_phi_draw_kernel");
-  lda_phi_norm_kernel<<<ceil_div(V, LDA_NORM_ROWS), LDA_THREADS, sizeof(double) * K, st>>>(
-      K, V, Kp, nrm, phiT);
+  const size_t n2 = (size_t)V * (Kp / 2);
+  const unsigned nb = (unsigned)std::min<size_t>((n2 + LDA_THREADS - 1) / LDA_THREADS, 148u * 8u);
+  lda_phi_norm_kernel<<<nb, LDA_THREADS, sizeof(double) * K, st>>>(K, V, Kp, nrm, phiT);
   AB_LAUNCH_CHECK("lda_phi_norm_kernel");
   return AB_OK;
 }
@@ -418,19 +556,24 @@ int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double
 int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
                  const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
-  // theta [KT] doubles, hist [K] ints (rounded to whole 16 bytes), then the stage
-  const size_t KT = 16 * (size_t)((K + 15) / 16);
-  const size_t base = sizeof(double) * (KT + ((K + 3) & ~3) / 2 + 2);
-  if (K <= LDA_Z_STAGE_MAX_K) {
-    const size_t smem = base + 16 * (size_t)(LDA_Z_THREADS / 32) * 32 * ((Kp / 2) | 1);
-    AB_CUDA(cudaFuncSetAttribute(lda_z_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    lda_z_kernel<true><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk,
-                                                        cnt_kw, seed, iter_dev, iter, done_ctr);
-  } else {
-    lda_z_kernel<false><<<D, LDA_Z_THREADS, base, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk,
-                                                         cnt_kw, seed, iter_dev, iter, done_ctr);
+#define AB_ZQ(nq)                                                                                      \
+  case nq:                                                                                             \
+    return launch_lda_zq<nq>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, iter_dev, iter, \
+                             done_ctr, st);
+  if (K <= LDA_ZQ_MAX_K) {
+    switch (Kp / 4) {
+      AB_ZQ(1) AB_ZQ(2) AB_ZQ(3) AB_ZQ(4) AB_ZQ(5) AB_ZQ(6) AB_ZQ(7) AB_ZQ(8)
+      AB_ZQ(9) AB_ZQ(10) AB_ZQ(11) AB_ZQ(12) AB_ZQ(13) AB_ZQ(14) AB_ZQ(15) AB_ZQ(16)
+      default: break;
+    }
+    return fail(AB_ERR_STATE, "lda: no z kernel for Kp=%d", Kp);
   }
+#undef AB_ZQ
+  // theta [KT] doubles, then hist [K] ints
+  const size_t KT = 16 * (size_t)((K + 15) / 16);
+  const size_t smem = sizeof(double) * KT + sizeof(int) * (size_t)K;
+  lda_z_kernel<<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw,
+                                               seed, iter_dev, iter, done_ctr);
   AB_LAUNCH_CHECK("lda_z_kernel");
   return AB_OK;
 }
@@ -490,6 +633,7 @@ extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int*
   int rc = check_lda_dims(D, K, V);
   if (rc) return rc;
   AB_REQUIRE(doc_off && w && theta && phiT && z, AB_ERR_ARG, "ab_lda_disc_z: null pointer");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_disc_z: phiT must be 16-byte aligned");
   AB_REQUIRE((cnt_dk == nullptr) == (cnt_kw == nullptr), AB_ERR_ARG,
              "ab_lda_disc_z: pass both count tables or neither");
   return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, nullptr,
@@ -581,6 +725,7 @@ extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
   AB_REQUIRE(desc->doc_off && desc->w && desc->z && desc->theta && desc->phiT && desc->alpha &&
                  desc->beta && desc->cnt_dk && desc->cnt_kw && desc->scratch,
              AB_ERR_ARG, "ab_lda_create: every device pointer of the descriptor is required");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(desc->phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_create: phiT must be 16-byte aligned");
   ab_lda* h = new ab_lda();
   h->d = *desc;
   h->Kp = lda_kp(desc->K);

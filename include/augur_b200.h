@@ -51,8 +51,9 @@ const char* ab_version(void);
  * LDA Gibbs (model compiler/augur/test/lda.rv, schedule
  *   ConjGibbs [theta] (*) ConjGibbs [phi] (*) DiscGibbs [z])
  * Layouts: w, z int32[T] (documents contiguous); doc_off int32[D+1];
- * theta f64[D][K]; phiT f64[V][Kp] word-major with Kp = ab_lda_phi_stride(K);
- * cnt_dk int32[D][K]; cnt_kw int32[K][V].
+ * theta f64[D][K]; phiT f64[V][Kp] word-major with Kp = ab_lda_phi_stride(K),
+ * 16-byte aligned, padding columns zero; theta and phi hold probabilities
+ * (nonnegative); cnt_dk int32[D][K]; cnt_kw int32[K][V].
  * ======================================================================= */
 
 /* Row stride (in doubles) of phiT for K topics. */

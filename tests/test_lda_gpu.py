@@ -50,7 +50,9 @@ def phiT_of(phi):
 
 
 @pytest.mark.parametrize("seed,K,V", [(0, 50, 700), (1, 50, 700), (2, 1, 30), (3, 2, 30), (4, 3, 40),
-                                      (5, 17, 90), (6, 64, 300), (7, 200, 500), (8, 1024, 64)])
+                                      (5, 17, 90), (6, 64, 300), (7, 200, 500), (8, 1024, 64),
+                                      (9, 65, 200), (10, 100, 300), (11, 128, 90), (12, 256, 400),
+                                      (13, 257, 100), (14, 8, 20), (15, 9, 50)])
 def test_disc_z_and_counts_bit_exact(orc, seed, K, V):
     off, w, theta, phi = random_problem(seed, D=60 if K > 100 else 150, K=K, V=V)
     if seed % 3 == 2:                                 # exact zeros in theta and phi
@@ -71,6 +73,26 @@ def test_disc_z_and_counts_bit_exact(orc, seed, K, V):
     c_dk, c_kw = orc.lda_conj_stat(off, w, z_ref, D, K, V)
     np.testing.assert_array_equal(cdk.cpu().numpy(), c_dk)
     np.testing.assert_array_equal(ckw.cpu().numpy(), c_kw)
+
+
+@pytest.mark.parametrize("K", [50, 100, 200, 300])
+def test_disc_z_degenerate_norms(orc, K):
+    """Tokens whose normaliser is zero, subnormal or tiny (the division-free
+    test cannot decide them) take the reference's own loop: still bit-exact."""
+    off, w, theta, phi = random_problem(20 + K, D=40, K=K, V=120)
+    theta[1::4] *= 1e-300            # products underflow to subnormals or zero
+    theta[2::4] *= 1e-150            # norm near 1e-150 * phi: tiny but normal
+    phi[:, 7] = 0.0                  # word 7: every product zero, norm 0
+    phi[:, 9] = 1e-310               # word 9: subnormal phi entries
+    D, K = theta.shape
+    V = phi.shape[1]
+    phiT, _ = phiT_of(phi)
+    z = torch.zeros(len(w), dtype=torch.int32, device="cuda")
+    g = [dev(off, torch.int32), dev(w, torch.int32), dev(theta, torch.float64), dev(phiT, torch.float64)]
+    N.check(N.lib().ab_lda_disc_z(D, K, V, N.ptr(g[0]), N.ptr(g[1]), N.ptr(g[2]), N.ptr(g[3]),
+                                  N.ptr(z), None, None, 3, 1, N.stream_ptr()), "disc_z")
+    z_ref = orc.lda_disc_z(off, w, theta, phi, np.zeros(len(w), np.int32), 3, 1)
+    np.testing.assert_array_equal(z.cpu().numpy(), z_ref)
 
 
 def test_count_kernel(orc):
