@@ -85,10 +85,14 @@ _SIGS = {
     "ab_hlrb_transpose": (i32, [i32, i32, vp, i32, vp, vp]),
     "ab_hlrb_workspace_bytes": (sz, [i32, i32, i32]),
     "ab_hlrb_logp_grad": (i32, [vp, i32, vp, i32, vp, vp, i32, vp, vp, vp]),
+    "ab_hlrb_workspace_bytes_cfg": (sz, [i32, i32, i32, vp]),
+    "ab_hlrb_logp_grad_cfg": (i32, [vp, i32, vp, i32, vp, vp, i32, vp, vp, vp, vp]),
     "ab_nutsb_state_bytes": (sz, [i32, i32, i32]),
+    "ab_nutsb_reset_history": (i32, [vp, i32, i32, i32, vp]),
     "ab_nutsb_init": (i32, [vp, i32, i32, i32, vp, vp, vp, u32, vp]),
     "ab_nutsb_thprop": (i32, [vp, i32, i32, i32, vp, vp, vp]),
     "ab_nutsb_advance": (i32, [vp, i32, i32, i32, i32, f64, u64, u32, vp, vp, vp]),
+    "ab_nutsb_advance_variant": (i32, [vp, i32, i32, i32, i32, f64, u64, u32, i32, vp, vp, vp]),
     "ab_nutsb_info": (i32, [vp, i32, i32, i32, vp, vp]),
     "ab_hmcb_begin": (i32, [vp, vp]),
     "ab_hmcb_step": (i32, [vp, vp, vp]),

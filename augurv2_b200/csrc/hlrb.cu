@@ -39,29 +39,51 @@ namespace ab {
 namespace {
 
 constexpr int FWD_BN = 128;   // data rows per forward tile
-constexpr int FWD_WARPS = 8;  // epilogue warps of the forward pass (two column groups)
-constexpr int FWD_GROUPS = FWD_WARPS / 4;
-// gradient columns per backward tile: the narrowest of 32 / 64 / 128 that
-// covers D (wider D takes several 128-column tiles)
+constexpr int FWD_MAX_GROUPS = 2;   // column groups of the forward epilogue (8 warps)
+// gradient columns per backward tile by default: the narrowest of 32 / 64 /
+// 128 that covers D (wider D takes several 128-column tiles)
 inline int bwd_bn(int D) { return D <= 32 ? 32 : (D <= 64 ? 64 : 128); }
 
 inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
 inline size_t align256(size_t a) { return (a + 255) & ~size_t(255); }
 
+// Launch shape of one pass: the built-in choice, or the fields a caller (the
+// autotuner) set in ab_hlrb_config.
+struct Launch {
+  int fwd_warps, bn, splits;
+};
+
 struct Layout {
-  int Np, Dp, fwd_tiles, splits, ldw;
+  int Np, Dp, fwd_tiles, groups, splits, ldw, bn;
   size_t off_t3, off_r3, off_ll, off_w, total;
 };
 
-Layout layout(int N, int D, int C) {
+int check_config(const ab_hlrb_config* cfg) {
+  if (!cfg) return AB_OK;
+  AB_REQUIRE(cfg->fwd_warps == 0 || cfg->fwd_warps == 4 || cfg->fwd_warps == 8, AB_ERR_ARG,
+             "hlrb: fwd_warps must be 0, 4 or 8 (got %d)", cfg->fwd_warps);
+  AB_REQUIRE(cfg->bwd_bn == 0 || cfg->bwd_bn == 32 || cfg->bwd_bn == 64 || cfg->bwd_bn == 128, AB_ERR_ARG,
+             "hlrb: bwd_bn must be 0, 32, 64 or 128 (got %d)", cfg->bwd_bn);
+  AB_REQUIRE(cfg->bwd_splits >= 0, AB_ERR_ARG, "hlrb: bwd_splits must be >= 0 (got %d)", cfg->bwd_splits);
+  return AB_OK;
+}
+
+Layout layout(int N, int D, int C, const ab_hlrb_config* cfg) {
+  Launch q{8, bwd_bn(D), 0};
+  if (cfg) {
+    if (cfg->fwd_warps) q.fwd_warps = cfg->fwd_warps;
+    if (cfg->bwd_bn) q.bn = cfg->bwd_bn;
+    q.splits = cfg->bwd_splits;
+  }
   Layout L;
   L.Np = round_up(N, 64);
   L.Dp = round_up(D, 64);
   L.fwd_tiles = (N + FWD_BN - 1) / FWD_BN;
-  const int bn = bwd_bn(D);
-  const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + bn - 1) / bn);
+  L.groups = q.fwd_warps / 4;
+  L.bn = q.bn;
+  const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + L.bn - 1) / L.bn);
   const int kb = L.Np / tc::BK;
-  int sp = tc::sm_count() / tiles;
+  int sp = q.splits > 0 ? q.splits : tc::sm_count() / tiles;
   if (sp < 1) sp = 1;
   if (sp > kb) sp = kb;
   // the kernel's own split arithmetic (whole K steps per split)
@@ -74,7 +96,7 @@ Layout layout(int N, int D, int C) {
   L.off_r3 = o;
   o = align256(o + (size_t)C * 3 * L.Np * 2);
   L.off_ll = o;
-  o = align256(o + (size_t)L.fwd_tiles * FWD_GROUPS * C * 4);
+  o = align256(o + (size_t)L.fwd_tiles * FWD_MAX_GROUPS * C * 4);
   L.off_w = o;
   o = align256(o + (size_t)L.splits * C * L.ldw * 4);
   L.total = o;
@@ -128,13 +150,14 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
 // Forward epilogue: rows are chains, columns are data rows.  LL: sum the
 // log-likelihood terms; R: write the residual parts for the backward pass
 // (a leapfrog step that only needs the gradient skips the LL work).
-template <bool LL, bool R>
+template <bool LL, bool R, int W>
 struct FwdEpi {
   static constexpr int kSmem = FWD_BN * 4;
-  static constexpr int kWarps = FWD_WARPS;
+  static constexpr int kWarps = W;
+  static constexpr int kGroups = W / 4;
   const int* y;
   __nv_bfloat16* r3;   // NULL: log density only
-  float* llpart;       // [fwd_tiles][FWD_GROUPS][C]
+  float* llpart;       // [fwd_tiles][kGroups][C]
   int N, Np, C;
   // per-thread state
   const int* ys;
@@ -144,7 +167,7 @@ struct FwdEpi {
   __device__ void begin(int, int nt, int, char* smem, int etid) {
     int* s = reinterpret_cast<int*>(smem);
     n0 = nt * FWD_BN;
-    for (int j = etid; j < FWD_BN; j += 32 * FWD_WARPS) {
+    for (int j = etid; j < FWD_BN; j += 32 * W) {
       const int n = n0 + j;
       s[j] = n < N ? y[n] : -1;
     }
@@ -206,7 +229,7 @@ struct FwdEpi {
   }
 
   __device__ void end(int, int nt, int, int c, bool ok, int cg) {
-    if (LL && ok) llpart[((size_t)nt * FWD_GROUPS + cg) * C + c] = acc;
+    if (LL && ok) llpart[((size_t)nt * kGroups + cg) * C + c] = acc;
   }
 };
 
@@ -274,10 +297,25 @@ __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_
 
 }  // namespace
 
+template <int W>
+int launch_forward(const ab_hlrb_model* m, const CUtensorMap& ma, const CUtensorMap& mb, const tc::Shape& fs,
+                   bool logp, bool grad, __nv_bfloat16* r3, float* llp, int Np, int C, int* err, cudaStream_t st) {
+  if (logp && grad) {
+    FwdEpi<true, true, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+    return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  }
+  if (logp) {
+    FwdEpi<true, false, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+    return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  }
+  FwdEpi<false, true, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+  return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+}
+
 int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad, int ldg,
-                   void* work, int* err, cudaStream_t st) {
+                   const ab_hlrb_config* cfg, void* work, int* err, cudaStream_t st) {
   const int N = m->N, D = m->D;
-  const Layout L = layout(N, D, C);
+  const Layout L = layout(N, D, C, cfg);
   char* wb = static_cast<char*>(work);
   __nv_bfloat16* t3 = reinterpret_cast<__nv_bfloat16*>(wb + L.off_t3);
   __nv_bfloat16* r3 = reinterpret_cast<__nv_bfloat16*>(wb + L.off_r3);
@@ -292,22 +330,14 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
   if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
   const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), FWD_BN);
-  if (logp && grad) {
-    FwdEpi<true, true> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
-    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
-  } else if (logp) {
-    FwdEpi<true, false> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
-    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
-  } else {
-    FwdEpi<false, true> fe{m->y, r3, llp, N, L.Np, C, nullptr, 0, 0.0f, 0.0f};
-    rc = tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
-  }
+  rc = L.groups == 1 ? launch_forward<4>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
+                     : launch_forward<8>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st);
   if (rc) return rc;
 
   if (grad) {
     const int nb = L.Np / 64;
     if ((rc = tc::encode_2d_bf16(&ma, r3, (uint64_t)nb * 3 * C, 64, 64, tc::BM))) return rc;
-    const int bn = bwd_bn(D);
+    const int bn = L.bn;
     if ((rc = tc::encode_2d_bf16(&mb, m->Xt, (uint64_t)nb * D, 64, 64, bn))) return rc;
     GradEpi ge{w, C, D, L.ldw, 0};
     const tc::Shape bs = tc::make_shape(C, D, N, L.splits, tc::k_blocked(3, C), tc::k_blocked(1, D), bn);
@@ -317,7 +347,7 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
     else rc = tc::launch_gemm<128, 3, 1>(ma, mb, bs, ge, err, st);
     if (rc) return rc;
   }
-  hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles * FWD_GROUPS, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
+  hlrb_finish_kernel<<<C, 256, 0, st>>>(C, D, L.fwd_tiles * L.groups, L.splits, L.ldw, llp, w, theta, ldt, m->prior,
                                         m->prior_a, m->prior_b, logp, grad, ldg);
   AB_LAUNCH_CHECK("hlrb_finish_kernel");
   return AB_OK;
@@ -334,7 +364,7 @@ int hlrb_check_model(const ab_hlrb_model* m) {
   return AB_OK;
 }
 
-size_t hlrb_workspace_bytes(int N, int D, int C) { return layout(N, D, C).total; }
+size_t hlrb_workspace_bytes(int N, int D, int C, const ab_hlrb_config* cfg) { return layout(N, D, C, cfg).total; }
 
 }  // namespace ab
 
@@ -357,16 +387,28 @@ extern "C" int ab_hlrb_transpose(int N, int D, const void* X, int ldx, void* Xt,
 
 extern "C" size_t ab_hlrb_workspace_bytes(int N, int D, int C) {
   if (N <= 0 || D <= 0 || C <= 0) return 0;
-  return hlrb_workspace_bytes(N, D, C);
+  return hlrb_workspace_bytes(N, D, C, nullptr);
 }
 
-extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp,
-                                 float* grad, int ldg, void* work, int* err, void* stream) {
+extern "C" size_t ab_hlrb_workspace_bytes_cfg(int N, int D, int C, const ab_hlrb_config* cfg) {
+  if (N <= 0 || D <= 0 || C <= 0 || check_config(cfg)) return 0;
+  return hlrb_workspace_bytes(N, D, C, cfg);
+}
+
+extern "C" int ab_hlrb_logp_grad_cfg(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp,
+                                     float* grad, int ldg, const ab_hlrb_config* cfg, void* work, int* err,
+                                     void* stream) {
   int rc = hlrb_check_model(m);
   if (rc) return rc;
+  if ((rc = check_config(cfg))) return rc;
   AB_REQUIRE(C > 0 && C <= 65535, AB_ERR_ARG, "ab_hlrb_logp_grad: C must be 1..65535");
   AB_REQUIRE(theta && work && (logp || grad), AB_ERR_ARG, "ab_hlrb_logp_grad: null pointer");
   AB_REQUIRE(ldt >= m->D && (!grad || ldg >= m->D), AB_ERR_ARG, "ab_hlrb_logp_grad: leading dimension too small");
   AB_REQUIRE((reinterpret_cast<uintptr_t>(work) & 255) == 0, AB_ERR_ARG, "ab_hlrb_logp_grad: workspace must be 256-byte aligned");
-  return hlrb_logp_grad(m, C, theta, ldt, logp, grad, ldg, work, err, as_stream(stream));
+  return hlrb_logp_grad(m, C, theta, ldt, logp, grad, ldg, cfg, work, err, as_stream(stream));
+}
+
+extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp,
+                                 float* grad, int ldg, void* work, int* err, void* stream) {
+  return ab_hlrb_logp_grad_cfg(m, C, theta, ldt, logp, grad, ldg, nullptr, work, err, stream);
 }

@@ -361,8 +361,7 @@ __device__ __noinline__ int lda_reference_draw(int K, const double* __restrict__
 // NaN norm) runs the reference's loop itself (lda_reference_draw).  theta and
 // phi are probabilities (nonnegative), which keeps c_k monotone.
 // Counts of the new z: the document's row of cnt_dk is accumulated in shared
-// memory and stored whole; cnt_kw receives warp-aggregated atomic increments
-// (lanes with the same (z, w) key elect one leader that adds the group size).
+// memory and stored whole; cnt_kw receives one atomic increment per token.
 // ---------------------------------------------------------------------------
 constexpr int LDA_ZQ_MAX_K = 64;
 
@@ -447,14 +446,9 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
       z[t] = zk;
       atomicAdd(&hist[zk], 1);
     }
-    if (cnt_kw != nullptr) {
-      const unsigned mask = __ballot_sync(0xffffffffu, active);
-      if (active) {
-        const long long key = (long long)zk * V + wt;
-        const unsigned peers = __match_any_sync(mask, key);
-        if (lane == __ffs(peers) - 1) atomicAdd(cnt_kw + key, __popc(peers));
-      }
-    }
+    // topic-word counts: one fire-and-forget atomic per token (measured
+    // faster than aggregating equal (z, w) keys across the warp first)
+    if (cnt_kw != nullptr && active) atomicAdd(cnt_kw + (size_t)zk * V + wt, 1);
     __syncwarp();   // the stage is rewritten by the next chunk
   }
   __syncthreads();

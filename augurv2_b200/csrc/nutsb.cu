@@ -78,6 +78,7 @@ __device__ __forceinline__ void copy_vec(float* dst, const float* src, int P) {
 // Everything the advance kernel touches, by chain.
 struct NutsbDev {
   int C, P, max_depth, hist_cap;
+  int standard;               // 0: the reference's selection (quirks), 1: Hoffman & Gelman's
   uint64_t seed;
   uint32_t comp;
   float eps;
@@ -208,6 +209,7 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
         S.n = 1;
         S.jd = 0;
         S.s = 1;
+        S.f_cpy = 0;
         S.leaves = 0;
         S.overflow = 0;
         S.tp_h = -1;
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
     if (mode == M_DOUBLING) {
       const double u = draw_u();
       if (tid == 0) {
-        S.f_cpy = 0;
+        if (!dv.standard) S.f_cpy = 0;   // the reference keeps only the last doubling's pick
         S.ts_h = -1;
         S.ms_h = -1;
         S.dir = u < 0.5 ? 0 : 1;
@@ -339,8 +341,13 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
       copy_vec(minus ? gm : gp, gprop, P);
       const int pp = pop_slot(&S.tp_h);
       if (rs == 1) {
-        const unsigned ratio = (unsigned)(((double)rn) / n_s);   // augur_min on unsigned
-        const double bias = (double)(ratio < 1u ? ratio : 1u);
+        double bias;
+        if (dv.standard) {
+          bias = fmin(1.0, ((double)rn) / n_s);
+        } else {
+          const unsigned ratio = (unsigned)(((double)rn) / n_s);   // augur_min on unsigned
+          bias = (double)(ratio < 1u ? ratio : 1u);
+        }
         if (draw_u() < bias) {
           copy_vec(sel, tp + (size_t)pp * P, P);
           copy_vec(selg, tpg + (size_t)pp * P, P);
@@ -364,7 +371,8 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
         if (tid == 0) S.mode = M_DOUBLING;
         continue;
       }
-      // iteration done: the draw is th0 (replaced by the last doubling's proposal)
+      // iteration done: the draw is th0, replaced by the selected proposal (the
+      // reference: the last doubling's pick only; standard: the latest pick)
       if (S.f_cpy) {
         copy_vec(th0, sel, P);
         copy_vec(g0, selg, P);
@@ -456,6 +464,16 @@ __global__ void nutsb_info_kernel(NutsbDev d, double* info) {
   o[4] = s.iter;
   o[5] = s.ndraws > 0 ? s.depth_sum / s.ndraws : 0.0;
 }
+
+// Forget the recorded draws (end of warm-up): every chain keeps its position,
+// tree state and iteration counter; its draw count and depth statistics
+// restart from zero.
+__global__ void nutsb_reset_history_kernel(NutsbDev d) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= d.C) return;
+  d.st[c].ndraws = 0;
+  d.st[c].depth_sum = 0.0;
+}
 }  // namespace
 }  // namespace ab
 
@@ -498,6 +516,15 @@ extern "C" int ab_nutsb_thprop(void* mem, int C, int P, int hist_cap, float** th
 
 extern "C" int ab_nutsb_advance(void* mem, int C, int P, int hist_cap, int max_depth, double eps, uint64_t seed,
                                 uint32_t comp, const double* logp_new, const float* g_new, void* stream) {
+  return ab_nutsb_advance_variant(mem, C, P, hist_cap, max_depth, eps, seed, comp, AB_NUTS_REFERENCE, logp_new, g_new,
+                                  stream);
+}
+
+extern "C" int ab_nutsb_advance_variant(void* mem, int C, int P, int hist_cap, int max_depth, double eps,
+                                        uint64_t seed, uint32_t comp, int variant, const double* logp_new,
+                                        const float* g_new, void* stream) {
+  AB_REQUIRE(variant == AB_NUTS_REFERENCE || variant == AB_NUTS_STANDARD, AB_ERR_ARG,
+             "ab_nutsb_advance: unknown variant %d", variant);
   AB_REQUIRE(mem && logp_new && g_new && C > 0 && P > 0, AB_ERR_ARG, "ab_nutsb_advance: bad arguments");
   AB_REQUIRE(max_depth >= 1 && max_depth <= 14, AB_ERR_ARG, "ab_nutsb_advance: max_depth must be 1..14");
   AB_REQUIRE(eps > 0.0 && eps < 1e5, AB_ERR_ARG, "ab_nutsb_advance: bad step size");
@@ -508,6 +535,7 @@ extern "C" int ab_nutsb_advance(void* mem, int C, int P, int hist_cap, int max_d
   d.comp = comp;
   d.logp_new = logp_new;
   d.g_new = g_new;
+  d.standard = variant == AB_NUTS_STANDARD;
   nutsb_advance_kernel<<<C, NB_THREADS, 0, as_stream(stream)>>>(d);
   AB_LAUNCH_CHECK("nutsb_advance_kernel");
   return AB_OK;
@@ -518,5 +546,13 @@ extern "C" int ab_nutsb_info(void* mem, int C, int P, int hist_cap, double* info
   NutsbDev d = layout(mem, C, P, hist_cap);
   nutsb_info_kernel<<<ceil_div(C, 128), 128, 0, as_stream(stream)>>>(d, info);
   AB_LAUNCH_CHECK("nutsb_info_kernel");
+  return AB_OK;
+}
+
+extern "C" int ab_nutsb_reset_history(void* mem, int C, int P, int hist_cap, void* stream) {
+  AB_REQUIRE(mem && C > 0 && P > 0 && hist_cap >= 0, AB_ERR_ARG, "ab_nutsb_reset_history: bad arguments");
+  NutsbDev d = layout(mem, C, P, hist_cap);
+  nutsb_reset_history_kernel<<<ceil_div(C, 128), 128, 0, as_stream(stream)>>>(d);
+  AB_LAUNCH_CHECK("nutsb_reset_history_kernel");
   return AB_OK;
 }

@@ -64,29 +64,53 @@ class HlrbData:
         self.c = HlrbModelC(self.N, self.D, self.D, self.X.data_ptr(), self.Xt.data_ptr(), self.y.data_ptr(),
                             self.prior, self.pa, self.pb)
         self.device = self.X.device
+        self.config = None     # ab_hlrb_config chosen by autotune(); None: built-in shapes
 
-    def workspace(self, C_):
-        nb = int(N.lib().ab_hlrb_workspace_bytes(self.N, self.D, C_))
+    def workspace(self, C_, config=None):
+        """Device workspace for C_ chains under a launch shape (default: the
+        shape chosen by autotune(), else the built-in one)."""
+        cfg = self.config if config is None else config
+        nb = int(N.lib().ab_hlrb_workspace_bytes_cfg(self.N, self.D, C_, C.byref(cfg) if cfg is not None else None))
+        if nb == 0:
+            raise N.AugurError("ab_hlrb_workspace_bytes_cfg: bad sizes or launch shape")
         return torch.empty(nb, dtype=torch.uint8, device=self.device)
 
+    def autotune(self, C_, grad=True, tuner=None):
+        """Time the candidate launch shapes of the pass for C_ chains on this
+        GPU (augurv2_b200.autotune) and use the fastest from now on.  Call it
+        before creating samplers: their workspaces are sized for the shape in
+        force when they are made."""
+        from . import autotune as T
+        tuner = tuner or T.default_tuner()
+        self.config = T.HlrbConfigC.of(tuner.hlrb(self, C_, grad))
+        return self.config.as_dict()
+
     def logp_grad(self, theta, grad=True, logp_out=None, grad_out=None, work=None, err=None, stream=None,
-                  logp=True):
+                  logp=True, config=None):
         """(logp [C] f64 or None, grad [C, D] f32 or None) at theta [C, D] f32
-        (device); logp=False skips the log-likelihood terms."""
+        (device); logp=False skips the log-likelihood terms.  `config` (an
+        autotune.HlrbConfigC) overrides the launch shape for this call; the
+        workspace must have been sized for the same shape."""
         C_ = theta.shape[0]
         if not (grad or logp):
             raise ValueError("nothing to compute")
+        cfg = self.config if config is None else config
         if logp and logp_out is None:
             logp_out = torch.empty(C_, dtype=torch.float64, device=self.device)
         if grad and grad_out is None:
             grad_out = torch.empty((C_, self.D), dtype=torch.float32, device=self.device)
         if work is None:
-            work = self.workspace(C_)
-        N.check(N.lib().ab_hlrb_logp_grad(C.byref(self.c), C_, N.ptr(theta), theta.stride(0),
-                                          N.ptr(logp_out) if logp else None,
-                                          N.ptr(grad_out) if grad else None, self.D, N.ptr(work),
-                                          N.ptr(err) if err is not None else None, N.stream_ptr(stream)),
-                "ab_hlrb_logp_grad")
+            work = self.workspace(C_, cfg)
+        need = int(N.lib().ab_hlrb_workspace_bytes_cfg(self.N, self.D, C_, C.byref(cfg) if cfg is not None else None))
+        if work.numel() * work.element_size() < need:
+            raise N.AugurError("hlrb workspace holds %d bytes, this launch shape needs %d"
+                               % (work.numel() * work.element_size(), need))
+        N.check(N.lib().ab_hlrb_logp_grad_cfg(C.byref(self.c), C_, N.ptr(theta), theta.stride(0),
+                                              N.ptr(logp_out) if logp else None,
+                                              N.ptr(grad_out) if grad else None, self.D,
+                                              C.byref(cfg) if cfg is not None else None, N.ptr(work),
+                                              N.ptr(err) if err is not None else None, N.stream_ptr(stream)),
+                "ab_hlrb_logp_grad_cfg")
         return (logp_out if logp else None), (grad_out if grad else None)
 
 
@@ -508,9 +532,21 @@ class BatchedNuts:
     next leaf (ab_nutsb_advance) and one tensor-core pass evaluates the log
     density and gradient at all chains' leaf positions.  Chains restart as
     soon as their tree terminates, each recording its draws (up to
-    `hist_cap`).  One round can be captured as a CUDA graph."""
+    `hist_cap`).  One round can be captured as a CUDA graph.
 
-    def __init__(self, data, C_, eps, max_depth=10, seed=0, init=None, hist_cap=256, comp=0, iter0=0):
+    variant="reference" selects each iteration's draw as the reference does
+    (the last doubling's pick only, with the truncated acceptance ratio), so
+    draws equal the reference sampler's; variant="standard" uses Hoffman &
+    Gelman's rule (the latest accepted pick of any doubling, probability
+    min(1, n'/n)), which moves the chain on far more iterations."""
+
+    VARIANTS = {"reference": 0, "standard": 1}
+
+    def __init__(self, data, C_, eps, max_depth=10, seed=0, init=None, hist_cap=256, comp=0, iter0=0,
+                 variant="reference"):
+        if variant not in self.VARIANTS:
+            raise ValueError("variant must be 'reference' or 'standard'")
+        self.variant = variant
         self.data, self.C, self.D = data, int(C_), data.D
         self.eps, self.max_depth, self.seed, self.comp = float(eps), int(max_depth), int(seed), int(comp)
         self.hist_cap = int(hist_cap)
@@ -545,9 +581,10 @@ class BatchedNuts:
         del f32
 
     def _round(self, stream=None):
-        N.check(N.lib().ab_nutsb_advance(N.ptr(self.mem), self.C, self.D, self.hist_cap, self.max_depth, self.eps,
-                                         self.seed, self.comp, N.ptr(self.logp_new), N.ptr(self.g_new),
-                                         N.stream_ptr(stream)), "ab_nutsb_advance")
+        N.check(N.lib().ab_nutsb_advance_variant(N.ptr(self.mem), self.C, self.D, self.hist_cap, self.max_depth,
+                                                 self.eps, self.seed, self.comp, self.VARIANTS[self.variant],
+                                                 N.ptr(self.logp_new), N.ptr(self.g_new), N.stream_ptr(stream)),
+                "ab_nutsb_advance_variant")
         self.data.logp_grad(self.thprop, True, self.logp_new, self.g_new, self.work, self.err, stream)
 
     def capture(self, stream=None):
@@ -567,6 +604,11 @@ class BatchedNuts:
                 self._round()
             self.rounds += 1
 
+    def reset_history(self, stream=None):
+        """End of warm-up: forget the recorded draws, keep every chain's state."""
+        N.check(N.lib().ab_nutsb_reset_history(N.ptr(self.mem), self.C, self.D, self.hist_cap,
+                                               N.stream_ptr(stream)), "ab_nutsb_reset_history")
+
     def info(self):
         N.check(N.lib().ab_nutsb_info(N.ptr(self.mem), self.C, self.D, self.hist_cap, N.ptr(self.info_buf),
                                       N.stream_ptr()), "ab_nutsb_info")
@@ -579,3 +621,105 @@ class BatchedNuts:
             raise N.AugurError("batched NUTS: a chain reported an error")
         n = int(min(inf[:, 0].min(), self.hist_cap))
         return self.hist[:, :n].permute(1, 0, 2).cpu().numpy()
+
+
+def lpt_assign(costs, n_streams, keys=None):
+    """Longest-processing-time-first assignment of jobs to streams: the
+    costliest job goes to the least-loaded stream, and so on.  Returns
+    {key: stream index} (keys default to 0..len(costs)-1)."""
+    keys = list(range(len(costs))) if keys is None else list(keys)
+    load = [0.0] * int(n_streams)
+    out = {}
+    for c, k in sorted(zip(costs, keys), key=lambda ck: -ck[0]):
+        q = min(range(len(load)), key=lambda j: load[j])
+        out[k] = q
+        load[q] += c
+    return out
+
+
+class NutsPool:
+    """Many BatchedNuts samplers of uneven cost (model instances with their
+    own N and D) sharing one GPU.
+
+    Each sampler's round (leaf advance + tensor-core pass) is a captured CUDA
+    graph; rounds are replayed in blocks over a few streams, samplers
+    assigned to streams longest-processing-time first on their cost per
+    round and re-balanced every block among the samplers still running.
+    Shares: by default every running sampler replays `block` rounds per
+    block; with share="time" a sampler replays rounds in inverse proportion
+    to its cost per round (N * D plus a fixed launch overhead, up to
+    MAX_SHARE times the block).  A sampler stops once every one of its chains
+    has `min_draws` draws (or its draw history is full, or it ran
+    `max_rounds` rounds in this call); the pool returns when all have
+    stopped."""
+
+    OVERHEAD = 5.0e6      # fixed cost of a round (launch latency), in N * D units
+    MAX_SHARE = 4         # a block gives a sampler at most this many times `block` rounds
+                          # (bounds the host time spent enqueueing graph launches)
+
+    def __init__(self, samplers, streams=8, costs=None):
+        self.samplers = list(samplers)
+        self.streams = [torch.cuda.Stream() for _ in range(int(streams))]
+        self.costs = [float(c) for c in costs] if costs is not None else \
+            [float(s.data.N) * float(s.data.D) + self.OVERHEAD for s in self.samplers]
+        self.rounds = [0] * len(self.samplers)
+        self.done = [False] * len(self.samplers)
+        for i, s in enumerate(self.samplers):
+            if s.graph is None:
+                st = self.streams[i % len(self.streams)]
+                with torch.cuda.stream(st):
+                    s.capture(st)
+                self.rounds[i] = s.rounds
+        torch.cuda.synchronize()
+
+    def _assign(self, active, reps):
+        return lpt_assign([self.costs[i] * reps[i] for i in active], len(self.streams), keys=active)
+
+    def reset(self):
+        """Start a new phase: every sampler runs again and its recorded draws
+        are forgotten (the chains keep their states)."""
+        for s in self.samplers:
+            s.reset_history()
+        self.done = [False] * len(self.samplers)
+
+    def draws(self, i):
+        """Draws recorded by sampler i's slowest chain."""
+        return int(self.samplers[i].info()[:, 0].min())
+
+    def run(self, min_draws, max_rounds, block=25, share="equal"):
+        """Replay rounds until every sampler has min_draws draws per chain;
+        returns the number of rounds each sampler ran in this call.  share:
+        "equal" (block rounds each per block) or "time" (rounds per block in
+        inverse proportion to cost: cheap samplers keep drawing while the
+        expensive ones finish, at the price of competing with them)."""
+        cur = torch.cuda.current_stream()
+        start = list(self.rounds)
+        ran = lambda i: self.rounds[i] - start[i]
+        cmax = max(self.costs) if self.costs else 1.0
+        counts = [0] * len(self.samplers)
+        self.done = [False] * len(self.samplers)
+        while True:
+            active = [i for i, d in enumerate(self.done) if not d]
+            if not active:
+                break
+            reps = {i: (block if share == "equal" else
+                        max(1, min(self.MAX_SHARE * block, int(round(block * cmax / self.costs[i])))))
+                    for i in active}
+            reps = {i: max(0, min(r, max_rounds - ran(i))) for i, r in reps.items()}
+            where = self._assign(active, reps)
+            for st in self.streams:
+                st.wait_stream(cur)
+            for i in active:
+                with torch.cuda.stream(self.streams[where[i]]):
+                    for _ in range(reps[i]):
+                        self.samplers[i].graph.replay()
+                self.rounds[i] += reps[i]
+            for st in self.streams:
+                cur.wait_stream(st)
+            for i in active:
+                s = self.samplers[i]
+                s.rounds = self.rounds[i]
+                counts[i] = self.draws(i)
+                if ran(i) >= max_rounds or counts[i] >= min(min_draws, s.hist_cap):
+                    self.done[i] = True
+        return [ran(i) for i in range(len(self.samplers))]

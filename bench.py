@@ -42,6 +42,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 K_TOPICS, V_WORDS, D_DOCS, MEAN_LEN, ALPHA, BETA, DATA_SEED = 50, 10000, 2000, 200, 0.1, 0.01, 0
+# DRAM bytes of one z-kernel launch on this workload, from the ncu capture summarised in
+# profiles/lda_zq_kernel_k50_v10000_d2000.md (phi and the count tables stay in L2)
+Z_KERNEL_DRAM_BYTES = 6_703_104
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -133,6 +136,17 @@ def measured_tensor_peak(sustained=False):
 
 
 HLR_N, HLR_D, HLR_C, HLR_L, HLR_SEED = 2_000_000, 512, 256, 10, 5
+_TUNER = None
+
+
+def bench_tuner():
+    """The launch-shape autotuner for this run: its cache lives in the run's
+    working directory (a fresh box tunes once, outside every timed region)."""
+    global _TUNER
+    if _TUNER is None:
+        from augurv2_b200 import autotune as T
+        _TUNER = T.Autotuner(cache_path=os.path.join(os.getcwd(), ".augur_autotune.json"), reps=3, warmup=1)
+    return _TUNER
 
 
 def run_hlr_pass(n_rows, steps, warmup):
@@ -143,6 +157,7 @@ def run_hlr_pass(n_rows, steps, warmup):
     from augurv2_b200 import hlrb as H
     X, y, beta = H.synthetic(n_rows, HLR_D, seed=HLR_SEED)
     d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    tuned = d.autotune(HLR_C, tuner=bench_tuner())
     th = torch.as_tensor(beta, device="cuda").repeat(HLR_C, 1).contiguous()
     work = d.workspace(HLR_C)
     err = torch.zeros(1, dtype=torch.int32, device="cuda")
@@ -166,7 +181,7 @@ def run_hlr_pass(n_rows, steps, warmup):
             "tflops": {"forward": fwd / (out["logp"] / 1e3) / 1e12, "forward+backward": 2 * fwd / (out["grad"] / 1e3) / 1e12},
             "peak": peak, "peak_source": kind,
             "config": {"workload": "hlr_pass_n%d_d%d_c%d" % (n_rows, HLR_D, HLR_C), "N": n_rows, "D": HLR_D,
-                       "chains": HLR_C}}
+                       "chains": HLR_C, "launch_shape": tuned}}
 
 
 # ---- config 1: small HLR, plain HMC (the reference's CPU case) -------------
@@ -264,22 +279,28 @@ def nuts_instances(n_inst=NUTS_INST, seed=0):
     return [(int(n), int(d)) for n, d in zip(Ns, Ds)]
 
 
-def run_hlr_nuts(rounds=600, n_inst=NUTS_INST, chains=NUTS_C, streams=8, hist_cap=128):
+def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INST, chains=NUTS_C, streams=8,
+                 hist_cap=128, variants=("reference", "standard"), share="equal"):
     """64 HLR instances (X ~ N(0,1) bf16, sigma^2 ~ InvGamma(1,1),
     beta ~ N(0, sigma^2 I), y ~ Bern(sigmoid(X beta)); sigma^2 held at its
     generating value), 512 NUTS chains each, max tree depth 10.  Every round
     each instance advances all its chains to their next leaf and evaluates
-    one batched tensor-core pass; an instance's round is one CUDA graph, the
-    instances' graphs are spread over `streams` streams.  min-ESS/s per
-    instance = min-ESS of its draws / the whole run's device time; the line
-    reports the minimum over instances."""
+    one batched tensor-core pass; an instance's round is one CUDA graph, and
+    a NutsPool replays the instances' rounds over `streams` streams until
+    every chain of every instance has `min_draws` draws (instances with deep
+    trees run more rounds), after an untimed warm-up of `warmup_draws` draws
+    per chain whose draws are discarded.  min-ESS/s per instance = min-ESS
+    of its draws / the whole run's device time; the line reports the minimum
+    over instances.  Each selection rule in `variants` runs on the same data
+    and starting points; the first is the line's value (the reference's
+    rule), the others are reported beside it."""
     import torch
     from augurv2_b200 import hlrb as H
     from augurv2_b200.diagnostics import ess
     specs = nuts_instances(n_inst)
     rng = np.random.default_rng(42)
-    insts = []
-    flops_round = 0.0
+    datas = []
+    flops_round_i = []
     for i, (Ni, Di) in enumerate(specs):
         s2 = 1.0 / rng.gamma(1.0, 1.0)
         beta = (rng.standard_normal(Di) * np.sqrt(s2)).astype(np.float32)
@@ -291,50 +312,61 @@ def run_hlr_nuts(rounds=600, n_inst=NUTS_INST, chains=NUTS_C, streams=8, hist_ca
         w = (torch.sigmoid(t) * (1 - torch.sigmoid(t))).mean().item()
         eps = 0.6 / np.sqrt(Ni * w + 1.0 / s2)       # ~ 0.6 of the posterior scale
         d = H.HlrbData(X, y, prior="normal", var=s2)
+        d.autotune(chains, tuner=bench_tuner())
         init = beta[None] + (0.1 * eps) * rng.standard_normal((chains, Di)).astype(np.float32)
-        nuts = H.BatchedNuts(d, chains, eps=eps, max_depth=NUTS_DEPTH, seed=7 + i, init=init, hist_cap=hist_cap)
-        insts.append((d, nuts))
-        flops_round += 12.0 * Ni * Di * chains
-    sts = [torch.cuda.Stream() for _ in range(streams)]
-    for i, (_, nuts) in enumerate(insts):
-        with torch.cuda.stream(sts[i % streams]):
-            nuts.capture(sts[i % streams])
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for st in sts:
-        st.wait_stream(torch.cuda.current_stream())
-    for r in range(rounds):
-        for i, (_, nuts) in enumerate(insts):
-            with torch.cuda.stream(sts[i % streams]):
-                nuts.graph.replay()
-    for st in sts:
-        torch.cuda.current_stream().wait_stream(st)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
-    per = []
-    for i, (d, nuts) in enumerate(insts):
-        dr = nuts.draws()
-        inf = nuts.info()
-        e = ess(dr) if dr.shape[0] >= 4 else np.zeros(d.D)
-        per.append({"N": d.N, "D": d.D, "draws_per_chain": int(dr.shape[0]), "min_ess": float(e.min()),
-                    "mean_depth": float(inf[:, 5].mean()), "min_ess_per_s": float(e.min() / (ms / 1e3))})
-    worst = min(per, key=lambda q: q["min_ess_per_s"])
+        datas.append((d, eps, init))
+        flops_round_i.append(12.0 * Ni * Di * chains)
     peak, kind = measured_tensor_peak(sustained=True)
-    ach = flops_round * rounds / (ms / 1e3) / 1e12
-    return {"metric": "min-ESS/sec per instance, min over 64 instances (batched NUTS, HLR)",
-            "value": worst["min_ess_per_s"], "unit": "min-ESS/s", "rounds": rounds, "seconds": ms / 1e3,
-            "worst_instance": worst, "median_instance_min_ess_per_s": float(np.median([q["min_ess_per_s"] for q in per])),
+    results = {}
+    for variant in variants:
+        insts = [H.BatchedNuts(d, chains, eps=eps, max_depth=NUTS_DEPTH, seed=7 + i, init=init, hist_cap=hist_cap,
+                               variant=variant) for i, (d, eps, init) in enumerate(datas)]
+        pool = H.NutsPool(insts, streams=streams)
+        # warm-up (untimed, draws discarded): the chains leave their common start
+        pool.run(warmup_draws, max_rounds, share=share)
+        pool.reset()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        rounds = pool.run(min_draws, max_rounds, share=share)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        per = []
+        for i, nuts in enumerate(insts):
+            dr = nuts.draws()
+            inf = nuts.info()
+            e = ess(dr) if dr.shape[0] >= 4 else np.zeros(nuts.D)
+            per.append({"N": nuts.data.N, "D": nuts.D, "rounds": rounds[i], "draws_per_chain": int(dr.shape[0]),
+                        "min_ess": float(e.min()), "mean_depth": float(inf[:, 5].mean()),
+                        "min_ess_per_s": float(e.min() / (ms / 1e3))})
+        worst = min(per, key=lambda q: q["min_ess_per_s"])
+        ach = sum(f * r for f, r in zip(flops_round_i, rounds)) / (ms / 1e3) / 1e12
+        results[variant] = {
+            "value": worst["min_ess_per_s"], "unit": "min-ESS/s", "rounds_total": int(sum(rounds)),
+            "seconds": ms / 1e3, "worst_instance": worst,
+            "median_instance_min_ess_per_s": float(np.median([q["min_ess_per_s"] for q in per])),
             "total_draws": int(sum(q["draws_per_chain"] for q in per) * chains),
             "roofline": {"bound": "tensor", "kernel": "gemm_kernel (batched passes, all instances)", "achieved": ach,
                          "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "peak_source": kind + " (sustained)"},
-            "instances": per,
-            "config": {"workload": "hlr_nuts_64_instances_c512", "instances": n_inst, "chains": chains,
-                       "max_depth": NUTS_DEPTH, "x_dtype": "bf16", "N": "log-uniform [1e3, 1e6]",
-                       "D": "{16, 64, 256}", "prior": "normal(0, sigma^2), sigma^2 at its generating value",
-                       "step_size": "0.6 / sqrt(N E[w] + 1/sigma^2) at the generating coefficients",
-                       "streams": streams}}
+            "instances": per}
+        del pool, insts
+        torch.cuda.empty_cache()
+    head = dict(results[variants[0]])
+    head.update({"metric": "min-ESS/sec per instance, min over 64 instances (batched NUTS, HLR)",
+                 "selection_rule": variants[0], "min_draws_per_chain": min_draws,
+                 "warmup_draws_per_chain": warmup_draws,
+                 "other_rules": {v: {k: results[v][k] for k in ("value", "seconds", "median_instance_min_ess_per_s",
+                                                                "worst_instance", "rounds_total")}
+                                 for v in variants[1:]},
+                 "config": {"workload": "hlr_nuts_64_instances_c512", "instances": n_inst, "chains": chains,
+                            "max_depth": NUTS_DEPTH, "x_dtype": "bf16", "N": "log-uniform [1e3, 1e6]",
+                            "D": "{16, 64, 256}", "prior": "normal(0, sigma^2), sigma^2 at its generating value",
+                            "step_size": "0.6 / sqrt(N E[w] + 1/sigma^2) at the generating coefficients",
+                            "streams": streams,
+                            "schedule": "NutsPool (%s shares): rounds until %d draws per chain, LPT streams"
+                                        % (share, min_draws)}})
+    return head
 
 
 # ---- config 3: Gaussian mixture Gibbs ----------------------------------------
@@ -437,6 +469,7 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
 
     X, y, beta = H.synthetic(HLR_N, HLR_D, seed=HLR_SEED)
     d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    tuned = d.autotune(HLR_C, tuner=bench_tuner())
     rs = np.random.default_rng(HLR_SEED)
     init = np.asarray(beta, np.float32)[None] + 1e-3 * rs.standard_normal((HLR_C, HLR_D)).astype(np.float32)
 
@@ -522,6 +555,7 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
         "config": {"workload": "hlr_surrogate_n2000000_d512_c256", "N": HLR_N, "D": HLR_D, "chains": HLR_C,
                    "x_dtype": "bf16", "prior": "student_t(3)", "mlp": "512-256-256-512 gelu, bf16 weights",
                    "init": "generating coefficients + N(0, 1e-6), then the plain sampler's warm-up",
+                   "launch_shape": tuned,
                    "warmup": warm, "surrogate_warmup": sur_warm,
                    "train_every": train_every, "train_steps": train_steps},
     }
@@ -597,7 +631,9 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clocks.summary(),
             "roofline": {"bound": "hbm", "kernel": "lda_z_kernel", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind, "traffic": Z_KERNEL_DRAM_BYTES,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
+                                           "(profiles/lda_zq_kernel_k50_v10000_d2000.md)",
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": z_ms,
                          "note": "algorithmic bytes per token = 4 w + 4 z + 8 count RMW + 8K phi row"},
             "sweep_roofline_frac": (T * 442.0) / (ms_max / args.steps / 1e3) / 1e9 / hbm,
@@ -613,7 +649,8 @@ def run_ours(args, rank, world, local_rank):
                                                                          train_steps=args.train_steps)),
                             ("hlr_small", lambda: run_hlr_small(cpu=not args.no_cpu_baseline)),
                             ("gmm", lambda: run_gmm(cpu=not args.no_cpu_baseline)),
-                            ("hlr_nuts", lambda: run_hlr_nuts(rounds=400))):
+                            ("hlr_nuts", lambda: run_hlr_nuts(min_draws=args.nuts_draws,
+                                                              max_rounds=args.nuts_rounds))):
                 try:
                     line[key] = fn()
                 except Exception as e:
@@ -747,7 +784,8 @@ def main():
     ap.add_argument("--no-secondary", action="store_true", help="skip the surrogate HLR measurement")
     ap.add_argument("--workload", default="lda",
                     choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm", "hlr_nuts"])
-    ap.add_argument("--nuts-rounds", type=int, default=600)
+    ap.add_argument("--nuts-rounds", type=int, default=2400, help="batched NUTS: round cap per instance")
+    ap.add_argument("--nuts-draws", type=int, default=48, help="batched NUTS: draws per chain per instance")
     ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
     ap.add_argument("--hlr-iters", type=int, default=100)
     ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
@@ -767,7 +805,7 @@ def main():
     elif args.workload == "hlr_nuts":
         import torch
         torch.cuda.set_device(local_rank)
-        line = run_hlr_nuts(rounds=args.nuts_rounds) if rank == 0 else None
+        line = run_hlr_nuts(min_draws=args.nuts_draws, max_rounds=args.nuts_rounds) if rank == 0 else None
     elif args.workload == "hlr_pass":
         import torch
         torch.cuda.set_device(local_rank)

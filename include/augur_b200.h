@@ -281,6 +281,23 @@ size_t ab_hlrb_workspace_bytes(int N, int D, int C);
 int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad,
                       int ldg, void* work, int* err, void* stream);
 
+/* Launch shape of the batched pass, the knobs of the autotuner
+ * (augurv2_b200/autotune.py); no reference counterpart (the reference's
+ * gradient is a thrust reduction with no tiling, compiler/augur/src/Low/
+ * SplitBlk.hs:382-389).  A zero field takes the built-in choice:
+ *   fwd_warps   epilogue warps of the forward GEMM: 4 or 8 (default 8)
+ *   bwd_bn      gradient columns per backward tile: 32, 64 or 128 (default
+ *               the narrowest that covers D)
+ *   bwd_splits  row splits of the backward GEMM, >= 1 (default SMs / tiles)
+ * Results of different shapes agree to FP32 rounding (the backward partial
+ * sums are grouped differently); each shape is deterministic. */
+typedef struct ab_hlrb_config {
+  int fwd_warps, bwd_bn, bwd_splits;
+} ab_hlrb_config;
+size_t ab_hlrb_workspace_bytes_cfg(int N, int D, int C, const ab_hlrb_config* cfg);
+int ab_hlrb_logp_grad_cfg(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad,
+                          int ldg, const ab_hlrb_config* cfg, void* work, int* err, void* stream);
+
 /* ======================================================================= *
  * Batched HMC driver (h_augur_mcmc_hmc / h_augur_mcmc_leapfrog,
  * cbits/augur_mcmclib.h:343-424, for C chains at once).  All pointers are
@@ -327,7 +344,25 @@ int ab_nutsb_init(void* state, int C, int P, int hist_cap, const float* theta, c
 int ab_nutsb_thprop(void* state, int C, int P, int hist_cap, float** thprop, float** hist, int** hist_depth);
 int ab_nutsb_advance(void* state, int C, int P, int hist_cap, int max_depth, double eps, uint64_t seed, uint32_t comp,
                      const double* logp_new, const float* g_new, void* stream);
+/* The same with a choice of selection rule.  AB_NUTS_REFERENCE is the
+ * reference's (what ab_nutsb_advance runs): an iteration's draw is the pick
+ * of its last doubling only (f_cpy reset per doubling,
+ * cbits/augur_mcmclib.h:744-774) and the doubling's acceptance bias is
+ * augur_min on the truncated ratio n'/n, so a chain moves only when the
+ * final doubling is accepted whole.  AB_NUTS_STANDARD is Hoffman & Gelman's
+ * efficient NUTS (2014, Algorithm 3): the latest accepted pick of any
+ * doubling is the draw, accepted with probability min(1, n'/n).  Same tree
+ * walk, leaves and random streams; no reference counterpart for the
+ * standard rule. */
+enum { AB_NUTS_REFERENCE = 0, AB_NUTS_STANDARD = 1 };
+int ab_nutsb_advance_variant(void* state, int C, int P, int hist_cap, int max_depth, double eps, uint64_t seed,
+                             uint32_t comp, int variant, const double* logp_new, const float* g_new, void* stream);
 int ab_nutsb_info(void* state, int C, int P, int hist_cap, double* info, void* stream);
+/* End of warm-up: the recorded draws are forgotten (draw counts and depth
+ * statistics restart at zero) while every chain keeps its state; the
+ * reference keeps no draw history of its own (pyaugur's samplen collects
+ * draws on the host, pyaugur/augurlib.py:195-222). */
+int ab_nutsb_reset_history(void* state, int C, int P, int hist_cap, void* stream);
 
 /* ======================================================================= *
  * Gradient-surrogate MLP (no counterpart in the reference): d_in -> h1 ->

@@ -157,3 +157,106 @@ def test_batched_nuts_matches_fp64_oracle_nuts():
                                           comp=0, max_depth=depth)
             assert dep == depths[c, it], (c, it, dep, depths[c, it])
             np.testing.assert_allclose(got[it, c], par[:D], rtol=2e-4, atol=2e-5)
+
+
+@pytest.mark.parametrize("N,D,C", [(3000, 64, 40), (20000, 16, 130), (2500, 200, 256)])
+def test_every_launch_shape_matches_fp64(N, D, C, tmp_path):
+    """Every launch shape the autotuner may pick computes the same log
+    density and gradient (within the FP64-oracle tolerance), and the tuner's
+    pick is one of them and is reused from its cache."""
+    from augurv2_b200 import autotune as T
+    d, X64, y = _data(N, D, seed=N + D, prior="student_t")
+    th = np.random.default_rng(C).standard_normal((C, D)) * 0.3
+    cands = T.hlrb_candidates(N, D, C, torch.cuda.get_device_properties(0).multi_processor_count)
+    for cand in cands:
+        d.config = T.HlrbConfigC.of(cand)
+        _check(d, X64, y, th)
+    tuner = T.Autotuner(cache_path=str(tmp_path / "tune.json"), reps=2, warmup=1)
+    d.config = None
+    best = d.autotune(C, tuner=tuner)
+    assert best in cands and tuner.timed == len(cands)
+    _check(d, X64, y, th)
+    again = T.Autotuner(cache_path=str(tmp_path / "tune.json"))
+    d.config = None
+    assert d.autotune(C, tuner=again) == best and again.timed == 0
+
+
+def test_workspace_too_small_for_shape_is_refused():
+    from augurv2_b200 import _native as Nn
+    from augurv2_b200 import autotune as T
+    d, X64, y = _data(50000, 16, seed=3)
+    th = torch.zeros((8, 16), device="cuda")
+    small = d.workspace(8, T.HlrbConfigC.of({"bwd_splits": 1}))
+    with pytest.raises(Nn.AugurError):
+        d.logp_grad(th, work=small, config=T.HlrbConfigC.of({"bwd_splits": 300}))
+
+
+def test_nuts_pool_runs_until_every_instance_has_its_draws():
+    insts = []
+    for i, (N_, D, eps) in enumerate([(300, 8, 0.08), (2000, 16, 0.03), (800, 64, 0.03)]):
+        d, X64, y = _data(N_, D, seed=40 + i, prior="normal")
+        init = (np.random.default_rng(i).standard_normal((6, D)) * 0.1).astype(np.float32)
+        insts.append(H.BatchedNuts(d, 6, eps=eps, max_depth=5, seed=3 + i, init=init, hist_cap=16))
+    # the same sampler run alone, for comparison of the draws
+    d0, _, _ = _data(300, 8, seed=40, prior="normal")
+    solo = H.BatchedNuts(d0, 6, eps=0.08, max_depth=5, seed=3,
+                         init=(np.random.default_rng(0).standard_normal((6, 8)) * 0.1).astype(np.float32), hist_cap=16)
+    pool = H.NutsPool(insts, streams=2)
+    ran = pool.run(min_draws=5, max_rounds=500, block=10)
+    for s, r in zip(insts, ran):
+        assert 0 < r <= 500
+        assert s.info()[:, 0].min() >= 5
+    # a pool changes only the scheduling: instance 0's draws equal a solo run's
+    solo.capture()
+    solo.run(pool.rounds[0] - 1)
+    n = min(solo.draws().shape[0], insts[0].draws().shape[0])
+    np.testing.assert_array_equal(solo.draws()[:n], insts[0].draws()[:n])
+    pool.reset()
+    assert all(s.info()[:, 0].max() == 0 for s in insts)
+    ran2 = pool.run(min_draws=3, max_rounds=500, block=10)
+    assert all(s.info()[:, 0].min() >= 3 for s in insts) and all(r > 0 for r in ran2)
+
+
+def _posterior_summary(draws):
+    """draws [n, C, D] -> (mean [D], sd [D], ESS [D])"""
+    from augurv2_b200.diagnostics import ess
+    x = np.asarray(draws, np.float64)
+    flat = x.reshape(-1, x.shape[-1])
+    return flat.mean(0), flat.std(0), ess(x)
+
+
+def test_nuts_posterior_moments_match_exact_hmc():
+    """ESS-scaled z-tests of posterior means (and a check of the sds): the
+    batched NUTS, under both selection rules, against plain exact-gradient
+    HMC (whose transitions equal the FP64 oracle's) on the same HLR
+    posterior; both rules mix well here (ESS at least 0.2 per draw)."""
+    N_, D, v = 400, 8, 2.0
+    d, X64, y = _data(N_, D, seed=77, prior="normal")
+    d = H.HlrbData(torch.as_tensor(X64, dtype=torch.float32).to(torch.bfloat16), y, prior="normal", var=v)
+    rs = np.random.default_rng(5)
+    C_ = 256
+    init = (rs.standard_normal((C_, D)) * 0.5).astype(np.float32)
+    w = 0.2
+    eps = 0.6 / np.sqrt(N_ * w + 1.0 / v)
+    out = {}
+    for variant in ("standard", "reference"):
+        nuts = H.BatchedNuts(d, C_, eps=eps, max_depth=8, seed=21, init=init, hist_cap=160, variant=variant)
+        nuts.capture()
+        pool = H.NutsPool([nuts], streams=1)
+        pool.run(min_draws=40, max_rounds=20000)          # warm-up
+        pool.reset()
+        pool.run(min_draws=150, max_rounds=40000)
+        out[variant] = _posterior_summary(nuts.draws()[:150])
+    hmc = H.BatchedHmc(d, C_, L=10, eps=eps, jitter=0.1, seed=8, init=init)
+    hmc.capture()
+    hmc.run(100)
+    rec = []
+    for _ in range(300):
+        hmc.run(1)
+        rec.append(hmc.theta.detach().cpu().numpy().copy())
+    m_h, s_h, e_h = _posterior_summary(np.stack(rec))
+    for variant, (m_n, s_n, e_n) in out.items():
+        z = (m_n - m_h) / np.sqrt(s_h ** 2 / e_h + s_n ** 2 / e_n)
+        assert np.all(np.abs(z) < 4.5), (variant, z)
+        np.testing.assert_allclose(s_n, s_h, rtol=0.15, err_msg=variant)
+        assert e_n.min() > 0.2 * 150 * C_, (variant, e_n.min())
