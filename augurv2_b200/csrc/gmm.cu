@@ -194,7 +194,7 @@ gmm_prep_kernel(int d, const double* __restrict__ cov, double* __restrict__ Linv
 // discrete draw of augur_dist.c:798-813 with the uniform of substream
 // (n, iter, 1|comp<<8).
 template <int DT, bool UNROLL>
-__global__ void __launch_bounds__(GMM_THREADS)
+__global__ void __launch_bounds__(GMM_THREADS, 3)   // 3 CTAs per SM: measured 6 % faster than 1 at d = 32
 gmm_z_kernel(int N, int d, int K, int shared_cov, const float* __restrict__ Y, const double* __restrict__ pis,
              const double* __restrict__ mu, const double* __restrict__ Linv, const double* __restrict__ hdet,
              int* __restrict__ z, uint64_t seed, uint32_t iter, uint32_t comp) {
@@ -246,27 +246,75 @@ gmm_z_kernel(int N, int d, int K, int shared_cov, const float* __restrict__ Y, c
 }
 
 // ---- conjugate statistics ----------------------------------------------------
-// CTA b accumulates points [b*chunk, (b+1)*chunk) in point order into shared
-// memory: counts, sum of y (want_sum) and the lower triangle of
-// sum (y - mu_z)(y - mu_z)^T (want_obs; the reference's full-matrix update
-// augur_mat_atm_inc_vtmt is symmetric elementwise).  Each thread owns fixed
-// table entries, so no two threads touch one entry.  Partials go to
-// scratch and gmm_stats_reduce_kernel adds them in CTA order (deterministic;
-// the reference adds in point order).
+// CTA b accumulates points [b*chunk, (b+1)*chunk): counts, sum of y
+// (want_sum) and the lower triangle of sum (y - mu_z)(y - mu_z)^T
+// (want_obs; the reference's full-matrix update augur_mat_atm_inc_vtmt is
+// symmetric elementwise).  The CTA first sorts its chunk by component with
+// a stable counting sort in shared memory (warp 0, match_any ranks), then
+// walks the components one at a time: each thread owns fixed table entries
+// and accumulates them in registers over the component's points in point
+// order, so every (component, entry) sum is the same sequence of additions
+// as a point-order pass, without a shared-memory read-modify-write per
+// point.  Partials go to scratch [CTA][K][W] and gmm_stats_reduce_kernel
+// adds them in CTA order (deterministic; the reference adds in point
+// order).
+constexpr int GMM_STAT_MAXE = 4;       // table entries per thread (W <= 4 * GMM_THREADS)
+
 __global__ void __launch_bounds__(GMM_THREADS)
 gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __restrict__ z,
                  const double* __restrict__ mu, int want_sum, int want_obs, int chunk,
                  double* __restrict__ part) {
-  extern __shared__ double acc[];   // [K][1 + d + d(d+1)/2]
+  extern __shared__ int sidx[];          // zs [chunk], perm [chunk]
+  __shared__ int koff[GMM_MAX_K + 1];
+  int* zs = sidx;
+  int* perm = sidx + chunk;
   const int T = d * (d + 1) / 2;
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
-  for (int e = threadIdx.x; e < K * W; e += blockDim.x) acc[e] = 0.0;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int n0 = blockIdx.x * chunk, n1 = min(N, n0 + chunk);
+  const int cnt_pts = max(0, n1 - n0);
+  for (int p = tid; p < cnt_pts; p += blockDim.x) {
+    const int k = z[n0 + p];
+    zs[p] = (k >= 0 && k < K) ? k : -1;      // a label outside [0, K) is not counted
+  }
+  __syncthreads();
+  if (tid < 32) {
+    // stable counting sort of the chunk by component
+    for (int k = lane; k <= K; k += 32) koff[k] = 0;
+    __syncwarp();
+    for (int p = lane; p < cnt_pts; p += 32)
+      if (zs[p] >= 0) atomicAdd(&koff[zs[p] + 1], 1);
+    __syncwarp();
+    if (lane == 0)
+      for (int k = 0; k < K; ++k) koff[k + 1] += koff[k];
+    __syncwarp();
+    // koff[k] now the start of component k; a running cursor per component
+    // lives in the upper half of the prefix (restored below)
+    for (int p0 = 0; p0 < cnt_pts; p0 += 32) {
+      const int p = p0 + lane;
+      const int k = p < cnt_pts ? zs[p] : -1;
+      const bool act = k >= 0;
+      const unsigned mask = __ballot_sync(0xffffffffu, act);
+      if (act) {
+        const unsigned peers = __match_any_sync(mask, k);
+        const int rank = __popc(peers & ((1u << lane) - 1u));
+        perm[koff[k] + rank] = p;
+        __syncwarp(mask);
+        if (lane == __ffs(peers) - 1) koff[k] += __popc(peers);
+      }
+      __syncwarp();
+    }
+    // undo the cursor advance: koff[k] is now the end of component k
+    if (lane == 0) {
+      for (int k = K; k > 0; --k) koff[k] = koff[k - 1];
+      koff[0] = 0;
+    }
+  }
   __syncthreads();
   // entries owned by this thread: kind 0 count, 1 sum of y_i, 2 scatter (i, j)
-  constexpr int MAXE = 4;
-  int ekind[MAXE], ei[MAXE], ej[MAXE];
+  int ekind[GMM_STAT_MAXE], ei[GMM_STAT_MAXE], ej[GMM_STAT_MAXE];
   int ne = 0;
-  for (int e = threadIdx.x; e < W && ne < MAXE; e += blockDim.x, ++ne) {
+  for (int e = tid; e < W && ne < GMM_STAT_MAXE; e += blockDim.x, ++ne) {
     if (e == 0) { ekind[ne] = 0; ei[ne] = 0; ej[ne] = 0; }
     else if (want_sum && e <= d) { ekind[ne] = 1; ei[ne] = e - 1; ej[ne] = 0; }
     else {
@@ -276,26 +324,35 @@ gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __
       ekind[ne] = 2; ei[ne] = i; ej[ne] = t;
     }
   }
-  const int n0 = blockIdx.x * chunk, n1 = min(N, n0 + chunk);
-  for (int n = n0; n < n1; ++n) {
-    const int k = z[n];
-    double* row = acc + (size_t)k * W;
-    const float* y = Y + (size_t)n * d;
-    for (int q = 0; q < ne; ++q) {
-      const int e = threadIdx.x + q * blockDim.x;
-      if (ekind[q] == 0) {
-        row[e] = __dadd_rn(row[e], 1.0);
-      } else if (ekind[q] == 1) {
-        row[e] = __dadd_rn(row[e], (double)y[ei[q]]);
-      } else {
-        const double di = __dadd_rn((double)y[ei[q]], -mu[(size_t)k * d + ei[q]]);
-        const double dj = __dadd_rn((double)y[ej[q]], -mu[(size_t)k * d + ej[q]]);
-        row[e] = __dadd_rn(row[e], __dmul_rn(di, dj));
+  for (int k = 0; k < K; ++k) {
+    double acc[GMM_STAT_MAXE], mi[GMM_STAT_MAXE], mj[GMM_STAT_MAXE];
+#pragma unroll
+    for (int q = 0; q < GMM_STAT_MAXE; ++q) {
+      acc[q] = 0.0;
+      mi[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ei[q]] : 0.0;
+      mj[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ej[q]] : 0.0;
+    }
+    for (int p = koff[k]; p < koff[k + 1]; ++p) {
+      const float* y = Y + (size_t)(n0 + perm[p]) * d;
+#pragma unroll
+      for (int q = 0; q < GMM_STAT_MAXE; ++q) {
+        if (q < ne) {
+          if (ekind[q] == 0) {
+            acc[q] = __dadd_rn(acc[q], 1.0);
+          } else if (ekind[q] == 1) {
+            acc[q] = __dadd_rn(acc[q], (double)__ldg(y + ei[q]));
+          } else {
+            const double di = __dadd_rn((double)__ldg(y + ei[q]), -mi[q]);
+            const double dj = __dadd_rn((double)__ldg(y + ej[q]), -mj[q]);
+            acc[q] = __dadd_rn(acc[q], __dmul_rn(di, dj));
+          }
+        }
       }
     }
+#pragma unroll
+    for (int q = 0; q < GMM_STAT_MAXE; ++q)
+      if (q < ne) part[((size_t)blockIdx.x * K + k) * W + tid + q * blockDim.x] = acc[q];
   }
-  __syncthreads();
-  for (int e = threadIdx.x; e < K * W; e += blockDim.x) part[(size_t)blockIdx.x * K * W + e] = acc[e];
 }
 
 __global__ void gmm_stats_reduce_kernel(int d, int K, int want_sum, int want_obs, int nparts,
@@ -384,21 +441,48 @@ gmm_conj_mu_kernel(int d, int shared_cov, const double* __restrict__ mu0, const 
   for (int i = lane; i < d; i += 32) mu[(size_t)k * d + i] = res[i];
 }
 
+// Bartlett diagonal for the inverse-Wishart draw (bartlett_decomp,
+// augur_dist.c:722-738): the chi-square of n - i degrees of freedom in row i
+// is the sum of squares of the n - i normals at stream positions
+// i*n + i + t, t < n - i (n = cnt[k] + df), substream (k, iter, 9|comp<<8).
+// One CTA per (k, i): thread-strided partial sums, then the fixed-order
+// block sum.  That is O(d * cnt[k]) normals per component per sweep (the
+// reference's algorithm), spread over K * d CTAs.  The sums are staged on
+// the diagonal of cov[k], which gmm_conj_cov_kernel then reads and
+// overwrites with the draw.
+__global__ void __launch_bounds__(GMM_THREADS)
+gmm_bartlett_chi_kernel(int d, int df, const int* __restrict__ cnt, double* __restrict__ cov, uint64_t seed,
+                        uint32_t iter, uint32_t comp) {
+  __shared__ double red[34];
+  const int k = blockIdx.x / d, i = blockIdx.x - k * d;
+  const int n = cnt[k] + df;
+  const Stream s0 = make_stream(seed, (uint32_t)k, iter, TAG_COV | (comp << 8));
+  double local = 0.0;
+  for (int t = threadIdx.x; t < n - i; t += blockDim.x) {
+    Stream s = s0;
+    s.pos = (uint32_t)(i * n + i + t);
+    const double zz = s.normal();
+    local = __dadd_rn(local, __dmul_rn(zz, zz));
+  }
+  const double chi = block_sum_f64(local, red);
+  if (threadIdx.x == 0) cov[(size_t)k * d * d + (size_t)i * d + i] = chi;
+}
+
 // augur_invwishart_mvnormal_conj (augur_dist.c:751-757) and
 // augur_invwishart_sample (:740-749) with bartlett_decomp (:722-738) for
 // component k, one thread block, substream (k, iter, 9|comp<<8).  The
 // Bartlett normals are drawn at the stream positions the reference's loop
 // consumes them (row-major over the lower triangle; each diagonal
 // chi-square of n - i normals follows its row's off-diagonal normals).  The
-// chi-square sums of up to cnt + df squares are added by the whole block in
-// a fixed tree order instead of sequentially (a rounding-level difference);
-// the d x d algebra runs on warp 0.
+// chi-square sums of up to cnt + df squares come from
+// gmm_bartlett_chi_kernel (on cov's diagonal), added in a fixed tree order
+// instead of sequentially (a rounding-level difference); the d x d algebra
+// runs on warp 0.
 __global__ void __launch_bounds__(GMM_THREADS)
 gmm_conj_cov_kernel(int d, int df, const double* __restrict__ scale0, const int* __restrict__ cnt,
                     const double* __restrict__ obs, double* __restrict__ cov, uint64_t seed, uint32_t iter,
                     uint32_t comp) {
   extern __shared__ double sm[];
-  __shared__ double red[34];
   const int k = blockIdx.x, tid = threadIdx.x;
   const int dd = d * d;
   double* S = sm;          // obs + scale0
@@ -417,8 +501,7 @@ gmm_conj_cov_kernel(int d, int df, const double* __restrict__ scale0, const int*
     w_chol(L, d);
   }
   // Bartlett factor: element (i, j < i) is the normal at position i*n + j;
-  // the diagonal (i, i) is sqrt of the sum of squares of the n - i normals
-  // starting at position i*n + i.
+  // the diagonal (i, i) is the square root of the row's chi-square sum.
   const Stream s0 = make_stream(seed, (uint32_t)k, iter, TAG_COV | (comp << 8));
   for (int e = tid; e < dd; e += blockDim.x) {
     const int i = e / d, j = e - i * d;
@@ -428,18 +511,9 @@ gmm_conj_cov_kernel(int d, int df, const double* __restrict__ scale0, const int*
       A[e] = s.normal();
     } else if (j > i) {
       A[e] = 0.0;
+    } else {
+      A[e] = __dsqrt_rn(cov[(size_t)k * dd + e]);
     }
-  }
-  for (int i = 0; i < d; ++i) {
-    double local = 0.0;
-    for (int t = tid; t < n - i; t += blockDim.x) {
-      Stream s = s0;
-      s.pos = (uint32_t)(i * n + i + t);
-      const double zz = s.normal();
-      local = __dadd_rn(local, __dmul_rn(zz, zz));
-    }
-    const double chi = block_sum_f64(local, red);
-    if (tid == 0) A[i * d + i] = __dsqrt_rn(chi);
   }
   __syncthreads();
   if (tid < 32) {
@@ -631,11 +705,11 @@ int launch_gmm_stats(int N, int d, int K, const float* Y, const int* z, const do
                      int want_obs, int* cnt, double* sum, double* obs, double* part, cudaStream_t st) {
   const int T = d * (d + 1) / 2;
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
-  const size_t smem = sizeof(double) * (size_t)K * W;
-  AB_REQUIRE(smem <= 200 * 1024, AB_ERR_ARG, "gmm: K * d^2 too large for the statistics pass");
-  AB_REQUIRE(W <= 4 * GMM_THREADS, AB_ERR_ARG, "gmm: d too large for the statistics pass");
+  AB_REQUIRE(W <= GMM_STAT_MAXE * GMM_THREADS, AB_ERR_ARG, "gmm: d too large for the statistics pass");
   const int chunk = (N + GMM_STAT_CTAS - 1) / GMM_STAT_CTAS;
   const int nparts = (N + chunk - 1) / chunk;
+  const size_t smem = sizeof(int) * 2 * (size_t)chunk;
+  AB_REQUIRE(smem <= 200 * 1024, AB_ERR_ARG, "gmm: N too large for the statistics pass (chunk of %d points)", chunk);
   AB_CUDA(cudaFuncSetAttribute(gmm_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gmm_stats_kernel<<<nparts, GMM_THREADS, smem, st>>>(N, d, K, Y, z, mu, want_sum, want_obs, chunk, part);
   AB_LAUNCH_CHECK("gmm_stats_kernel");
@@ -657,6 +731,8 @@ int launch_gmm_conj_mu(int K, int d, int shared, const double* mu0, const double
 
 int launch_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
                         double* cov, uint64_t seed, uint32_t iter, uint32_t comp, cudaStream_t st) {
+  gmm_bartlett_chi_kernel<<<K * d, GMM_THREADS, 0, st>>>(d, df, cnt, cov, seed, iter, comp);
+  AB_LAUNCH_CHECK("gmm_bartlett_chi_kernel");
   const size_t smem = sizeof(double) * 4 * (size_t)d * d;
   AB_CUDA(cudaFuncSetAttribute(gmm_conj_cov_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gmm_conj_cov_kernel<<<K, GMM_THREADS, smem, st>>>(d, df, scale0, cnt, obs, cov, seed, iter, comp);

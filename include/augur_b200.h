@@ -227,7 +227,9 @@ int ab_gmm_conj_mu(int K, int d, int shared_cov, const double* mu0, const double
                    void* stream);
 
 /* ConjGibbs [cov]: augur_invwishart_mvnormal_conj (cbits/augur_dist.c:751-757,
- * InvWishart(cnt + df, obs + scale0) by Bartlett); (k, iter, 9|comp<<8). */
+ * InvWishart(cnt + df, obs + scale0) by Bartlett); (k, iter, 9|comp<<8).
+ * cov is output only: its diagonal holds the Bartlett chi-square sums
+ * between the two kernels of the call. */
 int ab_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs, double* cov,
                     uint64_t seed, uint32_t iter, uint32_t comp, void* stream);
 
