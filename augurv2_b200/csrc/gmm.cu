@@ -249,68 +249,37 @@ gmm_z_kernel(int N, int d, int K, int shared_cov, const float* __restrict__ Y, c
 // CTA b accumulates points [b*chunk, (b+1)*chunk): counts, sum of y
 // (want_sum) and the lower triangle of sum (y - mu_z)(y - mu_z)^T
 // (want_obs; the reference's full-matrix update augur_mat_atm_inc_vtmt is
-// symmetric elementwise).  The CTA first sorts its chunk by component with
-// a stable counting sort in shared memory (warp 0, match_any ranks), then
-// walks the components one at a time: each thread owns fixed table entries
-// and accumulates them in registers over the component's points in point
-// order, so every (component, entry) sum is the same sequence of additions
-// as a point-order pass, without a shared-memory read-modify-write per
-// point.  Partials go to scratch [CTA][K][W] and gmm_stats_reduce_kernel
-// adds them in CTA order (deterministic; the reference adds in point
-// order).
+// symmetric elementwise).  The chunk is taken in sub-chunks of at most
+// `sub` points: a sub-chunk's rows of Y are copied to shared memory with
+// coalesced loads (all in flight at once), sorted by component with a
+// stable counting sort (warp 0, match_any ranks), and the components are
+// walked one at a time: each thread owns fixed table entries and
+// accumulates them in registers over the component's points in point order,
+// adding the sub-chunk's sum to its partial.  Partials go to scratch
+// [CTA][K][W] and gmm_stats_reduce_kernel adds them in CTA order
+// (deterministic; the reference adds in point order).
 constexpr int GMM_STAT_MAXE = 4;       // table entries per thread (W <= 4 * GMM_THREADS)
+constexpr int GMM_STAT_SMEM = 96 * 1024;
+
+__host__ __device__ inline int gmm_stat_sub(int d, int chunk) {
+  const int fit = GMM_STAT_SMEM / (4 * d + 8);
+  return chunk < fit ? chunk : fit;
+}
 
 __global__ void __launch_bounds__(GMM_THREADS)
 gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __restrict__ z,
                  const double* __restrict__ mu, int want_sum, int want_obs, int chunk,
                  double* __restrict__ part) {
-  extern __shared__ int sidx[];          // zs [chunk], perm [chunk]
+  extern __shared__ int sidx[];          // zs [sub], perm [sub], ys [sub][d] (float)
   __shared__ int koff[GMM_MAX_K + 1];
+  const int sub = gmm_stat_sub(d, chunk);
   int* zs = sidx;
-  int* perm = sidx + chunk;
+  int* perm = sidx + sub;
+  float* ys = reinterpret_cast<float*>(sidx + 2 * sub);
   const int T = d * (d + 1) / 2;
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
   const int tid = threadIdx.x, lane = tid & 31;
   const int n0 = blockIdx.x * chunk, n1 = min(N, n0 + chunk);
-  const int cnt_pts = max(0, n1 - n0);
-  for (int p = tid; p < cnt_pts; p += blockDim.x) {
-    const int k = z[n0 + p];
-    zs[p] = (k >= 0 && k < K) ? k : -1;      // a label outside [0, K) is not counted
-  }
-  __syncthreads();
-  if (tid < 32) {
-    // stable counting sort of the chunk by component
-    for (int k = lane; k <= K; k += 32) koff[k] = 0;
-    __syncwarp();
-    for (int p = lane; p < cnt_pts; p += 32)
-      if (zs[p] >= 0) atomicAdd(&koff[zs[p] + 1], 1);
-    __syncwarp();
-    if (lane == 0)
-      for (int k = 0; k < K; ++k) koff[k + 1] += koff[k];
-    __syncwarp();
-    // koff[k] now the start of component k; a running cursor per component
-    // lives in the upper half of the prefix (restored below)
-    for (int p0 = 0; p0 < cnt_pts; p0 += 32) {
-      const int p = p0 + lane;
-      const int k = p < cnt_pts ? zs[p] : -1;
-      const bool act = k >= 0;
-      const unsigned mask = __ballot_sync(0xffffffffu, act);
-      if (act) {
-        const unsigned peers = __match_any_sync(mask, k);
-        const int rank = __popc(peers & ((1u << lane) - 1u));
-        perm[koff[k] + rank] = p;
-        __syncwarp(mask);
-        if (lane == __ffs(peers) - 1) koff[k] += __popc(peers);
-      }
-      __syncwarp();
-    }
-    // undo the cursor advance: koff[k] is now the end of component k
-    if (lane == 0) {
-      for (int k = K; k > 0; --k) koff[k] = koff[k - 1];
-      koff[0] = 0;
-    }
-  }
-  __syncthreads();
   // entries owned by this thread: kind 0 count, 1 sum of y_i, 2 scatter (i, j)
   int ekind[GMM_STAT_MAXE], ei[GMM_STAT_MAXE], ej[GMM_STAT_MAXE];
   int ne = 0;
@@ -324,34 +293,79 @@ gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __
       ekind[ne] = 2; ei[ne] = i; ej[ne] = t;
     }
   }
-  for (int k = 0; k < K; ++k) {
-    double acc[GMM_STAT_MAXE], mi[GMM_STAT_MAXE], mj[GMM_STAT_MAXE];
-#pragma unroll
-    for (int q = 0; q < GMM_STAT_MAXE; ++q) {
-      acc[q] = 0.0;
-      mi[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ei[q]] : 0.0;
-      mj[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ej[q]] : 0.0;
+  for (int base = n0; base < n1 || base == n0; base += sub) {
+    const int m = max(0, min(sub, n1 - base));
+    for (int p = tid; p < m; p += blockDim.x) {
+      const int k = z[base + p];
+      zs[p] = (k >= 0 && k < K) ? k : -1;    // a label outside [0, K) is not counted
     }
-    for (int p = koff[k]; p < koff[k + 1]; ++p) {
-      const float* y = Y + (size_t)(n0 + perm[p]) * d;
+    for (int e = tid; e < m * d; e += blockDim.x) ys[e] = Y[(size_t)base * d + e];
+    __syncthreads();
+    if (tid < 32) {
+      // stable counting sort of the sub-chunk by component
+      for (int k = lane; k <= K; k += 32) koff[k] = 0;
+      __syncwarp();
+      for (int p = lane; p < m; p += 32)
+        if (zs[p] >= 0) atomicAdd(&koff[zs[p] + 1], 1);
+      __syncwarp();
+      if (lane == 0)
+        for (int k = 0; k < K; ++k) koff[k + 1] += koff[k];
+      __syncwarp();
+      for (int p0 = 0; p0 < m; p0 += 32) {       // koff[k] serves as component k's cursor
+        const int p = p0 + lane;
+        const int k = p < m ? zs[p] : -1;
+        const bool act = k >= 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, act);
+        if (act) {
+          const unsigned peers = __match_any_sync(mask, k);
+          const int rank = __popc(peers & ((1u << lane) - 1u));
+          perm[koff[k] + rank] = p;
+          __syncwarp(mask);
+          if (lane == __ffs(peers) - 1) koff[k] += __popc(peers);
+        }
+        __syncwarp();
+      }
+      if (lane == 0) {                           // cursors back to start offsets
+        for (int k = K; k > 0; --k) koff[k] = koff[k - 1];
+        koff[0] = 0;
+      }
+    }
+    __syncthreads();
+    for (int k = 0; k < K; ++k) {
+      double acc[GMM_STAT_MAXE], mi[GMM_STAT_MAXE], mj[GMM_STAT_MAXE];
 #pragma unroll
       for (int q = 0; q < GMM_STAT_MAXE; ++q) {
-        if (q < ne) {
-          if (ekind[q] == 0) {
-            acc[q] = __dadd_rn(acc[q], 1.0);
-          } else if (ekind[q] == 1) {
-            acc[q] = __dadd_rn(acc[q], (double)__ldg(y + ei[q]));
-          } else {
-            const double di = __dadd_rn((double)__ldg(y + ei[q]), -mi[q]);
-            const double dj = __dadd_rn((double)__ldg(y + ej[q]), -mj[q]);
-            acc[q] = __dadd_rn(acc[q], __dmul_rn(di, dj));
+        acc[q] = 0.0;
+        mi[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ei[q]] : 0.0;
+        mj[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ej[q]] : 0.0;
+      }
+      for (int p = koff[k]; p < koff[k + 1]; ++p) {
+        const float* y = ys + perm[p] * d;
+#pragma unroll
+        for (int q = 0; q < GMM_STAT_MAXE; ++q) {
+          if (q < ne) {
+            if (ekind[q] == 0) {
+              acc[q] = __dadd_rn(acc[q], 1.0);
+            } else if (ekind[q] == 1) {
+              acc[q] = __dadd_rn(acc[q], (double)y[ei[q]]);
+            } else {
+              const double di = __dadd_rn((double)y[ei[q]], -mi[q]);
+              const double dj = __dadd_rn((double)y[ej[q]], -mj[q]);
+              acc[q] = __dadd_rn(acc[q], __dmul_rn(di, dj));
+            }
           }
         }
       }
-    }
 #pragma unroll
-    for (int q = 0; q < GMM_STAT_MAXE; ++q)
-      if (q < ne) part[((size_t)blockIdx.x * K + k) * W + tid + q * blockDim.x] = acc[q];
+      for (int q = 0; q < GMM_STAT_MAXE; ++q) {
+        if (q < ne) {
+          double* dst = part + ((size_t)blockIdx.x * K + k) * W + tid + q * blockDim.x;
+          *dst = base == n0 ? acc[q] : __dadd_rn(*dst, acc[q]);
+        }
+      }
+    }
+    __syncthreads();                             // the next sub-chunk reuses shared memory
+    if (m == 0) break;
   }
 }
 
@@ -708,8 +722,8 @@ int launch_gmm_stats(int N, int d, int K, const float* Y, const int* z, const do
   AB_REQUIRE(W <= GMM_STAT_MAXE * GMM_THREADS, AB_ERR_ARG, "gmm: d too large for the statistics pass");
   const int chunk = (N + GMM_STAT_CTAS - 1) / GMM_STAT_CTAS;
   const int nparts = (N + chunk - 1) / chunk;
-  const size_t smem = sizeof(int) * 2 * (size_t)chunk;
-  AB_REQUIRE(smem <= 200 * 1024, AB_ERR_ARG, "gmm: N too large for the statistics pass (chunk of %d points)", chunk);
+  const int sub = gmm_stat_sub(d, chunk);
+  const size_t smem = (sizeof(int) * 2 + sizeof(float) * (size_t)d) * (size_t)sub;
   AB_CUDA(cudaFuncSetAttribute(gmm_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   gmm_stats_kernel<<<nparts, GMM_THREADS, smem, st>>>(N, d, K, Y, z, mu, want_sum, want_obs, chunk, part);
   AB_LAUNCH_CHECK("gmm_stats_kernel");

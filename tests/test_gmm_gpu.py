@@ -67,6 +67,41 @@ def test_stats_and_conj_draws(orc):
     np.testing.assert_allclose(g.cov.cpu().numpy(), O.gmm_conj_cov(orc, om, cnt, obs, 9, 2), rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("N_,K,d", [(300_000, 16, 32), (250_000, 3, 40), (1, 2, 3), (900, 16, 2)])
+def test_stats_sizes(orc, N_, K, d):
+    """Statistics at sizes where a CTA's chunk spans several shared-memory
+    sub-chunks (N = 3e5 at d = 32), the widest d of the pass, a single point,
+    and many components with few points each; a label outside [0, K) is not
+    counted."""
+    rng = np.random.default_rng(N_ + d)
+    Y = rng.standard_normal((N_, d)).astype(np.float32) * 3
+    z = rng.integers(0, K, size=N_).astype(np.int32)
+    mus = rng.standard_normal((K, d))
+    om = O.GmmModel(Y.astype(np.float64), K, np.zeros(d), 25 * np.eye(d), False, alpha=np.ones(K), df=d + 2,
+                    scale0=np.eye(d))
+    g = GmmGibbs(Y, K, np.zeros(d), 25 * np.eye(d), alpha=np.ones(K), df=d + 2, mu=mus, z=z, seed=1)
+    if N_ > 10:
+        g.z[N_ // 2] = K + 3                     # not a component: skipped
+    L = N.lib()
+    N.check(L.ab_gmm_stats(N_, d, K, N.ptr(g.Y), N.ptr(g.z), N.ptr(g.mu), N.ptr(g.cnt), N.ptr(g.sum), N.ptr(g.obs),
+                           N.ptr(g.scratch), N.stream_ptr()), "stats")
+    keep = np.ones(N_, bool)
+    if N_ > 10:
+        keep[N_ // 2] = False
+    cnt = np.bincount(z[keep], minlength=K)
+    s = np.zeros((K, d))
+    obs = np.zeros((K, d, d))
+    Y64 = Y.astype(np.float64)
+    for k in range(K):
+        m = keep & (z == k)
+        s[k] = Y64[m].sum(0)
+        c = Y64[m] - mus[k]
+        obs[k] = c.T @ c
+    np.testing.assert_array_equal(g.cnt.cpu().numpy(), cnt)
+    np.testing.assert_allclose(g.sum.cpu().numpy(), s, rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(g.obs.cpu().numpy(), obs, rtol=1e-12, atol=1e-8)
+
+
 def test_hmvgmm_sweeps_per_sweep_contract(orc):
     N_, K, d = 1500, 4, 5
     Y, z, mus, covs, pis, om = hmodel(N_, K, d, 11)
