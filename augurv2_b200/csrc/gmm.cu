@@ -376,8 +376,18 @@ __global__ void gmm_stats_reduce_kernel(int d, int K, int want_sum, int want_obs
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= K * W) return;
+  // CTA-order sum; eight partials are loaded ahead of their additions
   double a = 0.0;
-  for (int b = 0; b < nparts; ++b) a = __dadd_rn(a, part[(size_t)b * K * W + e]);
+  const size_t stride = (size_t)K * W;
+  int b = 0;
+  for (; b + 8 <= nparts; b += 8) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __ldg(part + (size_t)(b + q) * stride + e);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a = __dadd_rn(a, v[q]);
+  }
+  for (; b < nparts; ++b) a = __dadd_rn(a, __ldg(part + (size_t)b * stride + e));
   const int k = e / W, f = e - k * W;
   if (f == 0) {
     cnt[k] = (int)a;
