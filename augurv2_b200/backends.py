@@ -112,6 +112,9 @@ class HlrBackend:
             elif k.kind == "NUTS":
                 comps.append({"kind": "NUTS", "block": [role[v] for v in k.vars], "eps": k.params[0],
                               "max_depth": opt.max_depth})
+            elif k.kind == "RSlice":
+                comps.append({"kind": "RSlice", "block": [role[v] for v in k.vars], "simlen": k.params[0],
+                              "eps": k.params[1]})
             elif k.kind == "MWG":
                 p = k.proposal
                 v = k.vars[0]

@@ -34,7 +34,7 @@ constexpr int HLR_MAX_D = HLR_THREADS * HLR_MAX_COLS - 1;
 constexpr int HLR_STK = 16;              // NUTS stack entries (cbits/augur_blkstk.h:26)
 constexpr int HLR_MAX_COMPS = 8;
 
-enum { COMP_HMC = 0, COMP_NUTS = 1, COMP_MWG = 2 };
+enum { COMP_HMC = 0, COMP_NUTS = 1, COMP_MWG = 2, COMP_RSLICE = 3 };
 
 struct HlrModelDev {
   int N, D, ldx, has_b, vprior, compat, x_bf16;
@@ -81,6 +81,8 @@ struct Ws {
   double* aux2;    // [D+2]
   double* aux3;    // [D+2]
   double* aux4;    // [D+2]
+  double* pt_ll;   // [D+2]  per-coordinate prior terms (log density)
+  double* pt_dot;  // [D+2]  per-coordinate prior terms (d/dvar)
   double* gpart;   // [HLR_THREADS] per-thread partials (double)
   float* th;       // [D]    theta in FP32 for the data pass
   float* r;        // [HLR_CHUNK]
@@ -91,14 +93,18 @@ struct Ws {
 
 __device__ __forceinline__ double cta_sum(double v, double* red) { return block_sum_f64(v, red); }
 
-constexpr int SMALL_COLS = 32;   // small-D pass: D gradient columns, the bias column, the log-likelihood
+// Small-D pass widths: D gradient columns, the bias column, the
+// log-likelihood; 16 columns for D + 2 <= 16, else 32.
+constexpr int SMALL_COLS = 32;
 
-// Sum over the warp's lanes of each of 32 per-lane values, transposed: on
-// return v[0] of lane L holds the warp sum of column L (31 shuffles; fixed
-// butterfly order, so deterministic).
-__device__ __forceinline__ void warp_transpose_sum(double (&v)[SMALL_COLS], int lane) {
+// Sum over the warp's lanes of each of COLS per-lane values, transposed: on
+// return v[0] of lane L holds the warp sum of column L % COLS (fixed
+// butterfly order, so deterministic; COLS - 1 shuffles, plus one more round
+// folding the two half-warps when COLS = 16).
+template <int COLS>
+__device__ __forceinline__ void warp_transpose_sum(double (&v)[COLS], int lane) {
 #pragma unroll
-  for (int sft = 16; sft >= 1; sft >>= 1) {
+  for (int sft = COLS / 2; sft >= 1; sft >>= 1) {
     const bool up = (lane & sft) != 0;
 #pragma unroll
     for (int i = 0; i < sft; ++i) {
@@ -107,59 +113,61 @@ __device__ __forceinline__ void warp_transpose_sum(double (&v)[SMALL_COLS], int 
       v[i] = keep + __shfl_xor_sync(0xffffffffu, send, sft);
     }
   }
+  if (COLS == 16) v[0] += __shfl_xor_sync(0xffffffffu, v[0], 16);
 }
 
-// Data pass for D + 2 <= 32: one row per thread (t, the log-likelihood term
+// Data pass for D + 2 <= COLS: one row per thread (t, the log-likelihood term
 // and the residual's contributions to all D + 1 gradient columns in
 // registers, Kahan-compensated), then one transposed warp reduction and a
 // fixed-order sum over the warps, all in FP64.  The row-per-thread walk
 // keeps every thread busy at small N, where the segmented pass below is
 // bound by its per-row shuffle latency.
+template <int COLS>
 __device__ double data_pass_small(const HlrModelDev& m, const double* par, Ws& ws, bool want_grad) {
   const int D = m.D, N = m.N;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int k = tid; k < D; k += blockDim.x) ws.th[k] = (float)par[k];
   const float bias = m.has_b ? (float)par[D] : 0.0f;
   __syncthreads();
-  float th[SMALL_COLS - 2];
+  float th[COLS - 2];
 #pragma unroll
-  for (int k = 0; k < SMALL_COLS - 2; ++k) th[k] = k < D ? ws.th[k] : 0.0f;
-  float s[SMALL_COLS], c[SMALL_COLS];
+  for (int k = 0; k < COLS - 2; ++k) th[k] = k < D ? ws.th[k] : 0.0f;
+  float s[COLS], c[COLS];
 #pragma unroll
-  for (int j = 0; j < SMALL_COLS; ++j) { s[j] = 0.0f; c[j] = 0.0f; }
+  for (int j = 0; j < COLS; ++j) { s[j] = 0.0f; c[j] = 0.0f; }
   for (int n = tid; n < N; n += blockDim.x) {
     const size_t rb = (size_t)n * m.ldx;
-    float x[SMALL_COLS - 2];
+    float x[COLS - 2];
     float t = 0.0f;
 #pragma unroll
-    for (int k = 0; k < SMALL_COLS - 2; ++k) {
+    for (int k = 0; k < COLS - 2; ++k) {
       x[k] = k < D ? load_x(m, rb + k) : 0.0f;
       t += x[k] * th[k];
     }
     float llv, rv;
     bern_terms(m.y[n], t + bias, llv, rv);
-    kahan_add(s[SMALL_COLS - 1], c[SMALL_COLS - 1], llv);
+    kahan_add(s[COLS - 1], c[COLS - 1], llv);
     if (want_grad) {
 #pragma unroll
-      for (int k = 0; k < SMALL_COLS - 2; ++k)
+      for (int k = 0; k < COLS - 2; ++k)
         if (k < D) kahan_add(s[k], c[k], rv * x[k]);
 #pragma unroll
-      for (int k = 0; k < SMALL_COLS - 1; ++k)
+      for (int k = 0; k < COLS - 1; ++k)
         if (k == D) kahan_add(s[k], c[k], rv);
     }
   }
-  double v[SMALL_COLS];
+  double v[COLS];
 #pragma unroll
-  for (int j = 0; j < SMALL_COLS; ++j) v[j] = (double)s[j] - (double)c[j];
-  warp_transpose_sum(v, lane);
+  for (int j = 0; j < COLS; ++j) v[j] = (double)s[j] - (double)c[j];
+  warp_transpose_sum<COLS>(v, lane);
   __syncthreads();
-  ws.gpart[warp * 32 + lane] = v[0];
+  if (lane < COLS) ws.gpart[warp * COLS + lane] = v[0];
   __syncthreads();
-  if (tid < 32) {
+  if (tid < COLS) {
     double acc = 0.0;
     const int nw = blockDim.x >> 5;
-    for (int w = 0; w < nw; ++w) acc += ws.gpart[w * 32 + tid];
-    if (tid == SMALL_COLS - 1) ws.red[33] = acc;
+    for (int w = 0; w < nw; ++w) acc += ws.gpart[w * COLS + tid];
+    if (tid == COLS - 1) ws.red[33] = acc;
     else if (want_grad && tid <= D) ws.g[tid] = acc;
   }
   __syncthreads();
@@ -171,7 +179,8 @@ __device__ double data_pass_small(const HlrModelDev& m, const double* par, Ws& w
 // bias) — the full data gradient.
 __device__ double data_pass(const HlrModelDev& m, const double* par, Ws& ws, bool want_grad) {
   const int D = m.D, N = m.N;
-  if (D + 2 <= SMALL_COLS) return data_pass_small(m, par, ws, want_grad);
+  if (D + 2 <= 16) return data_pass_small<16>(m, par, ws, want_grad);
+  if (D + 2 <= SMALL_COLS) return data_pass_small<SMALL_COLS>(m, par, ws, want_grad);
   const int tid = threadIdx.x;
   for (int k = tid; k < D; k += blockDim.x) ws.th[k] = (float)par[k];
   const float bias = m.has_b ? (float)par[D] : 0.0f;
@@ -298,8 +307,15 @@ __device__ double block_ll_grad(const HlrModelDev& m, const double* par, const i
   double data_ll = 0.0;
   if (bi.th || bi.b) data_ll = data_pass(m, par, ws, want_grad);
   const double b = m.has_b ? par[D] : 0.0, v = par[D + 1];
-  // prior sums over theta (thread 0 walks k sequentially: D is small next
-  // to the data pass, and this keeps the reference's summation order)
+  // prior terms of the coefficients, one per thread; thread 0 then adds
+  // them in the reference's (sequential) order
+  if (bi.th || bi.v) {
+    for (int k = threadIdx.x; k < D; k += blockDim.x) {
+      ws.pt_ll[k] = normal_ll(m, par[k], 0.0, v);
+      if (bi.v) ws.pt_dot[k] = normal_dotarg2(m, par[k], 0.0, v);
+    }
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     double ll = 0.0, gv = 0.0;
     if (bi.v) { ll += vprior_ll(m, v); gv += vprior_dot(m, v); }
@@ -310,8 +326,8 @@ __device__ double block_ll_grad(const HlrModelDev& m, const double* par, const i
     if (bi.th || bi.v) {
       double s = 0.0;
       for (int k = 0; k < D; ++k) {
-        s += normal_ll(m, par[k], 0.0, v);
-        if (bi.v) gv += normal_dotarg2(m, par[k], 0.0, v);
+        s += ws.pt_ll[k];
+        if (bi.v) gv += ws.pt_dot[k];
       }
       ll += s;
     }
@@ -614,6 +630,59 @@ __device__ int nuts_transition(const HlrModelDev& m, const HlrComp& cp, const in
   return 0;
 }
 
+// ---- Reflective slice: cbits/augur_mcmclib.h:498-543 ------------------------
+// Momentum from (c*P + j, iter, MOM|ci<<8); slice level z = ll(curr) - Exp(1)
+// with the exponential from (c, iter, RSLICE|ci<<8); augur_max(1,
+// round(simlen / eps)) steps of q += eps p0, each followed by the log density
+// at the new point and, outside the slice, a reflection of p0 off the block
+// gradient there (p0 += -2 (p0.g)/(g.g) g, sequential dot products).  The
+// move is kept only if the last point is inside the slice.
+__device__ int rslice_transition(const HlrModelDev& m, const HlrComp& cp, const int* idx, Ws& ws,
+                                 uint64_t seed, uint32_t iter, uint32_t chain, uint32_t ci, int* refl_out) {
+  const int P = cp.P;
+  const int tid = threadIdx.x;
+  for (int j = tid; j < P; j += blockDim.x) {
+    Stream s = make_stream(seed, chain * (uint32_t)P + j, iter, TAG_MOM | (ci << 8));
+    ws.p0[j] = s.normal();
+  }
+  if (tid == 0) {
+    Stream h = make_stream(seed, chain, iter, TAG_RSLICE | (ci << 8));
+    ws.bcast[3] = -1.0 * log(h.uniform());
+    const unsigned rl = (unsigned)round(cp.simlen / cp.eps);
+    ws.ibcast[0] = (int)min(rl > 1u ? rl : 1u, 1u << 20);   // host bounds simlen/eps
+  }
+  for (int i = tid; i < m.D + 2; i += blockDim.x) ws.prop[i] = ws.par[i];
+  __syncthreads();
+  const double expo = ws.bcast[3];
+  const int L = ws.ibcast[0];
+  const double step = cp.eps;
+  const double z = block_ll_grad(m, ws.par, idx, P, ws, false) - expo;
+  for (int j = tid; j < P; j += blockDim.x) ws.q[j] = ws.par[idx[j]];
+  __syncthreads();
+  bool cond = false;
+  int refl = 0;
+  for (int l = 0; l < L; ++l) {
+    for (int j = tid; j < P; j += blockDim.x) ws.q[j] = __dadd_rn(ws.q[j], __dmul_rn(step, ws.p0[j]));
+    __syncthreads();
+    set_block(ws.prop, idx, P, ws.q);
+    cond = block_ll_grad(m, ws.prop, idx, P, ws, false) < z;    // same value on every thread
+    if (cond) {
+      block_ll_grad(m, ws.prop, idx, P, ws, true);
+      const double a1 = seq_dot(ws.p0, ws.blk_g, P, ws);
+      const double a2 = seq_dot(ws.blk_g, ws.blk_g, P, ws);
+      const double sc = __dmul_rn(-2.0, a1 / a2);
+      for (int j = tid; j < P; j += blockDim.x) ws.p0[j] = __dadd_rn(ws.p0[j], __dmul_rn(sc, ws.blk_g[j]));
+      __syncthreads();
+      ++refl;
+    }
+  }
+  if (!cond)
+    for (int i = tid; i < m.D + 2; i += blockDim.x) ws.par[i] = ws.prop[i];
+  __syncthreads();
+  *refl_out = refl;
+  return !cond;
+}
+
 // ---- MWG on one scalar of par: augur_mcmclib.h:89-105,178-193 ---------------
 __device__ int mwg_transition(const HlrModelDev& m, const HlrComp& cp, const int* idx, Ws& ws,
                               uint64_t seed, uint32_t iter, uint32_t chain, uint32_t ci) {
@@ -645,6 +714,7 @@ __device__ Ws carve(void* base, int D) {
   w.par = d; d += V; w.prop = d; d += V; w.g = d; d += V; w.blk_g = d; d += V;
   w.p0 = d; d += V; w.ps = d; d += V; w.q = d; d += V; w.aux1 = d; d += V; w.aux2 = d; d += V;
   w.aux3 = d; d += V; w.aux4 = d; d += V;
+  w.pt_ll = d; d += V; w.pt_dot = d; d += V;
   w.gpart = d; d += HLR_THREADS;
   w.red = d; d += 34;
   w.bcast = d; d += 8;
@@ -656,7 +726,7 @@ __device__ Ws carve(void* base, int D) {
 
 size_t hlr_smem_bytes(int D) {
   const int V = D + 2;
-  return sizeof(double) * (11 * (size_t)V + HLR_THREADS + 34 + 8 + 8 + (D + 1) / 2 + 1) +
+  return sizeof(double) * (13 * (size_t)V + HLR_THREADS + 34 + 8 + 8 + (D + 1) / 2 + 1) +
          sizeof(float) * HLR_CHUNK;
 }
 
@@ -689,6 +759,10 @@ hlr_chain_kernel(HlrModelDev m, const HlrComp* __restrict__ comps, int n_comps,
                         (uint32_t)c, (uint32_t)ci, &sh_out[0], &sh_out[1], &sh_out[2]);
         depth = sh_out[0]; leaves = sh_out[1]; err = sh_out[2];
         if (threadIdx.x == 0) { st[1] += depth; st[2] += leaves; st[3] += err; }
+      } else if (cp.kind == COMP_RSLICE) {
+        int refl = 0;
+        const int a = rslice_transition(m, cp, idx, ws, seed, iter, (uint32_t)c, (uint32_t)ci, &refl);
+        if (threadIdx.x == 0) { st[0] += a; st[2] += refl; }
       } else {
         const int a = mwg_transition(m, cp, idx, ws, seed, iter, (uint32_t)c, (uint32_t)ci);
         if (threadIdx.x == 0) st[0] += a;
@@ -775,12 +849,12 @@ extern "C" int ab_hlr_run_chains(const ab_hlr_model* model, const ab_hlr_comp* c
   bool has_nuts = false;
   for (int i = 0; i < n_comps; ++i) {
     const ab_hlr_comp& c = comps_host[i];
-    AB_REQUIRE(c.kind >= 0 && c.kind <= 2, AB_ERR_ARG, "component %d: unknown kind", i);
+    AB_REQUIRE(c.kind >= 0 && c.kind <= 3, AB_ERR_ARG, "component %d: unknown kind", i);
     AB_REQUIRE(c.P > 0 && c.P <= m.D + 2, AB_ERR_ARG, "component %d: bad block size", i);
     AB_REQUIRE(c.kind != 2 || c.P == 1, AB_ERR_ARG, "component %d: MWG moves one scalar", i);
     AB_REQUIRE(c.kind == 2 || c.eps > 0.0, AB_ERR_ARG, "component %d: step size must be > 0", i);
-    AB_REQUIRE(c.kind != 0 || (c.simlen >= 0.0 && c.simlen / c.eps <= 1e5), AB_ERR_ARG,
-               "component %d: HMC simlen/eps must be <= 1e5 leapfrog steps", i);
+    AB_REQUIRE((c.kind != 0 && c.kind != 3) || (c.simlen >= 0.0 && c.simlen / c.eps <= 1e5), AB_ERR_ARG,
+               "component %d: HMC / RSlice simlen/eps must be <= 1e5 steps", i);
     AB_REQUIRE(c.kind != 2 || c.mwg_var > 0.0, AB_ERR_ARG, "component %d: MWG variance must be > 0", i);
     AB_REQUIRE(c.kind != 1 || (c.max_depth > 0 && c.max_depth <= 14), AB_ERR_ARG,
                "component %d: NUTS max_depth must be 1..14", i);

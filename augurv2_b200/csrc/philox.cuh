@@ -78,6 +78,7 @@ enum Tag : uint32_t {
   TAG_MWG = 11,       // Metropolis-within-Gibbs
   TAG_INIT = 12,      // initial points
   TAG_DATA = 13,      // synthetic data
+  TAG_RSLICE = 14,    // reflective slice: the slice level's exponential
 };
 
 // A sequential cursor over one substream.

@@ -16,7 +16,7 @@ import torch
 
 from . import _native as N
 
-HMC, NUTS, MWG = 0, 1, 2
+HMC, NUTS, MWG, RSLICE = 0, 1, 2, 3
 
 
 class HlrComp(C.Structure):
@@ -86,6 +86,7 @@ class HlrChains:
       {"kind": "HMC", "block": ["theta"], "simlen": 0.5, "eps": 0.05}
       {"kind": "NUTS", "block": ["v", "b", "theta"], "eps": 0.05, "max_depth": 10}
       {"kind": "MWG", "var": "v", "scale": 1.0}
+      {"kind": "RSlice", "block": ["theta"], "simlen": 1.0, "eps": 0.05}
     """
 
     def __init__(self, data, schedule, C=1, init=None, seed=0, iter0=0):
@@ -104,6 +105,9 @@ class HlrChains:
                                          float(s.get("eps", 0.05)), 0.0))
                 elif kind == "NUTS":
                     comps.append(HlrComp(NUTS, len(bl), len(idx), int(s.get("max_depth", 10)), 0.0,
+                                         float(s.get("eps", 0.05)), 0.0))
+                elif kind == "RSLICE":
+                    comps.append(HlrComp(RSLICE, len(bl), len(idx), 0, float(s.get("simlen", 1.0)),
                                          float(s.get("eps", 0.05)), 0.0))
                 else:
                     raise ValueError("unknown component kind %r" % s["kind"])

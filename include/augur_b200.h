@@ -157,7 +157,8 @@ typedef struct ab_hlr_model {
 /* One schedule component: kind 0 = HMC [block] [simlen, eps]
  * (h_augur_mcmc_hmc, cbits/augur_mcmclib.h:389-424), 1 = NUTS [block] [eps]
  * (h_augur_mcmc_nuts, :693-776; max_depth bounds the doublings), 2 = MWG on
- * one scalar with a Normal(x, mwg_var) proposal (augur_mcmc_mwg, :178-193).
+ * one scalar with a Normal(x, mwg_var) proposal (augur_mcmc_mwg, :178-193),
+ * 3 = RSlice [block] [simlen, eps] (h_augur_mcmc_refl_slice, :498-543).
  * The block is idx[idx_off .. idx_off+P-1] of the index array. */
 typedef struct ab_hlr_comp {
   int kind, P, idx_off, max_depth;
@@ -174,12 +175,13 @@ int ab_hlr_ll_grad(const ab_hlr_model* model, const int* idx_dev, const int* idx
 
 /* n_iter augur_step calls of a schedule of components for C independent
  * chains (one thread block per chain, the whole iteration on chip).
- * pars f64[C][D+2] in/out; stats f64[C][n_comps][4] accumulates {accepts,
- * NUTS depth, NUTS leaves, stack overflows}.  scratch:
+ * pars f64[C][D+2] in/out; stats f64[C][n_comps][4] accumulates {accepts
+ * (moves for RSlice), NUTS depth, NUTS leaves or RSlice reflections, stack
+ * overflows}.  scratch:
  * ab_hlr_chain_scratch_bytes(C, D) bytes, needed when a NUTS component is
  * present.  Substreams: momentum (c*P+j, iter, 4|comp<<8), HMC jitter and
  * accept (c, iter, 5|comp<<8), NUTS (c, iter, 6|comp<<8), MWG (c, iter,
- * 11|comp<<8). */
+ * 11|comp<<8), RSlice slice level (c, iter, 14|comp<<8). */
 size_t ab_hlr_chain_scratch_bytes(int C, int D);
 int ab_hlr_run_chains(const ab_hlr_model* model, const ab_hlr_comp* comps_host, const void* comps_dev,
                       int n_comps, const int* idx_dev, const int* idx_host, int C, double* pars,

@@ -386,6 +386,55 @@ int orc_hlr_hmc(const orc_hlr* m, double* par, const int* idx, int P, double sim
   return acc;
 }
 
+/* ---- Reflective slice: cbits/augur_mcmclib.h:498-543 (h_augur_mcmc_refl_slice)
+ * Momentum p0 ~ N(0, I) from (c*P + j, iter, MOM|comp<<8); the slice level
+ * z = ll(curr) - Exp(1) with the exponential from (c, iter, RSLICE|comp<<8);
+ * simsteps = augur_max(1, round(simlen / eps)) (unsigned); each step moves
+ * the block by eps * p0 and, if the point left the slice (ll < z), reflects
+ * p0 off the gradient there: p0 += (-2 (p0.g)/(g.g)) g.  The move is kept
+ * only if the last point is inside the slice.  Returns 1 on a move;
+ * `reflections_out` counts the reflections. */
+int orc_hlr_rslice(const orc_hlr* m, double* par, const int* idx, int P, double simlen, double eps,
+                   uint64_t seed, uint32_t iter, uint32_t chain, uint32_t comp, int* simsteps_out,
+                   int* reflections_out) {
+  const int NP = m->D + 2;
+  double* p0 = (double*)malloc(sizeof(double) * P);
+  double* g = (double*)malloc(sizeof(double) * P);
+  double* ths = (double*)malloc(sizeof(double) * P);
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  for (int j = 0; j < P; ++j) {
+    orc_stream s = orc_make(seed, chain * (uint32_t)P + j, iter, ORC_TAG_MOM | (comp << 8));
+    p0[j] = orc_normal(&s);
+  }
+  orc_stream h = orc_make(seed, chain, iter, ORC_TAG_RSLICE | (comp << 8));
+  const double z = orc_hlr_ll(m, par, idx, P) - (-1.0 * log(orc_uniform(&h)));
+  const double stepsize = eps;
+  unsigned rl = (unsigned)round(simlen / stepsize);
+  const int simsteps = (int)(rl > 1u ? rl : 1u);
+  memcpy(prop, par, sizeof(double) * NP);
+  orc_get_block(par, idx, P, ths);
+  int cond = 0, refl = 0;
+  for (int i = 0; i < simsteps; ++i) {
+    for (int j = 0; j < P; ++j) ths[j] = ths[j] + stepsize * p0[j];
+    orc_set_block(prop, idx, P, ths);
+    cond = orc_hlr_ll(m, prop, idx, P) < z;
+    if (cond) {
+      orc_hlr_grad(m, prop, idx, P, g);
+      double a1 = 0.0, a2 = 0.0;
+      for (int j = 0; j < P; ++j) a1 += p0[j] * g[j];
+      for (int j = 0; j < P; ++j) a2 += g[j] * g[j];
+      const double scale = a1 / a2;
+      for (int j = 0; j < P; ++j) p0[j] = p0[j] + (-2.0 * scale) * g[j];
+      ++refl;
+    }
+  }
+  if (!cond) memcpy(par, prop, sizeof(double) * NP);
+  if (simsteps_out) *simsteps_out = simsteps;
+  if (reflections_out) *reflections_out = refl;
+  free(p0); free(g); free(ths); free(prop);
+  return !cond;
+}
+
 /* ---- NUTS: cbits/augur_mcmclib.h:575-776, restated with its exact control
  * flow (two gradients per leaf, the stacks of augur_blkstk.c, the subtree
  * endpoints taken from the most recent j == 1 push, the proposal kept only

@@ -218,6 +218,24 @@ def hlr_hmc(o, m, par, idx, simlen, eps, seed, it, chain=0, comp=0):
     return acc, L.value, prop
 
 
+def hlr_rslice(o, m, par, idx, simlen, eps, seed, it, chain=0, comp=0):
+    """One reflective-slice transition (cbits/augur_mcmclib.h:498-543); par
+    is updated in place.  Returns (moved, simsteps, reflections) for the
+    restatement, None for the reference build."""
+    idx = _idx(idx)
+    if o.kind == "ref":
+        _hlr_call(o, "hlr_rslice", m, None,
+                  [_dp, _ip, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32],
+                  dptr(par), iptr(idx), len(idx), simlen, eps, seed, it, chain, comp)
+        return None
+    L, R = C.c_int(), C.c_int()
+    moved = _hlr_call(o, "hlr_rslice", m, C.c_int,
+                      [_dp, _ip, C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_uint32, C.c_uint32,
+                       C.c_uint32, C.POINTER(C.c_int), C.POINTER(C.c_int)],
+                      dptr(par), iptr(idx), len(idx), simlen, eps, seed, it, chain, comp, C.byref(L), C.byref(R))
+    return moved, L.value, R.value
+
+
 def hlr_nuts(o, m, par, idx, eps, seed, it, chain=0, comp=0, max_depth=64):
     idx = _idx(idx)
     if o.kind == "ref":

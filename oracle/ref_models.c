@@ -342,6 +342,30 @@ int ref_hlr_hmc(int N, int D, int has_b, int vprior, double lam, double a0, doub
   return !moved;   /* invariant curr == prop holds after the kernel; 1 = states agree */
 }
 
+/* One reflective-slice transition through the reference's
+ * h_augur_mcmc_refl_slice (cbits/augur_mcmclib.h:498-543). */
+void ref_hlr_rslice(int N, int D, int has_b, int vprior, double lam, double a0, double s0,
+                    const double* X, const int* y, double* par, const int* idx, int P, double simlen,
+                    double eps, uint64_t seed, uint32_t iter, uint32_t chain, uint32_t comp) {
+  ref_hlr_setup(N, D, has_b, vprior, lam, a0, s0, X, y, idx, P, seed);
+  const int NP = D + 2;
+  double* prop = (double*)malloc(sizeof(double) * NP);
+  double* mem = (double*)calloc((size_t)2 * P, sizeof(double));
+  memcpy(prop, par, sizeof(double) * NP);
+  g_hlr.gbuf = mem;
+  ref_blk th0 = mk_blk_idx(par, idx, P), ths = mk_blk_idx(prop, idx, P);
+  ref_blk gb = mk_blk_dense(mem, P), p0 = mk_blk_dense(mem + P, P);
+  AugurAux_t aux; AugurMod_t curr, pr;
+  aux.rng = g_aux_rng; curr.par = par; pr.par = prop;
+  orc_shim_seek_elementwise(g_aux_rng, chain * (uint32_t)P, iter, ORC_TAG_MOM | (comp << 8));
+  orc_shim_seek(h_rng, chain, iter, ORC_TAG_RSLICE | (comp << 8));
+  MCMC.aux = aux; MCMC.curr = curr; MCMC.prop = pr;
+  h_augur_mcmc_refl_slice(AUGUR_CPU, aux, curr, pr, &th0.blk, &ths.blk, &gb.blk, &p0.blk, simlen, eps,
+                          ref_hlr_grad_fn, ref_hlr_ll_fn);
+  free_blk(&th0); free_blk(&ths); free_blk(&gb); free_blk(&p0);
+  free(prop); free(mem);
+}
+
 /* One NUTS transition through the reference's h_augur_mcmc_nuts.  The
  * reference prints its proposal stack at every inner node. */
 void ref_hlr_nuts(int N, int D, int has_b, int vprior, double lam, double a0, double s0,

@@ -130,7 +130,8 @@ def make_lda(ref):
 def make_hlr(ref):
     """HLR on the reference's hlr.rv model (Exponential variance prior with
     bias) and on the InvGamma variant without bias: log-densities, gradients
-    and HMC / NUTS / MWG transitions of the reference's own kernels."""
+    and HMC / NUTS / MWG / reflective-slice transitions of the reference's
+    own kernels."""
     out = {}
     for name, (N, D, has_b, vprior) in {"hlr": (120, 6, True, "exponential"),
                                         "ighlr": (150, 4, False, "invgamma")}.items():
@@ -163,7 +164,11 @@ def make_hlr(ref):
         for it in range(6):
             O.hlr_mwg(ref, m, p, D + 1, 0.5, 7, it)
             mwg.append(p.copy())
-        rec.update(par0=par0, hmc=np.array(hmc), nuts=np.array(nuts), mwg=np.array(mwg))
+        p = par0.copy(); rslice = []
+        for it in range(8):
+            O.hlr_rslice(ref, m, p, blocks["theta"], 0.5, 0.05, 7, it)
+            rslice.append(p.copy())
+        rec.update(par0=par0, hmc=np.array(hmc), nuts=np.array(nuts), mwg=np.array(mwg), rslice=np.array(rslice))
         np.savez_compressed(os.path.join(HERE, name + "_golden.npz"), **rec)
 
 

@@ -46,6 +46,22 @@ def test_hlr_example_schedules_run():
             assert all(v > 0 for v in s["v"])
 
 
+def test_hlr_rslice_schedule_runs():
+    """The reflective-slice kernel from the schedule language (RSlice [theta]
+    [simlen, eps], Rv/ParseRv.y:136) composed with MWG on the variance."""
+    rec = MODELS["examples"]["hlr"]
+    X, y, beta, s2 = O.hlr_synthetic(500, 6, 3, has_b=True)
+    with AugurInfer("config.yml", rec["model"]) as infer:
+        infer.set_compile_opt(AugurOpt(cached=False, target="cpu", paramScale=None, seed=2))
+        infer.set_user_sched("MWG [v] ~ Normal(v, 0.5) (*) MWG [b] ~ Normal(b, 0.5) (*) RSlice [theta] [0.5, 0.02]")
+        infer.compile(6, 500, 1.0, X)(y)
+        s = infer.samplen(burnIn=30, numSamples=40)
+        th = np.array(s["theta"])
+        assert th.shape == (40, 6) and np.isfinite(th).all()
+        assert len({tuple(r) for r in th}) > 5, "the reflective slice never moved"
+        assert all(v > 0 for v in s["v"])
+
+
 def test_dethlr_returns_the_deterministic_bias():
     src = MODELS["rv"]["dethlr"]
     X, y, beta, s2 = O.hlr_synthetic(200, 3, 4, has_b=True)

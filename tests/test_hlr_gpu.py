@@ -1,5 +1,5 @@
-"""GPU parity of the HLR log-density / gradient and of the HMC, NUTS and MWG
-transitions against the CPU oracle (itself pinned to the reference's own
+"""GPU parity of the HLR log-density / gradient and of the HMC, NUTS, MWG and
+reflective-slice transitions against the CPU oracle (itself pinned to the reference's own
 kernels).
 
 Tolerances: the data terms run in FP32 with compensated sums, so block
@@ -141,6 +141,29 @@ def test_mwg_matches_oracle(orc):
             assert int(st[0, 0, 0]) == acc
             np.testing.assert_allclose(got[0], p_ref, rtol=1e-12)
             p = p_ref
+
+
+@pytest.mark.parametrize("block,simlen,eps", [(["theta"], 0.5, 0.05), (["v", "b", "theta"], 1.0, 0.08)])
+def test_rslice_matches_oracle(orc, block, simlen, eps):
+    """Reflective slice (h_augur_mcmc_refl_slice): the same move or stay,
+    the same number of reflections, and the same end point (1e-4) as the
+    oracle, itself equal to the reference's kernel bit for bit."""
+    X, y, beta, s2, om, gd = make(400, 5, 17, True, "exponential", True)
+    D = 5
+    idx = H.block_indices(block, D)
+    par = np.concatenate([beta, [0.1], [max(s2, 0.5)]])
+    agree, refl_total = 0, 0
+    for it in range(10):
+        p_ref = par.copy()
+        moved, L, refl = O.hlr_rslice(orc, om, p_ref, idx, simlen, eps, 19, it)
+        got, st = run_one(gd, [{"kind": "RSlice", "block": block, "simlen": simlen, "eps": eps}], par, it, 19)
+        refl_total += refl
+        if int(st[0, 0, 0]) == moved and int(st[0, 0, 2]) == refl and \
+                np.allclose(got[0], p_ref, rtol=1e-4, atol=1e-6):
+            agree += 1
+        par = p_ref
+    assert agree >= 9
+    assert refl_total > 0
 
 
 def test_schedule_composition_runs():

@@ -143,6 +143,10 @@ def test_hlr_golden_transitions(orc, name):
     for it in range(6):
         O.hlr_mwg(orc, m, p, D + 1, 0.5, 7, it)
         np.testing.assert_array_equal(p, g["mwg"][it])
+    p = g["par0"].copy()
+    for it in range(8):
+        O.hlr_rslice(orc, m, p, g["idx_theta"], 0.5, 0.05, 7, it)
+        np.testing.assert_array_equal(p, g["rslice"][it])
 
 
 @pytest.mark.parametrize("seed", [0, 1])
@@ -159,6 +163,14 @@ def test_hlr_oracle_vs_reference_live(orc, ref, seed):
         O.hlr_nuts(orc, m, a, [4, 3, 0, 1, 2], 0.1, seed, it)
         O.hlr_nuts(ref, m, b, [4, 3, 0, 1, 2], 0.1, seed, it)
         np.testing.assert_array_equal(a, b)
+    a, b = par.copy(), par.copy()
+    refl = 0
+    for it in range(10):
+        _, _, r = O.hlr_rslice(orc, m, a, [0, 1, 2, 3], 1.0, 0.08, seed, it, chain=2, comp=1)
+        O.hlr_rslice(ref, m, b, [0, 1, 2, 3], 1.0, 0.08, seed, it, chain=2, comp=1)
+        np.testing.assert_array_equal(a, b)
+        refl += r
+    assert refl > 0, "the chain never left the slice: reflections untested"
 
 
 def test_hlr_gradient_finite_difference(orc):
