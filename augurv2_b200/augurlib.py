@@ -250,6 +250,24 @@ class AugurInfer:
         assert self.backend is not None
         return self.backend.curr_ll()
 
+    def checkpoint(self, path):
+        """Save the sampler's state (device tensors, iteration counters) to
+        `path`; resume() on a model compiled with the same data continues the
+        chains bit for bit (no reference counterpart: the reference keeps its
+        state in process globals)."""
+        import torch
+        assert self.backend is not None
+        torch.save({"param_names": list(self.param_names), "state": self.backend.state_dict()}, path)
+
+    def resume(self, path):
+        import torch
+        assert self.backend is not None
+        d = torch.load(path, weights_only=False)
+        if list(d["param_names"]) != list(self.param_names):
+            raise ValueError("checkpoint of a model with parameters %s, this one has %s"
+                             % (d["param_names"], self.param_names))
+        self.backend.load_state_dict(d["state"])
+
     def sample(self):
         assert self.backend is not None
         self.backend.step(1)

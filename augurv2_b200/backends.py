@@ -70,6 +70,12 @@ class LdaBackend:
         z = np.concatenate([np.asarray(x, np.int32) for x in pt[self.info["z"]]])
         self.s.set_state(theta=pt[self.info["theta"]], phi=pt[self.info["phi"]], z=z)
 
+    def state_dict(self):
+        return self.s.state_dict()
+
+    def load_state_dict(self, d):
+        self.s.load_state_dict(d)
+
     def curr_ll(self):
         """Joint log density in the reference's terms (augur_dirichlet_ll has
         no normalising constant, cbits/augur_dist.c:489-497)."""
@@ -176,6 +182,12 @@ class HlrBackend:
             s[:, D] = np.asarray(pt[self.info["b"]], np.float64)
         self.chains.pars.copy_(torch.as_tensor(s))
 
+    def state_dict(self):
+        return self.chains.state_dict()
+
+    def load_state_dict(self, d):
+        self.chains.load_state_dict(d)
+
     def curr_ll(self):
         """Joint log density (augur_get_curr_ll, CgStInit.hs:597-602): the
         block of all parameters has every factor in its full conditional."""
@@ -263,6 +275,12 @@ class GmmBackend:
         if self.family == "hmvgmm":
             kw.update(pis=pt[self.info["pis"]], cov=pt[self.info["cov"]])
         self.s.set_state(**kw)
+
+    def state_dict(self):
+        return self.s.state_dict()
+
+    def load_state_dict(self, d):
+        self.s.load_state_dict(d)
 
     def curr_ll(self):
         from scipy.stats import multivariate_normal as mvn

@@ -16,9 +16,13 @@ import numpy as np
 import torch
 
 from . import _native as N
+from .checkpoint import Checkpointable
 
 
-class GmmGibbs:
+class GmmGibbs(Checkpointable):
+    _ckpt_tensors = ("mu", "cov", "pis", "z", "Linv", "hdet", "cnt", "sum", "obs", "shrinks", "accepts")
+    _ckpt_scalars = ("iteration", "seed")
+
     def __init__(self, Y, K, mu0, cov0, pis=None, covs=None, alpha=None, df=None, scale0=None,
                  mu=None, cov=None, z=None, move="conj", prop_cov=None, compat=True, seed=0, iter0=0,
                  device="cuda"):

@@ -15,6 +15,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from .checkpoint import Checkpointable
 
 HMC, NUTS, MWG, RSLICE = 0, 1, 2, 3
 
@@ -79,7 +80,10 @@ def ll_grad(data, pars, idx, stream=None):
     return ll.cpu().numpy(), g.cpu().numpy()
 
 
-class HlrChains:
+class HlrChains(Checkpointable):
+    _ckpt_tensors = ("pars", "stats")
+    _ckpt_scalars = ("iteration", "seed")
+
     """C chains of a schedule over one HLR data set.
 
     schedule: list of dicts, e.g.

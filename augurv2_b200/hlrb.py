@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from .checkpoint import Checkpointable
 
 PRIOR_NORMAL, PRIOR_STUDENT_T = 0, 1
 
@@ -162,7 +163,13 @@ class _ChainState:
                 "ab_hmcb_final")
 
 
-class BatchedHmc:
+_CHAIN_TENSORS = ("s.theta", "s.p", "s.g_cur", "s.logp_cur", "s.theta0", "s.g0", "s.logp0", "s.H0", "s.eps_c", "s.stats", "s.iter", "s.eps0")
+
+
+class BatchedHmc(Checkpointable):
+    _ckpt_tensors = _CHAIN_TENSORS
+    _ckpt_scalars = ("n_grad",)
+
     """C chains of exact-gradient HMC on an HlrbData: L leapfrog steps of size
     eps (jittered per chain by +-jitter), FP64 energies, one exact log density
     and gradient per step."""
@@ -236,7 +243,16 @@ class BatchedHmc:
         self.s.iter.zero_()
 
 
-class MlpSurrogate:
+class MlpSurrogate(Checkpointable):
+    _ckpt_tensors = ("w", "wb", "m", "v", "mu", "inv_s", "a", "h", "o", "buf_theta", "buf_grad")
+    _ckpt_scalars = ("step_count", "n_buf", "pos", "use_net")
+
+    def _ckpt_extra(self):
+        return {"gen": self.gen.get_state()}
+
+    def _ckpt_load_extra(self, extra):
+        self.gen.set_state(extra["gen"])
+
     """Gradient surrogate g(theta) ~ a + h (theta - mu) + o * MLP((theta - mu) / s).
 
     The diagonal linear part (a, h per coordinate) is a least-squares fit of
@@ -380,7 +396,16 @@ class MlpSurrogate:
         return float(torch.linalg.vector_norm(gh - grad) / torch.linalg.vector_norm(grad).clamp_min(1e-30))
 
 
-class SurrogateHmc:
+class SurrogateHmc(Checkpointable):
+    _ckpt_tensors = _CHAIN_TENSORS + ("g_exact",)
+    _ckpt_scalars = ("it", "fallback", "last_rel_err", "n_grad", "n_logp")
+
+    def _ckpt_extra(self):
+        return {"sur": self.sur.state_dict()}
+
+    def _ckpt_load_extra(self, extra):
+        self.sur.load_state_dict(extra["sur"])
+
     """HMC whose leapfrog uses the surrogate gradient; the exact log density
     (tensor-core forward pass) decides every accept, so each chain targets the
     exact posterior.  Every `train_every` iterations the exact gradient at the
@@ -526,7 +551,11 @@ def adapt_step_size(sampler, n, target=0.8, rate=1.5, lo=1e-6, hi=10.0, run_kw=N
     return eps
 
 
-class BatchedNuts:
+class BatchedNuts(Checkpointable):
+    # the resumable tree walks, draw histories and iteration counters
+    _ckpt_tensors = ("mem", "logp_new", "g_new")
+    _ckpt_scalars = ("rounds",)
+
     """C chains of the reference's NUTS (cbits/augur_mcmclib.h:575-776) on an
     HlrbData, advanced together: each round every chain walks its tree to the
     next leaf (ab_nutsb_advance) and one tensor-core pass evaluates the log

@@ -16,6 +16,7 @@ import numpy as np
 import torch
 
 from . import _native as N
+from .checkpoint import Checkpointable
 
 
 def flatten_docs(w):
@@ -32,7 +33,15 @@ def flatten_docs(w):
     return off.astype(np.int32), flat.astype(np.int32)
 
 
-class LdaGibbs:
+class LdaGibbs(Checkpointable):
+    # the assignments and the iteration determine the rest (the counts are
+    # recounted and theta / phi are redrawn before they are used)
+    _ckpt_tensors = ("theta", "phiT", "z", "cnt_dk", "cnt_kw")
+    _ckpt_scalars = ("iteration", "seed")
+
+    def _ckpt_after_load(self):
+        N.check(N.lib().ab_lda_init_state(self._h, self.iteration, N.stream_ptr()), "ab_lda_init_state")
+
     def __init__(self, K, V, doc_off, w, alpha, beta, seed=0, theta=None, phi=None, z=None,
                  iter0=0, device="cuda"):
         self.dev = torch.device(device)

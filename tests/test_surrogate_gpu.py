@@ -141,3 +141,30 @@ def test_surrogate_chain_targets_the_exact_posterior():
     assert np.max(np.abs(z)) < 5.0
     sd_s = ds.reshape(-1, D).std(0)
     assert np.all(np.abs(sd_s / sd - 1.0) < 0.1)
+
+
+def test_nan_surrogate_falls_back_to_exact_hmc():
+    """Host-side fault injection: the network's weights are overwritten with
+    NaN mid-run.  Trajectories it drives are rejected by the exact log
+    density (the chains stay finite), the next error check measures a NaN
+    error and switches the sampler to exact-gradient HMC, which accepts
+    again; no GPU fault is involved."""
+    N_, D, C = 20_000, 16, 32
+    X, y, beta = H.synthetic(N_, D, seed=6)
+    d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
+    init = np.asarray(beta, np.float32)[None] + 1e-3 * np.random.default_rng(0).standard_normal((C, D)).astype(np.float32)
+    sur = H.SurrogateHmc(d, C, L=5, eps=0.01, jitter=0.1, seed=2, init=init, train_every=4, train_steps=5)
+    sur.run(8)
+    assert not sur.fallback
+    before = sur.theta.clone()
+    sur.sur.w.fill_(float("nan"))
+    sur.sur.a.fill_(float("nan"))
+    N_check = 4 - sur.it % 4
+    sur.run(N_check)                      # up to and including the next check
+    assert sur.fallback and not np.isfinite(sur.last_rel_err)
+    assert torch.isfinite(sur.theta).all()
+    sur.reset_stats()
+    sur.run(12)                           # exact-gradient HMC from here
+    assert torch.isfinite(sur.theta).all()
+    assert sur.accept_rate()[0] > 0.3
+    assert not torch.equal(before, sur.theta)
