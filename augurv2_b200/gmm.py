@@ -17,6 +17,7 @@ import torch
 
 from . import _native as N
 from .checkpoint import Checkpointable
+from .trace import traced
 
 
 class GmmGibbs(Checkpointable):
@@ -74,6 +75,7 @@ class GmmGibbs(Checkpointable):
             N.check(L.ab_gmm_prep(1, d, N.ptr(self.cov), N.ptr(self.Linv), N.ptr(self.hdet), st), "prep")
 
     # ---- one augur_step ----------------------------------------------------
+    @traced("gmm.sweep")
     def sweep(self, n=1, stream=None):
         L = N.lib()
         st = N.stream_ptr(stream)

@@ -16,6 +16,7 @@ import torch
 
 from . import _native as N
 from .checkpoint import Checkpointable
+from .trace import traced
 
 HMC, NUTS, MWG, RSLICE = 0, 1, 2, 3
 
@@ -132,6 +133,7 @@ class HlrChains(Checkpointable):
         nbytes = int(N.lib().ab_hlr_chain_scratch_bytes(self.C, D)) if need_nuts else 8
         self.scratch = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
 
+    @traced("hlr.run_chains")
     def run(self, n_iter=1, stream=None):
         N.check(N.lib().ab_hlr_run_chains(C.byref(self.data.c), self.comps_h, N.ptr(self.comps_d),
                                           self.ncomp, N.ptr(self.idx_d),

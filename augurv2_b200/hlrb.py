@@ -19,6 +19,7 @@ import torch
 
 from . import _native as N
 from .checkpoint import Checkpointable
+from .trace import traced
 
 PRIOR_NORMAL, PRIOR_STUDENT_T = 0, 1
 
@@ -223,6 +224,7 @@ class BatchedHmc(Checkpointable):
         for t, v in zip(keep, saved):
             t.copy_(v)
 
+    @traced("hmcb.run")
     def run(self, n=1, record=None):
         for _ in range(int(n)):
             if self.graph is not None:
@@ -514,6 +516,7 @@ class SurrogateHmc(Checkpointable):
         for t, v in zip((self.s.theta, self.s.g_cur, self.s.logp_cur, self.s.stats, self.s.iter), saved):
             t.copy_(v)
 
+    @traced("surrogate.run")
     def run(self, n=1, learn=True, record=None):
         for _ in range(int(n)):
             check = learn and (self.it % self.train_every == 0)
@@ -625,6 +628,7 @@ class BatchedNuts(Checkpointable):
         with torch.cuda.graph(self.graph, stream=stream):
             self._round(torch.cuda.current_stream())
 
+    @traced("nutsb.run")
     def run(self, rounds):
         for _ in range(int(rounds)):
             if self.graph is not None:
@@ -715,6 +719,7 @@ class NutsPool:
         """Draws recorded by sampler i's slowest chain."""
         return int(self.samplers[i].info()[:, 0].min())
 
+    @traced("nuts_pool.run")
     def run(self, min_draws, max_rounds, block=25, share="equal"):
         """Replay rounds until every sampler has min_draws draws per chain;
         returns the number of rounds each sampler ran in this call.  share:

@@ -17,6 +17,7 @@ import torch
 
 from . import _native as N
 from .checkpoint import Checkpointable
+from .trace import traced
 
 
 def flatten_docs(w):
@@ -102,6 +103,7 @@ class LdaGibbs(Checkpointable):
                 self.z.cpu().numpy())
 
     # ---- sampling ----------------------------------------------------------
+    @traced("lda.sweep")
     def sweep(self, n=1, graph=True, stream=None):
         N.check(N.lib().ab_lda_run(self._h, int(n), int(bool(graph)), N.stream_ptr(stream)),
                 "ab_lda_run")
