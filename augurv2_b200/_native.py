@@ -19,6 +19,8 @@ class AugurError(RuntimeError):
 _lib = None
 
 i32, u32, u64, f64, f32 = C.c_int, C.c_uint32, C.c_uint64, C.c_double, C.c_float
+# status codes of include/augur_b200.h
+AB_OK, AB_ERR_ARG, AB_ERR_CUDA, AB_ERR_TIMEOUT, AB_ERR_NUMERIC, AB_ERR_STATE = range(6)
 vp, sz = C.c_void_p, C.c_size_t
 
 
@@ -110,6 +112,8 @@ _SIGS = {
     "ab_sur_post": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
     # tensor-core GEMM core
     "ab_tc_gemm_bf16": (i32, [i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp, vp]),
+    # scalar conjugate updates
+    "ab_conj_scalar": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, u64, u32, vp]),
     # GMM
     "ab_gmm_table_doubles": (sz, [i32, i32]),
     "ab_gmm_prep": (i32, [i32, i32, vp, vp, vp, vp]),

@@ -39,14 +39,19 @@ __device__ __forceinline__ double gamma_ge1(Stream& s, double alpha) {
 }
 
 // cbits/augur_dist.c:302-312: boost shape < 1 through Gamma(shape + 1).
+// The rejection loop is written once for both cases (its shape argument
+// selected first), so that a warp whose lanes mix shapes below and above 1
+// runs one copy of the loop instead of the two branches' copies in turn;
+// every lane still performs the reference's operations in its order.
 __device__ __forceinline__ double gamma_draw(Stream& s, double shape, double rate) {
   const double scale = 1.0 / rate;
-  if (shape < 1.0) {
-    double x = gamma_ge1(s, __dadd_rn(shape, 1.0));
+  const bool boost = shape < 1.0;
+  double x = gamma_ge1(s, boost ? __dadd_rn(shape, 1.0) : shape);
+  if (boost) {
     double u = s.uniform();
-    return __dmul_rn(__dmul_rn(x, pow(u, 1.0 / shape)), scale);
+    x = __dmul_rn(x, pow(u, 1.0 / shape));
   }
-  return __dmul_rn(gamma_ge1(s, shape), scale);
+  return __dmul_rn(x, scale);
 }
 
 }  // namespace ab

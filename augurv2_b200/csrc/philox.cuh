@@ -79,6 +79,7 @@ enum Tag : uint32_t {
   TAG_INIT = 12,      // initial points
   TAG_DATA = 13,      // synthetic data
   TAG_RSLICE = 14,    // reflective slice: the slice level's exponential
+  TAG_CONJ = 15,      // scalar conjugate updates
 };
 
 // A sequential cursor over one substream.

@@ -416,6 +416,46 @@ int ab_sur_post(int C, int D, const float* theta, const float* out, const float*
 int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                     int splits, int* err, void* stream);
 
+/* ======================================================================= *
+ * Scalar conjugate Gibbs updates: the one-parameter conjugate pairs of the
+ * reference library (cbits/augur_dist.c), which its compiler does not emit,
+ * as one batched step over G groups.  Replaces, per group g,
+ *   AB_CONJ_BETA_BERNOULLI     augur_beta_bernoulli_conj  (augur_dist.c:185-189)
+ *                              p ~ Beta(h0 + sum, h1 + cnt - sum)
+ *   AB_CONJ_BETA_GEOMETRIC     augur_beta_geometric_conj  (:191-195)
+ *                              p ~ Beta(h0 + cnt, h1 + sum)
+ *   AB_CONJ_GAMMA_POISSON      augur_gamma_poisson_conj   (:314-318)
+ *                              l ~ Gamma(h0 + sum, rate h1 + cnt)
+ *   AB_CONJ_GAMMA_EXPONENTIAL  augur_gamma_exponential_conj (:320-324)
+ *                              l ~ Gamma(h0 + cnt, rate h1 + sum)
+ *   AB_CONJ_GAMMA_GAMMASHAPE   augur_gamma_gammashape_conj (:326-330)
+ *                              b ~ Gamma(h0 + sum aux, rate h1 + sum)
+ *   AB_CONJ_GAMMA_INVGAMMA     augur_gamma_invgamma_conj  (:332-336)
+ *                              b ~ Gamma(h0 + sum aux, rate h1 + sum 1/x)
+ *   AB_CONJ_NORMAL_NORMALMEAN  augur_normal_normalmean_conj (:408-412)
+ *                              m ~ Normal posterior of prior N(h0, h1) and
+ *                              observations N(m, h2)
+ * with cnt = off[g+1] - off[g] and sums over the group's observations
+ * x[off[g] .. off[g+1]) (device, f64; aux = their known shapes for the
+ * gammashape / invgamma kinds, else ignored).  h0, h1, h2 are device arrays
+ * of G values (per_group = 1) or of one value (per_group = 0).  stat_sum /
+ * stat_aux (optional, G doubles) receive the statistics (stat_aux = sum of
+ * aux, or cnt).  Group g draws from Philox substream (g, iter, 15).
+ * Posterior parameters that are not positive and finite give NaN.
+ * ======================================================================= */
+enum {
+  AB_CONJ_BETA_BERNOULLI = 0,
+  AB_CONJ_BETA_GEOMETRIC = 1,
+  AB_CONJ_GAMMA_POISSON = 2,
+  AB_CONJ_GAMMA_EXPONENTIAL = 3,
+  AB_CONJ_GAMMA_GAMMASHAPE = 4,
+  AB_CONJ_GAMMA_INVGAMMA = 5,
+  AB_CONJ_NORMAL_NORMALMEAN = 6
+};
+int ab_conj_scalar(int kind, int G, const int* off, const double* x, const double* aux, const double* h0,
+                   const double* h1, const double* h2, int per_group, double* stat_sum, double* stat_aux,
+                   double* out, uint64_t seed, uint32_t iter, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -977,3 +977,54 @@ int orc_gmm_mwg(const orc_gmm* g, double* mu, const double* cov, const int* z, c
   return acc;
 }
 #undef M_
+
+/* ------------------------------------------------------------------------
+ * Scalar conjugate updates over G groups (group g owns observations
+ * x[off[g] .. off[g+1])).  Statistics as a generated conj_stat loop would
+ * form them (sequential over the observations, CgConj.hs:100-164); draws as
+ * cbits/augur_dist.c: beta kinds :185-195 over augur_beta_sample :179-183,
+ * gamma kinds :314-336, normal mean :408-412 over augur_normal_sample
+ * :404-406.  kind numbering: 0 beta_bernoulli, 1 beta_geometric,
+ * 2 gamma_poisson, 3 gamma_exponential, 4 gamma_gammashape,
+ * 5 gamma_invgamma, 6 normal_normalmean.  Group g draws from substream
+ * (g, iter, ORC_TAG_CONJ).
+ * --------------------------------------------------------------------- */
+static double orc_beta(orc_stream* s, double a, double b) {
+  double x = orc_gamma(s, a, 1.0);
+  double y = orc_gamma(s, b, 1.0);
+  return x / (x + y);
+}
+
+void orc_conj_scalar(int kind, int G, const int* off, const double* x, const double* aux,
+                     const double* h0, const double* h1, const double* h2, int per_group,
+                     double* stat_sum, double* stat_aux, double* out, uint64_t seed, uint32_t iter) {
+  for (int g = 0; g < G; ++g) {
+    const int cnt = off[g + 1] - off[g];
+    double sum = 0.0, asum = 0.0;
+    for (int n = off[g]; n < off[g + 1]; ++n) {
+      sum += kind == 5 ? 1.0 / x[n] : x[n];
+      if (kind == 4 || kind == 5) asum += aux[n];
+    }
+    if (stat_sum) stat_sum[g] = sum;
+    if (stat_aux) stat_aux[g] = (kind == 4 || kind == 5) ? asum : (double)cnt;
+    const int j = per_group ? g : 0;
+    const double a = h0[j], b = h1[j];
+    orc_stream s = orc_make(seed, (uint32_t)g, iter, ORC_TAG_CONJ);
+    double r;
+    switch (kind) {
+      case 0: r = orc_beta(&s, a + (double)(int)sum, b + (double)(cnt - (int)sum)); break;
+      case 1: r = orc_beta(&s, a + (double)cnt, b + (double)(int)sum); break;
+      case 2: r = orc_gamma(&s, a + (double)(int)sum, b + (double)cnt); break;
+      case 3: r = orc_gamma(&s, a + (double)cnt, b + sum); break;
+      case 4:
+      case 5: r = orc_gamma(&s, a + asum, b + sum); break;
+      default: {
+        const double var = h2[j];
+        const double pv = 1.0 / (1.0 / b + cnt / var);
+        const double pm = (a / b + sum / var) * pv;
+        r = pm + sqrt(pv) * orc_normal(&s);
+      }
+    }
+    out[g] = r;
+  }
+}

@@ -26,6 +26,7 @@ PREFIX = {"oracle": "orc_", "ref": "ref_"}
 
 TAG_Z, TAG_THETA, TAG_PHI, TAG_MOM, TAG_HMC, TAG_NUTS = 1, 2, 3, 4, 5, 6
 TAG_PI, TAG_MU, TAG_COV, TAG_ESLICE, TAG_MWG, TAG_INIT, TAG_DATA = 7, 8, 9, 10, 11, 12, 13
+TAG_RSLICE, TAG_CONJ = 14, 15
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -96,6 +97,25 @@ class Oracle:
         f.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_int, _dp]
         f(seed, elem, it, tag, n, int(normal), dptr(out))
         return out
+
+    # ---- scalar conjugate updates ----------------------------------------------
+    def conj_scalar(self, kind, off, x, h0, h1, h2=None, aux=None, seed=0, it=0):
+        """Per-group statistics and draws; returns (out, stat_sum, stat_aux).
+        h0 / h1 / h2: scalars or arrays of G values."""
+        off = np.ascontiguousarray(off, dtype=np.int32)
+        G = len(off) - 1
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        aux = None if aux is None else np.ascontiguousarray(aux, dtype=np.float64)
+        per_group = int(np.ndim(h0) > 0)
+        hs = [np.ascontiguousarray(np.atleast_1d(h if h is not None else 0.0), dtype=np.float64)
+              for h in (h0, h1, h2)]
+        out, ssum, saux = (np.zeros(G) for _ in range(3))
+        f = self.fn("conj_scalar")
+        f.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp,
+                      C.c_uint64, C.c_uint32]
+        f(kind, G, iptr(off), dptr(x) if len(x) else None, dptr(aux) if aux is not None and len(aux) else None,
+          dptr(hs[0]), dptr(hs[1]), dptr(hs[2]), per_group, dptr(ssum), dptr(saux), dptr(out), seed, it)
+        return out, ssum, saux
 
     # ---- LDA ----------------------------------------------------------------
     def lda_disc_z(self, doc_off, w, theta, phi, z, seed, it):

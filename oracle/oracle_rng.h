@@ -68,7 +68,7 @@ enum {
   ORC_TAG_Z = 1, ORC_TAG_THETA = 2, ORC_TAG_PHI = 3, ORC_TAG_MOM = 4,
   ORC_TAG_HMC = 5, ORC_TAG_NUTS = 6, ORC_TAG_PI = 7, ORC_TAG_MU = 8,
   ORC_TAG_COV = 9, ORC_TAG_ESLICE = 10, ORC_TAG_MWG = 11, ORC_TAG_INIT = 12,
-  ORC_TAG_DATA = 13, ORC_TAG_RSLICE = 14
+  ORC_TAG_DATA = 13, ORC_TAG_RSLICE = 14, ORC_TAG_CONJ = 15
 };
 
 #endif

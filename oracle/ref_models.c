@@ -669,3 +669,37 @@ void ref_gmm_mwg(const ref_gmm_t* g, double* mu, const double* cov, const int* z
   }
   free(prop); free(rows_c); free(rows_p);
 }
+
+/* Scalar conjugate updates over G groups through the reference's own
+ * samplers (cbits/augur_dist.c:185-195, 314-336, 408-412); the statistics
+ * loop is what a generated conj_stat would run (sequential over the
+ * observations, CgConj.hs:100-164).  Kind numbering and substreams as
+ * orc_conj_scalar. */
+void ref_conj_scalar(int kind, int G, const int* off, const double* x, const double* aux,
+                     const double* h0, const double* h1, const double* h2, int per_group,
+                     double* stat_sum, double* stat_aux, double* out, uint64_t seed, uint32_t iter) {
+  gsl_rng* rng = ref_rng(seed);
+  for (int g = 0; g < G; ++g) {
+    const int cnt = off[g + 1] - off[g];
+    double sum = 0.0, asum = 0.0;
+    int isum = 0;
+    for (int n = off[g]; n < off[g + 1]; ++n) {
+      if (kind <= 2) isum += (int)x[n];
+      sum += kind == 5 ? 1.0 / x[n] : x[n];
+      if (kind == 4 || kind == 5) asum += aux[n];
+    }
+    if (stat_sum) stat_sum[g] = kind <= 2 ? (double)isum : sum;
+    if (stat_aux) stat_aux[g] = (kind == 4 || kind == 5) ? asum : (double)cnt;
+    const int j = per_group ? g : 0;
+    orc_shim_seek(rng, (uint32_t)g, iter, ORC_TAG_CONJ);
+    switch (kind) {
+      case 0: out[g] = augur_beta_bernoulli_conj(rng, isum, cnt, h0[j], h1[j]); break;
+      case 1: out[g] = augur_beta_geometric_conj(rng, isum, cnt, h0[j], h1[j]); break;
+      case 2: out[g] = augur_gamma_poisson_conj(rng, isum, cnt, h0[j], h1[j]); break;
+      case 3: out[g] = augur_gamma_exponential_conj(rng, sum, cnt, h0[j], h1[j]); break;
+      case 4: out[g] = augur_gamma_gammashape_conj(rng, sum, asum, h0[j], h1[j]); break;
+      case 5: out[g] = augur_gamma_invgamma_conj(rng, sum, asum, h0[j], h1[j]); break;
+      default: out[g] = augur_normal_normalmean_conj(rng, sum, cnt, h0[j], h1[j], h2[j]);
+    }
+  }
+}

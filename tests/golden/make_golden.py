@@ -210,6 +210,51 @@ def make_gmm(ref):
     np.savez_compressed(os.path.join(HERE, "hmvgmm_k4_d5.npz"), **rec)
 
 
+CONJ_KINDS = ["beta_bernoulli", "beta_geometric", "gamma_poisson", "gamma_exponential",
+              "gamma_gammashape", "gamma_invgamma", "normal_normalmean"]
+
+
+def conj_inputs(kind, seed):
+    """Ragged groups (some empty) of observations of the kind's likelihood,
+    and its hyper-parameters (per group for odd kinds, shared otherwise)."""
+    rng = np.random.default_rng(seed)
+    G = 37
+    lens = rng.integers(0, 60, G)
+    lens[[3, 17]] = 0
+    off = np.zeros(G + 1, np.int32)
+    np.cumsum(lens, out=off[1:])
+    n = int(off[-1])
+    x = {"beta_bernoulli": lambda: (rng.random(n) < 0.3).astype(np.float64),
+         "beta_geometric": lambda: rng.geometric(0.4, n).astype(np.float64) - 1.0,
+         "gamma_poisson": lambda: rng.poisson(3.0, n).astype(np.float64),
+         "gamma_exponential": lambda: rng.exponential(0.5, n),
+         "gamma_gammashape": lambda: rng.gamma(2.0, 0.25, n),
+         "gamma_invgamma": lambda: 1.0 / rng.gamma(3.0, 1.0 / 2.0, n),
+         "normal_normalmean": lambda: rng.normal(1.5, 2.0, n)}[kind]()
+    aux = rng.uniform(0.5, 4.0, n) if kind in ("gamma_gammashape", "gamma_invgamma") else None
+    k = CONJ_KINDS.index(kind)
+    if k % 2:
+        h0, h1 = rng.uniform(0.05, 3.0, G), rng.uniform(0.05, 3.0, G)
+        h2 = rng.uniform(0.5, 5.0, G)
+    else:
+        h0, h1, h2 = 0.7, 1.3, 4.0
+    if kind == "normal_normalmean" and np.ndim(h0) == 0:
+        h0 = -0.5
+    return off, x, aux, h0, h1, h2
+
+
+def make_conj(ref):
+    rec = {}
+    for k, kind in enumerate(CONJ_KINDS):
+        off, x, aux, h0, h1, h2 = conj_inputs(kind, 100 + k)
+        for it in (0, 5):
+            out, ssum, saux = ref.conj_scalar(k, off, x, h0, h1, h2, aux=aux, seed=23, it=it)
+            rec["%s_it%d_out" % (kind, it)] = out
+            rec["%s_it%d_sum" % (kind, it)] = ssum
+            rec["%s_it%d_aux" % (kind, it)] = saux
+    np.savez_compressed(os.path.join(HERE, "conj_scalar.npz"), **rec)
+
+
 def make_models():
     """The reference's model files (compiler/augur/test/*.rv) and the model
     strings and schedules of its examples, as parser fixtures."""
@@ -245,4 +290,5 @@ if __name__ == "__main__":
     make_lda(ref)
     make_hlr(ref)
     make_gmm(ref)
+    make_conj(ref)
     print("golden fixtures written to", HERE)

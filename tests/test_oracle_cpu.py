@@ -237,3 +237,36 @@ def test_mvnormal_ll_matches_scipy(orc):
     cov = A @ A.T + 6 * np.eye(6)
     x, mu = rng.standard_normal(6), rng.standard_normal(6)
     assert abs(O.mvnormal_ll(orc, x, mu, cov) - multivariate_normal(mu, cov).logpdf(x)) < 1e-10
+
+
+def _conj_cases():
+    import sys
+    sys.path.insert(0, GOLD)
+    import make_golden as M
+    return M
+
+
+@pytest.mark.parametrize("kind", range(7))
+def test_conj_scalar_golden(orc, kind):
+    """The scalar conjugate restatement against fixtures from the reference's
+    own samplers (augur_dist.c:185-195, 314-336, 408-412), bit for bit."""
+    M = _conj_cases()
+    g = np.load(os.path.join(GOLD, "conj_scalar.npz"))
+    name = M.CONJ_KINDS[kind]
+    off, x, aux, h0, h1, h2 = M.conj_inputs(name, 100 + kind)
+    for it in (0, 5):
+        out, ssum, saux = orc.conj_scalar(kind, off, x, h0, h1, h2, aux=aux, seed=23, it=it)
+        np.testing.assert_array_equal(out, g["%s_it%d_out" % (name, it)])
+        np.testing.assert_array_equal(ssum, g["%s_it%d_sum" % (name, it)])
+        np.testing.assert_array_equal(saux, g["%s_it%d_aux" % (name, it)])
+
+
+@pytest.mark.parametrize("kind", range(7))
+def test_conj_scalar_live(orc, ref, kind):
+    M = _conj_cases()
+    off, x, aux, h0, h1, h2 = M.conj_inputs(M.CONJ_KINDS[kind], 300 + kind)
+    for seed, it in ((1, 0), (99, 12)):
+        a = orc.conj_scalar(kind, off, x, h0, h1, h2, aux=aux, seed=seed, it=it)
+        b = ref.conj_scalar(kind, off, x, h0, h1, h2, aux=aux, seed=seed, it=it)
+        for u, v in zip(a, b):
+            np.testing.assert_array_equal(u, v)
