@@ -280,6 +280,14 @@ class AugurInfer:
         samples = {name: [] for name in self.param_names}
         # a sample after the first step and then after every `thin` steps
         # (augurlib.py:207-221)
+        if not log_like and numSamples > 0 and hasattr(self.backend, "samples"):
+            # the same samples, each copied out while the next steps run
+            for cur in self.backend.samples(numSamples, 1, thin):
+                for name in self.param_names:
+                    samples[name].append(cur[name])
+            if thin > 1:
+                self.backend.step(thin - 1)
+            return samples
         pending = 0
         for i in range(numSamples * thin):
             pending += 1

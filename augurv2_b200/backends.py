@@ -66,6 +66,14 @@ class LdaBackend:
         return {self.info["theta"]: theta, self.info["phi"]: phi,
                 self.info["z"]: [z[off[d]:off[d + 1]] for d in range(len(off) - 1)]}
 
+    def samples(self, n, first, every):
+        """get() after `first` steps and then every `every` steps, n times,
+        with each copy to the host overlapping the next steps."""
+        off = self.doc_off
+        for theta, phi, z in self.s.samples(n, first, every):
+            yield {self.info["theta"]: theta, self.info["phi"]: phi,
+                   self.info["z"]: [z[off[d]:off[d + 1]] for d in range(len(off) - 1)]}
+
     def set_pt(self, pt):
         z = np.concatenate([np.asarray(x, np.int32) for x in pt[self.info["z"]]])
         self.s.set_state(theta=pt[self.info["theta"]], phi=pt[self.info["phi"]], z=z)

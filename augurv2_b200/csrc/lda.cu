@@ -393,10 +393,15 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
   const double m = (6.0 * K + 32.0) * 1.1102230246251565e-16;
   const double lo = 1.0 - m, hi = 1.0 + m;
   const double2* __restrict__ phi2 = reinterpret_cast<const double2*>(phiT);
-  for (int tb = t0 + warp * 32; tb < t1; tb += (LDA_Z_THREADS / 32) * 32) {
+  constexpr int STRIDE = (LDA_Z_THREADS / 32) * 32;
+  // word ids one chunk ahead: the load of the next chunk's ids is in flight
+  // while this chunk computes, instead of preceding the next chunk's copies
+  int w_next = t0 + warp * 32 + lane < t1 ? w[t0 + warp * 32 + lane] : 0;
+  for (int tb = t0 + warp * 32; tb < t1; tb += STRIDE) {
     const int t = tb + lane;
     const bool active = t < t1;
-    const int wt = active ? w[t] : 0;
+    const int wt = w_next;
+    w_next = t + STRIDE < t1 ? w[t + STRIDE] : 0;
     const int nrow = min(32, t1 - tb);
 #pragma unroll
     for (int r = 0; r < 32; ++r) {

@@ -115,6 +115,65 @@ class LdaGibbs(Checkpointable):
         st.synchronize()
         return tuple(h.numpy() for h in out)
 
+    def _sample_layout(self):
+        """Byte offsets of theta, phi [K][V] and z in one packed sample."""
+        def al(x):
+            return (x + 255) & ~255
+        nt, nphi, nz = 8 * self.D * self.K, 8 * self.K * self.V, 4 * self.T
+        return (0, al(nt), al(nt) + al(nphi)), al(nt) + al(nphi) + al(nz)
+
+    def _sample_views(self, buf):
+        (ot, op, oz), _ = self._sample_layout()
+        th = buf[ot:ot + 8 * self.D * self.K].view(torch.float64).view(self.D, self.K)
+        ph = buf[op:op + 8 * self.K * self.V].view(torch.float64).view(self.K, self.V)
+        z = buf[oz:oz + 4 * self.T].view(torch.int32)
+        return th, ph, z
+
+    def samples(self, n, first=1, every=1, stream=None):
+        """Yields n samples (theta, phi, z) as host numpy arrays: the first
+        after `first` sweeps, each further one `every` sweeps later.
+
+        Each sample is packed into one of two alternating device snapshot
+        buffers and copied, as one transfer, into a page-locked host buffer
+        on a second stream, so the copy of sample i overlaps the sweeps that
+        produce sample i + 1; the values are those state() would return at
+        the same points (the three arrays of a sample share one host
+        buffer)."""
+        main = stream if stream is not None else torch.cuda.current_stream(self.dev)
+        _, nbytes = self._sample_layout()
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(self.dev)
+            self._snap = [torch.empty(nbytes, dtype=torch.uint8, device=self.dev) for _ in range(2)]
+        cs = self._copy_stream
+        copied = [None, None]
+        pending = None
+        for i in range(int(n)):
+            self.sweep(first if i == 0 else every, stream=main)
+            b = i & 1
+            if copied[b] is not None:
+                main.wait_event(copied[b])        # the copy out of this buffer is done
+            th, ph, z = self._sample_views(self._snap[b])
+            with torch.cuda.stream(main):
+                th.copy_(self.theta)
+                ph.copy_(self.phiT[:, :self.K].t())
+                z.copy_(self.z)
+                snap = torch.cuda.Event()
+                snap.record(main)
+            cs.wait_event(snap)
+            with torch.cuda.stream(cs):
+                host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+                host.copy_(self._snap[b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+            copied[b] = ev
+            if pending is not None:
+                pending[1].synchronize()
+                yield tuple(t.numpy() for t in self._sample_views(pending[0]))
+            pending = (host, ev)
+        if pending is not None:
+            pending[1].synchronize()
+            yield tuple(t.numpy() for t in self._sample_views(pending[0]))
+
     # ---- sampling ----------------------------------------------------------
     @traced("lda.sweep")
     def sweep(self, n=1, graph=True, stream=None):

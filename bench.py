@@ -690,7 +690,8 @@ def run_e2e(args, off, w, seed, stream):
     """Same metric through the public Python API with host data: the corpus
     is uploaded from host memory inside the timed region, and every step
     copies the sample (theta, phi, z) back to host numpy arrays, as the
-    reference's AugurInfer.samplen does (pyaugur/pyaugur/augurlib.py:195-222)."""
+    reference's AugurInfer.samplen does (pyaugur/pyaugur/augurlib.py:195-222);
+    LdaGibbs.samples overlaps each copy with the next sweep."""
     import torch
     from augurv2_b200.lda import LdaGibbs
     steps = args.steps
@@ -699,9 +700,7 @@ def run_e2e(args, off, w, seed, stream):
     with torch.cuda.stream(stream):
         s = LdaGibbs(K_TOPICS, V_WORDS, off, w, ALPHA, BETA, seed=seed)
         d2h = 0
-        for _ in range(steps):
-            s.sweep(1, stream=stream)
-            th, ph, z = s.state()
+        for th, ph, z in s.samples(steps, stream=stream):
             d2h = th.nbytes + ph.nbytes + z.nbytes
     torch.cuda.synchronize()
     dt = time.perf_counter() - t0
@@ -709,7 +708,7 @@ def run_e2e(args, off, w, seed, stream):
     h2d = off.nbytes + w.nbytes + 8 * (K_TOPICS + V_WORDS)
     return {"value": len(w) * steps / dt, "unit": "tokens/s",
             "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h,
-            "note": "corpus upload + graph capture inside the timed region; sample copied to host every step"}
+            "note": "corpus upload + graph capture inside the timed region; sample copied to host every step (overlapping the next sweep)"}
 
 
 # ------------------------------------------------------- CPU reference ------

@@ -32,6 +32,32 @@ def test_lda_example_runs_and_matches_direct_sampler():
         np.testing.assert_allclose(samples["theta"][it], g["theta"][it], rtol=1e-12)
 
 
+def test_lda_samplen_thinned_pipelined_equals_stepwise():
+    """samplen with thin > 1 through the pipelined LDA sample copies equals
+    the step-by-step loop (taken when log_like is set), samples and final
+    state."""
+    g = np.load(os.path.join(GOLD, "lda_d4_k4_v8.npz"))
+    off, w = g["doc_off"], g["w"]
+    docs = [w[off[d]:off[d + 1]] for d in range(4)]
+    N = np.diff(off).astype(np.int32)
+    rec = MODELS["examples"]["lda"]
+    out = []
+    for log_like in (False, True):
+        with AugurInfer("config.yml", rec["model"]) as infer:
+            infer.set_compile_opt(AugurOpt(cached=False, target="cpu", initStrat=AugurDefault(), seed=3))
+            infer.set_user_sched(rec["scheds"][0])
+            infer.compile(4, 4, N, g["alpha"], g["beta"])(docs)
+            s = infer.samplen(burnIn=2, numSamples=4, thin=3, log_like=log_like)
+            out.append((s, infer.backend.get()))
+    (sa, fa), (sb, fb) = out
+    for name in sa:
+        for x, y in zip(sa[name], sb[name]):
+            np.testing.assert_array_equal(np.concatenate(x) if name == "z" else x,
+                                          np.concatenate(y) if name == "z" else y)
+    np.testing.assert_array_equal(np.concatenate(fa["z"]), np.concatenate(fb["z"]))
+    np.testing.assert_array_equal(fa["theta"], fb["theta"])
+
+
 def test_hlr_example_schedules_run():
     rec = MODELS["examples"]["hlr"]
     X, y, beta, s2 = O.hlr_synthetic(500, 6, 3, has_b=True)

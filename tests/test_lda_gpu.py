@@ -196,6 +196,27 @@ def test_sweep_runner_synthetic_graph_vs_eager(orc):
     a.close(); b.close()
 
 
+def test_pipelined_samples_equal_sweep_and_state():
+    """LdaGibbs.samples (device snapshots copied out on a second stream while
+    the next sweeps run) returns what sweep + state() return at the same
+    points, and leaves the sampler in the same state."""
+    K, V, D = 20, 500, 60
+    off, w = synthetic_corpus(K, V, D, 50, 0.1, 0.01, seed=5)
+    a = LdaGibbs(K, V, off, w, 0.1, 0.01, seed=9)
+    b = LdaGibbs(K, V, off, w, 0.1, 0.01, seed=9)
+    got = list(a.samples(6, first=2, every=3))
+    assert len(got) == 6
+    for i, sa in enumerate(got):
+        b.sweep(2 if i == 0 else 3)
+        for x, y in zip(sa, b.state()):
+            np.testing.assert_array_equal(x, y)
+    a.sweep(1)
+    b.sweep(1)
+    for x, y in zip(a.state(), b.state()):
+        np.testing.assert_array_equal(x, y)
+    a.close(); b.close()
+
+
 def test_full_size_properties():
     """Benchmark shape (K=50, V=1e4, D=2000, ~4e5 tokens): every count table
     sums to the token count, rows of theta/phi are distributions, and the
