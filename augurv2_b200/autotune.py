@@ -24,7 +24,7 @@ DEFAULT_CACHE = os.environ.get(
     "AUGUR_B200_TUNE_CACHE",
     os.path.join(os.path.expanduser("~"), ".cache", "augurv2_b200", "autotune.json"))
 
-FWD_WARPS = (4, 8)
+FWD_WARPS = (4, 8, 16)
 BWD_BN = (32, 64, 128)
 BM, BK = 128, 64
 
@@ -55,7 +55,7 @@ def default_splits(N_, D, C_, bn, sms):
 
 
 def hlrb_candidates(N_, D, C_, sms):
-    """Launch shapes worth timing for one problem: both epilogue widths, the
+    """Launch shapes worth timing for one problem: every epilogue width, the
     backward tile widths that are not mostly padding, and for each the
     built-in split count, half of it and twice it."""
     kb = _ceil(N_, 64) * 64 // BK

@@ -39,7 +39,7 @@ namespace ab {
 namespace {
 
 constexpr int FWD_BN = 128;   // data rows per forward tile
-constexpr int FWD_MAX_GROUPS = 2;   // column groups of the forward epilogue (8 warps)
+constexpr int FWD_MAX_GROUPS = 4;   // column groups of the forward epilogue (16 warps)
 // gradient columns per backward tile by default: the narrowest of 32 / 64 /
 // 128 that covers D (wider D takes several 128-column tiles)
 inline int bwd_bn(int D) { return D <= 32 ? 32 : (D <= 64 ? 64 : 128); }
@@ -60,8 +60,8 @@ struct Layout {
 
 int check_config(const ab_hlrb_config* cfg) {
   if (!cfg) return AB_OK;
-  AB_REQUIRE(cfg->fwd_warps == 0 || cfg->fwd_warps == 4 || cfg->fwd_warps == 8, AB_ERR_ARG,
-             "hlrb: fwd_warps must be 0, 4 or 8 (got %d)", cfg->fwd_warps);
+  AB_REQUIRE(cfg->fwd_warps == 0 || cfg->fwd_warps == 4 || cfg->fwd_warps == 8 || cfg->fwd_warps == 16,
+             AB_ERR_ARG, "hlrb: fwd_warps must be 0, 4, 8 or 16 (got %d)", cfg->fwd_warps);
   AB_REQUIRE(cfg->bwd_bn == 0 || cfg->bwd_bn == 32 || cfg->bwd_bn == 64 || cfg->bwd_bn == 128, AB_ERR_ARG,
              "hlrb: bwd_bn must be 0, 32, 64 or 128 (got %d)", cfg->bwd_bn);
   AB_REQUIRE(cfg->bwd_splits >= 0, AB_ERR_ARG, "hlrb: bwd_splits must be >= 0 (got %d)", cfg->bwd_splits);
@@ -334,8 +334,9 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
   if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
   const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), FWD_BN);
-  rc = L.groups == 1 ? launch_forward<4>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
-                     : launch_forward<8>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st);
+  rc = L.groups == 1   ? launch_forward<4>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
+       : L.groups == 2 ? launch_forward<8>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
+                       : launch_forward<16>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st);
   if (rc) return rc;
 
   if (grad) {

@@ -289,7 +289,7 @@ int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt
  * (augurv2_b200/autotune.py); no reference counterpart (the reference's
  * gradient is a thrust reduction with no tiling, compiler/augur/src/Low/
  * SplitBlk.hs:382-389).  A zero field takes the built-in choice:
- *   fwd_warps   epilogue warps of the forward GEMM: 4 or 8 (default 8)
+ *   fwd_warps   epilogue warps of the forward GEMM: 4, 8 or 16 (default 8)
  *   bwd_bn      gradient columns per backward tile: 32, 64 or 128 (default
  *               the narrowest that covers D)
  *   bwd_splits  row splits of the backward GEMM, >= 1 (default SMs / tiles)
