@@ -25,19 +25,22 @@ DEFAULT_CACHE = os.environ.get(
     os.path.join(os.path.expanduser("~"), ".cache", "augurv2_b200", "autotune.json"))
 
 FWD_WARPS = (4, 8, 16)
+FWD_BN = (128, 256)
 BWD_BN = (32, 64, 128)
 BM, BK = 128, 64
 
 
 class HlrbConfigC(C.Structure):
-    _fields_ = [("fwd_warps", C.c_int), ("bwd_bn", C.c_int), ("bwd_splits", C.c_int)]
+    _fields_ = [("fwd_warps", C.c_int), ("bwd_bn", C.c_int), ("bwd_splits", C.c_int), ("fwd_bn", C.c_int)]
 
     def as_dict(self):
-        return {"fwd_warps": self.fwd_warps, "bwd_bn": self.bwd_bn, "bwd_splits": self.bwd_splits}
+        return {"fwd_warps": self.fwd_warps, "bwd_bn": self.bwd_bn, "bwd_splits": self.bwd_splits,
+                "fwd_bn": self.fwd_bn}
 
     @classmethod
     def of(cls, d):
-        return cls(int(d.get("fwd_warps", 0)), int(d.get("bwd_bn", 0)), int(d.get("bwd_splits", 0)))
+        return cls(int(d.get("fwd_warps", 0)), int(d.get("bwd_bn", 0)), int(d.get("bwd_splits", 0)),
+                   int(d.get("fwd_bn", 0)))
 
 
 def _ceil(a, b):
@@ -55,19 +58,23 @@ def default_splits(N_, D, C_, bn, sms):
 
 
 def hlrb_candidates(N_, D, C_, sms):
-    """Launch shapes worth timing for one problem: every epilogue width, the
+    """Launch shapes worth timing for one problem: every forward tile width
+    and epilogue width (4 epilogue warps only with 128-row tiles), the
     backward tile widths that are not mostly padding, and for each the
     built-in split count, half of it and twice it."""
     kb = _ceil(N_, 64) * 64 // BK
     widest = max(32, _ceil(D, 32) * 32)
     out = []
-    for fw in FWD_WARPS:
-        for bn in BWD_BN:
-            if bn > 2 * widest and bn != 32:
+    for fbn in FWD_BN:
+        for fw in FWD_WARPS:
+            if fw == 4 and fbn == 256:
                 continue
-            sp0 = default_splits(N_, D, C_, bn, sms)
-            for sp in sorted({max(1, sp0 // 2), sp0, min(kb, 2 * sp0)}):
-                out.append({"fwd_warps": fw, "bwd_bn": bn, "bwd_splits": sp})
+            for bn in BWD_BN:
+                if bn > 2 * widest and bn != 32:
+                    continue
+                sp0 = default_splits(N_, D, C_, bn, sms)
+                for sp in sorted({max(1, sp0 // 2), sp0, min(kb, 2 * sp0)}):
+                    out.append({"fwd_warps": fw, "bwd_bn": bn, "bwd_splits": sp, "fwd_bn": fbn})
     return out
 
 

@@ -42,7 +42,7 @@
 namespace ab {
 namespace {
 
-constexpr int FWD_BN = 128;   // data rows per forward tile
+constexpr int FWD_BN_DEFAULT = 256;   // data rows per forward tile (launch shape: 128 or 256)
 constexpr int R_PARTS = 2;          // bf16 parts of the residual
 constexpr int FWD_MAX_GROUPS = 4;   // column groups of the forward epilogue (16 warps)
 // gradient columns per backward tile by default: the narrowest of 32 / 64 /
@@ -55,11 +55,11 @@ inline size_t align256(size_t a) { return (a + 255) & ~size_t(255); }
 // Launch shape of one pass: the built-in choice, or the fields a caller (the
 // autotuner) set in ab_hlrb_config.
 struct Launch {
-  int fwd_warps, bn, splits;
+  int fwd_warps, bn, splits, fwd_bn;
 };
 
 struct Layout {
-  int Np, Dp, fwd_tiles, groups, splits, ldw, bn;
+  int Np, Dp, fwd_tiles, groups, splits, ldw, bn, fwd_bn;
   size_t off_t3, off_r3, off_ll, off_w, total;
 };
 
@@ -70,20 +70,24 @@ int check_config(const ab_hlrb_config* cfg) {
   AB_REQUIRE(cfg->bwd_bn == 0 || cfg->bwd_bn == 32 || cfg->bwd_bn == 64 || cfg->bwd_bn == 128, AB_ERR_ARG,
              "hlrb: bwd_bn must be 0, 32, 64 or 128 (got %d)", cfg->bwd_bn);
   AB_REQUIRE(cfg->bwd_splits >= 0, AB_ERR_ARG, "hlrb: bwd_splits must be >= 0 (got %d)", cfg->bwd_splits);
+  AB_REQUIRE(cfg->fwd_bn == 0 || cfg->fwd_bn == 128 || cfg->fwd_bn == 256, AB_ERR_ARG,
+             "hlrb: fwd_bn must be 0, 128 or 256 (got %d)", cfg->fwd_bn);
   return AB_OK;
 }
 
 Layout layout(int N, int D, int C, const ab_hlrb_config* cfg) {
-  Launch q{8, bwd_bn(D), 0};
+  Launch q{8, bwd_bn(D), 0, FWD_BN_DEFAULT};
   if (cfg) {
     if (cfg->fwd_warps) q.fwd_warps = cfg->fwd_warps;
+    if (cfg->fwd_bn) q.fwd_bn = cfg->fwd_bn;
     if (cfg->bwd_bn) q.bn = cfg->bwd_bn;
     q.splits = cfg->bwd_splits;
   }
   Layout L;
   L.Np = round_up(N, 64);
   L.Dp = round_up(D, 64);
-  L.fwd_tiles = (N + FWD_BN - 1) / FWD_BN;
+  L.fwd_bn = q.fwd_bn;
+  L.fwd_tiles = (N + L.fwd_bn - 1) / L.fwd_bn;
   L.groups = q.fwd_warps / 4;
   L.bn = q.bn;
   const int tiles = ((C + tc::BM - 1) / tc::BM) * ((D + L.bn - 1) / L.bn);
@@ -160,9 +164,9 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
 // Forward epilogue: rows are chains, columns are data rows.  LL: sum the
 // log-likelihood terms; R: write the residual parts for the backward pass
 // (a leapfrog step that only needs the gradient skips the LL work).
-template <bool LL, bool R, int W>
+template <bool LL, bool R, int W, int BN>
 struct FwdEpi {
-  static constexpr int kSmem = FWD_BN * 4;
+  static constexpr int kSmem = BN * 4;
   static constexpr int kWarps = W;
   static constexpr int kGroups = W / 4;
   const int* y;
@@ -176,8 +180,8 @@ struct FwdEpi {
 
   __device__ void begin(int, int nt, int, char* smem, int etid) {
     int* s = reinterpret_cast<int*>(smem);
-    n0 = nt * FWD_BN;
-    for (int j = etid; j < FWD_BN; j += 32 * W) {
+    n0 = nt * BN;
+    for (int j = etid; j < BN; j += 32 * W) {
       const int n = n0 + j;
       s[j] = n < N ? y[n] : -1;
     }
@@ -308,19 +312,28 @@ __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_
 
 }  // namespace
 
-template <int W>
+template <int W, int BN>
 int launch_forward(const ab_hlrb_model* m, const CUtensorMap& ma, const CUtensorMap& mb, const tc::Shape& fs,
                    bool logp, bool grad, __nv_bfloat16* r3, float* llp, int Np, int C, int* err, cudaStream_t st) {
   if (logp && grad) {
-    FwdEpi<true, true, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
-    return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+    FwdEpi<true, true, W, BN> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+    return tc::launch_gemm<BN, 3, 1>(ma, mb, fs, fe, err, st);
   }
   if (logp) {
-    FwdEpi<true, false, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
-    return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+    FwdEpi<true, false, W, BN> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+    return tc::launch_gemm<BN, 3, 1>(ma, mb, fs, fe, err, st);
   }
-  FwdEpi<false, true, W> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
-  return tc::launch_gemm<FWD_BN, 3, 1>(ma, mb, fs, fe, err, st);
+  FwdEpi<false, true, W, BN> fe{m->y, r3, llp, m->N, Np, C, nullptr, 0, 0.0f, 0.0f};
+  return tc::launch_gemm<BN, 3, 1>(ma, mb, fs, fe, err, st);
+}
+
+template <int BN>
+int launch_forward_w(int groups, const ab_hlrb_model* m, const CUtensorMap& ma, const CUtensorMap& mb,
+                     const tc::Shape& fs, bool logp, bool grad, __nv_bfloat16* r3, float* llp, int Np, int C,
+                     int* err, cudaStream_t st) {
+  if (groups == 1) return launch_forward<4, BN>(m, ma, mb, fs, logp, grad, r3, llp, Np, C, err, st);
+  if (groups == 2) return launch_forward<8, BN>(m, ma, mb, fs, logp, grad, r3, llp, Np, C, err, st);
+  return launch_forward<16, BN>(m, ma, mb, fs, logp, grad, r3, llp, Np, C, err, st);
 }
 
 int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad, int ldg,
@@ -339,11 +352,11 @@ int hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, d
   int rc;
   CUtensorMap ma, mb;
   if ((rc = tc::encode_2d_bf16(&ma, t3, C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
-  if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, FWD_BN))) return rc;
-  const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), FWD_BN);
-  rc = L.groups == 1   ? launch_forward<4>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
-       : L.groups == 2 ? launch_forward<8>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
-                       : launch_forward<16>(m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st);
+  if ((rc = tc::encode_2d_bf16(&mb, m->X, N, D, m->ldx, L.fwd_bn))) return rc;
+  const tc::Shape fs = tc::make_shape(C, N, D, 1, tc::row_major(L.Dp), tc::row_major(0), L.fwd_bn);
+  rc = L.fwd_bn == 128
+           ? launch_forward_w<128>(L.groups, m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st)
+           : launch_forward_w<256>(L.groups, m, ma, mb, fs, logp != nullptr, grad != nullptr, r3, llp, L.Np, C, err, st);
   if (rc) return rc;
 
   if (grad) {

@@ -293,10 +293,11 @@ int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt
  *   bwd_bn      gradient columns per backward tile: 32, 64 or 128 (default
  *               the narrowest that covers D)
  *   bwd_splits  row splits of the backward GEMM, >= 1 (default SMs / tiles)
+ *   fwd_bn      data rows per forward tile: 128 or 256 (default 256)
  * Results of different shapes agree to FP32 rounding (the backward partial
  * sums are grouped differently); each shape is deterministic. */
 typedef struct ab_hlrb_config {
-  int fwd_warps, bwd_bn, bwd_splits;
+  int fwd_warps, bwd_bn, bwd_splits, fwd_bn;
 } ab_hlrb_config;
 size_t ab_hlrb_workspace_bytes_cfg(int N, int D, int C, const ab_hlrb_config* cfg);
 int ab_hlrb_logp_grad_cfg(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp, float* grad,

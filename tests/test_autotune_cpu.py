@@ -13,13 +13,14 @@ def test_candidates_are_valid_launch_shapes():
         assert cands, (N, D, C)
         kb = (N + 63) // 64
         for c in cands:
-            assert c["fwd_warps"] in (4, 8, 16)
+            assert c["fwd_warps"] in (4, 8, 16) and c["fwd_bn"] in (128, 256)
+            assert not (c["fwd_warps"] == 4 and c["fwd_bn"] == 256)
             assert c["bwd_bn"] in (32, 64, 128)
             assert 1 <= c["bwd_splits"] <= kb
         # the built-in shape is among them
         bn0 = 32 if D <= 32 else (64 if D <= 64 else 128)
         sp0 = T.default_splits(N, D, C, bn0, 148)
-        assert {"fwd_warps": 8, "bwd_bn": bn0, "bwd_splits": sp0} in cands
+        assert {"fwd_warps": 8, "bwd_bn": bn0, "bwd_splits": sp0, "fwd_bn": 256} in cands
         assert len({json.dumps(c, sort_keys=True) for c in cands}) == len(cands)
 
 
@@ -55,9 +56,12 @@ def test_cache_round_trip_skips_timing(tmp_path):
 
 
 def test_config_struct_round_trip():
-    c = T.HlrbConfigC.of({"fwd_warps": 4, "bwd_bn": 32, "bwd_splits": 7})
-    assert c.as_dict() == {"fwd_warps": 4, "bwd_bn": 32, "bwd_splits": 7}
-    assert T.HlrbConfigC.of({}).as_dict() == {"fwd_warps": 0, "bwd_bn": 0, "bwd_splits": 0}
+    c = T.HlrbConfigC.of({"fwd_warps": 4, "bwd_bn": 32, "bwd_splits": 7, "fwd_bn": 128})
+    assert c.as_dict() == {"fwd_warps": 4, "bwd_bn": 32, "bwd_splits": 7, "fwd_bn": 128}
+    assert T.HlrbConfigC.of({}).as_dict() == {"fwd_warps": 0, "bwd_bn": 0, "bwd_splits": 0, "fwd_bn": 0}
+    # the ctypes layout is the C struct's (four ints, in declaration order)
+    import ctypes
+    assert ctypes.sizeof(T.HlrbConfigC) == 16 and T.HlrbConfigC.fwd_bn.offset == 12
 
 
 def test_lpt_assignment_balances_streams():
