@@ -112,6 +112,7 @@ _SIGS = {
     "ab_sur_post": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
     # tensor-core GEMM core
     "ab_tc_gemm_bf16": (i32, [i32, i32, i32, vp, i32, vp, i32, vp, i32, i32, vp, vp]),
+    "ab_tc_wait_probe": (i32, [C.c_longlong, vp, vp, vp]),
     # scalar conjugate updates
     "ab_conj_scalar": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, u64, u32, vp]),
     # GMM

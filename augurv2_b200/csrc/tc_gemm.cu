@@ -77,6 +77,20 @@ struct StoreEpi {
   __device__ void end(int, int, int, int, bool, int) {}
 };
 
+// Self-test of the bounded wait: one thread waits on an mbarrier that
+// expects an arrival nothing makes, through the same routine the GEMM
+// pipeline uses, and records AB_ERR_TIMEOUT and the cycles it waited.
+__global__ void wait_probe_kernel(long long limit, int* status, long long* cycles) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const long long t0 = clock64();
+  const bool ok = mbar_wait_for(&bar, 0, limit);
+  *cycles = clock64() - t0;
+  *status = ok ? AB_OK : AB_ERR_TIMEOUT;
+}
+
 }  // namespace tc
 }  // namespace ab
 
@@ -102,4 +116,13 @@ extern "C" int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, cons
   else if (BN == 128) rc = launch_gemm<128, 1, 1>(ta, tb, sh, epi, err, st);
   else rc = launch_gemm<64, 1, 1>(ta, tb, sh, epi, err, st);
   return rc;
+}
+
+extern "C" int ab_tc_wait_probe(long long limit_cycles, int* status, long long* cycles, void* stream) {
+  AB_REQUIRE(limit_cycles > 0 && limit_cycles <= ab::tc::WAIT_CYCLES, AB_ERR_ARG,
+             "ab_tc_wait_probe: limit must be in (0, %lld] cycles", (long long)ab::tc::WAIT_CYCLES);
+  AB_REQUIRE(status && cycles, AB_ERR_ARG, "ab_tc_wait_probe: null output");
+  ab::tc::wait_probe_kernel<<<1, 32, 0, ab::as_stream(stream)>>>(limit_cycles, status, cycles);
+  AB_LAUNCH_CHECK("wait_probe_kernel");
+  return AB_OK;
 }

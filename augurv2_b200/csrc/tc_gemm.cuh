@@ -65,8 +65,9 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Bounded wait for the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity; false once `limit`
+// cycles have passed without it.
+__device__ __forceinline__ bool mbar_wait_for(uint64_t* bar, uint32_t parity, long long limit) {
   const uint32_t a = smem_u32(bar);
   const long long t0 = clock64();
   for (;;) {
@@ -79,8 +80,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (clock64() - t0 > WAIT_CYCLES) return false;
+    if (clock64() - t0 > limit) return false;
   }
+}
+
+// The kernels' wait: about two seconds at the SM clock.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  return mbar_wait_for(bar, parity, WAIT_CYCLES);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {

@@ -417,6 +417,13 @@ int ab_sur_post(int C, int D, const float* theta, const float* out, const float*
 int ab_tc_gemm_bf16(int M, int N, int K, const void* A, int lda, const void* B, int ldb, float* C, int ldc,
                     int splits, int* err, void* stream);
 
+/* Self-test of the kernels' bounded waits: one thread waits, through the
+ * routine every tensor-core pipeline wait uses, on an mbarrier that nothing
+ * completes, for at most limit_cycles SM cycles (at most the kernels' own
+ * limit, about 2 s), then writes AB_ERR_TIMEOUT to *status and the cycles
+ * it waited to *cycles (device pointers).  The context stays usable. */
+int ab_tc_wait_probe(long long limit_cycles, int* status, long long* cycles, void* stream);
+
 /* ======================================================================= *
  * Scalar conjugate Gibbs updates: the one-parameter conjugate pairs of the
  * reference library (cbits/augur_dist.c), which its compiler does not emit,
