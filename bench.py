@@ -664,7 +664,7 @@ def run_ours(args, rank, world, local_rank):
             "config": cfg, "tokens_per_step": T,
             "gpu_launches": 4 * args.steps,
             "clocks": clocks.summary(),
-            "roofline": {"bound": "hbm", "kernel": "lda_z_kernel", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "lda_zq_kernel<13> (K=50)", "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": peak_kind, "traffic": Z_KERNEL_DRAM_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
