@@ -422,30 +422,38 @@ __global__ void gmm_conj_pis_kernel(int K, const double* __restrict__ alpha, con
 
 // augur_mvnormal_mvnormal_conj (augur_dist.c:633-669) for component k, one
 // warp, substream (k, iter, 8|comp<<8).
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(64)
 gmm_conj_mu_kernel(int d, int shared_cov, const double* __restrict__ mu0, const double* __restrict__ cov0,
                    const int* __restrict__ cnt, const double* __restrict__ sum, const double* __restrict__ cov,
                    double* __restrict__ mu, uint64_t seed, uint32_t iter, uint32_t comp) {
   extern __shared__ double sm[];
-  const int k = blockIdx.x, lane = threadIdx.x;
+  const int k = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int dd = d * d;
   double* L0 = sm;
   double* L = L0 + dd;
   double* T = L + dd;
-  double* res = T + dd;
+  double* T2 = T + dd;
+  double* res = T2 + dd;
   double* w0 = res + d;
   double* mean = w0 + d;
   double* sk = mean + d;
   double* tmp = sk + d;
   double* mu0s = tmp + d;
   const double* ck = cov + (size_t)(shared_cov ? 0 : k) * dd;
-  for (int e = lane; e < dd; e += 32) { L0[e] = cov0[e]; L[e] = ck[e]; }
-  for (int i = lane; i < d; i += 32) { sk[i] = sum[(size_t)k * d + i]; mu0s[i] = mu0[i]; }
-  __syncwarp();
-  w_chol(L0, d);
-  w_cholinv(L0, T, d);
-  w_chol(L, d);
-  w_cholinv(L, T, d);
+  for (int e = threadIdx.x; e < dd; e += blockDim.x) { L0[e] = cov0[e]; L[e] = ck[e]; }
+  for (int i = threadIdx.x; i < d; i += blockDim.x) { sk[i] = sum[(size_t)k * d + i]; mu0s[i] = mu0[i]; }
+  __syncthreads();
+  // the two inverses are independent: one warp each (each the reference's
+  // sequential routine, so the values are unchanged), then warp 0 alone
+  if (warp == 0) {
+    w_chol(L0, d);
+    w_cholinv(L0, T, d);
+  } else {
+    w_chol(L, d);
+    w_cholinv(L, T2, d);
+  }
+  __syncthreads();
+  if (warp != 0) return;
   const int n = cnt[k];
   for (int e = lane; e < dd; e += 32) L[e] = __dmul_rn((double)n, L[e]);           // augur_mat_ms
   __syncwarp();
@@ -746,9 +754,9 @@ int launch_gmm_stats(int N, int d, int K, const float* Y, const int* z, const do
 int launch_gmm_conj_mu(int K, int d, int shared, const double* mu0, const double* cov0, const int* cnt,
                        const double* sum, const double* cov, double* mu, uint64_t seed, uint32_t iter,
                        uint32_t comp, cudaStream_t st) {
-  const size_t smem = sizeof(double) * (3 * (size_t)d * d + 6 * (size_t)d);
+  const size_t smem = sizeof(double) * (4 * (size_t)d * d + 6 * (size_t)d);
   AB_CUDA(cudaFuncSetAttribute(gmm_conj_mu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  gmm_conj_mu_kernel<<<K, 32, smem, st>>>(d, shared, mu0, cov0, cnt, sum, cov, mu, seed, iter, comp);
+  gmm_conj_mu_kernel<<<K, 64, smem, st>>>(d, shared, mu0, cov0, cnt, sum, cov, mu, seed, iter, comp);
   AB_LAUNCH_CHECK("gmm_conj_mu_kernel");
   return AB_OK;
 }

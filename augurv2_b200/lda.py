@@ -69,9 +69,13 @@ class LdaGibbs(Checkpointable):
         self.cnt_dk = torch.zeros((self.D, self.K), dtype=torch.int32, device=self.dev)
         self.cnt_kw = torch.zeros((self.K, self.V), dtype=torch.int32, device=self.dev)
         self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V)), dtype=torch.uint8, device=self.dev)
-        self.set_state(theta=theta if theta is not None else np.full((self.D, self.K), 1.0 / self.K),
-                       phi=phi if phi is not None else np.full((self.K, self.V), 1.0 / self.V),
-                       z=z if z is not None else np.zeros(self.T, np.int32), iteration=iter0)
+        # defaults (uniform theta and phi, z = 0) are filled on the device;
+        # given values are uploaded
+        if theta is None:
+            self.theta.fill_(1.0 / self.K)
+        if phi is None:
+            self.phiT[:, :self.K].fill_(1.0 / self.V)
+        self.set_state(theta=theta, phi=phi, z=z, iteration=iter0)
         desc = N.LdaDesc(self.D, self.K, self.V, self.doc_off.data_ptr(), self.w.data_ptr(),
                          self.alpha.data_ptr(), self.beta.data_ptr(), self.z.data_ptr(),
                          self.theta.data_ptr(), self.phiT.data_ptr(), self.cnt_dk.data_ptr(),
@@ -87,8 +91,8 @@ class LdaGibbs(Checkpointable):
         if theta is not None:
             self.theta.copy_(torch.as_tensor(np.asarray(theta, np.float64).reshape(self.D, self.K)))
         if phi is not None:
-            ph = torch.as_tensor(np.asarray(phi, np.float64).reshape(self.K, self.V))
-            self.phiT[:, :self.K].copy_(ph.t())
+            ph = torch.as_tensor(np.asarray(phi, np.float64).reshape(self.K, self.V)).to(self.dev)
+            self.phiT[:, :self.K].copy_(ph.t())      # transposed on the device
         if z is not None:
             self.z.copy_(torch.as_tensor(np.asarray(z, np.int32).ravel()))
         if iteration is not None:
