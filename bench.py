@@ -44,7 +44,7 @@ sys.path.insert(0, ROOT)
 K_TOPICS, V_WORDS, D_DOCS, MEAN_LEN, ALPHA, BETA, DATA_SEED = 50, 10000, 2000, 200, 0.1, 0.01, 0
 # DRAM bytes of one z-kernel launch on this workload, from the ncu capture summarised in
 # profiles/lda_zq_kernel_k50_v10000_d2000.md (phi and the count tables stay in L2)
-Z_KERNEL_DRAM_BYTES = 6_703_104
+Z_KERNEL_DRAM_BYTES = 6_699_264
 L2_FLUSH_BYTES = 512 << 20
 
 
