@@ -59,7 +59,35 @@ class LdaDesc(C.Structure):
     _fields_ = [("D", i32), ("K", i32), ("V", i32),
                 ("doc_off", vp), ("w", vp), ("alpha", vp), ("beta", vp),
                 ("z", vp), ("theta", vp), ("phiT", vp), ("cnt_dk", vp), ("cnt_kw", vp),
-                ("scratch", vp), ("seed", u64)]
+                ("scratch", vp), ("seed", u64), ("T", i32)]
+
+
+_dp, _ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+
+
+class HlrCompC(C.Structure):
+    _fields_ = [("kind", i32), ("P", i32), ("idx_off", i32), ("max_depth", i32), ("simlen", f64), ("eps", f64),
+                ("mwg_var", f64)]
+
+
+class LdaInit(C.Structure):
+    """ab_lda_init: host arrays of an LDA model for ab_init_lda."""
+    _fields_ = [("D", i32), ("K", i32), ("V", i32), ("doc_off", _ip), ("w", _ip), ("alpha", _dp), ("beta", _dp),
+                ("theta", _dp), ("phi", _dp), ("z", _ip), ("seed", u64), ("iter0", u32)]
+
+
+class HlrInit(C.Structure):
+    """ab_hlr_init: host arrays of an HLR model and schedule for ab_init_hlr."""
+    _fields_ = [("N", i32), ("D", i32), ("has_b", i32), ("vprior", i32), ("compat", i32), ("lam", f64),
+                ("a0", f64), ("s0", f64), ("X", _dp), ("y", _ip), ("C", i32), ("pars", _dp), ("n_comps", i32),
+                ("comps", C.POINTER(HlrCompC)), ("idx", _ip), ("n_idx", i32), ("seed", u64), ("iter0", u32)]
+
+
+class GmmInit(C.Structure):
+    """ab_gmm_init: host arrays of a Gaussian-mixture model for ab_init_gmm."""
+    _fields_ = [("N", i32), ("d", i32), ("K", i32), ("shared_cov", i32), ("move", i32), ("compat", i32),
+                ("Y", _dp), ("mu0", _dp), ("cov0", _dp), ("pis", _dp), ("covs", _dp), ("alpha", _dp), ("df", i32),
+                ("scale0", _dp), ("prop_cov", _dp), ("mu", _dp), ("z", _ip), ("seed", u64), ("iter0", u32)]
 
 
 _SIGS = {
@@ -73,7 +101,7 @@ _SIGS = {
     "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp, vp]),
     "ab_lda_conj_phi_noalloc": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp]),
     "ab_lda_disc_z": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
-    "ab_lda_scratch_bytes": (sz, [i32, i32]),
+    "ab_lda_scratch_bytes": (sz, [i32, i32, i32]),
     "ab_lda_create": (i32, [C.POINTER(LdaDesc), C.POINTER(vp)]),
     "ab_lda_init_state": (i32, [vp, u32, vp]),
     "ab_lda_run": (i32, [vp, i32, i32, vp]),
@@ -126,6 +154,31 @@ _SIGS = {
     "ab_gmm_conj_cov": (i32, [i32, i32, i32, vp, vp, vp, vp, u64, u32, u32, vp]),
     "ab_gmm_eslice": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, u64, u32, u32, vp, vp]),
     "ab_gmm_mwg": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, i32, i32, vp, u64, u32, u32, vp, vp]),
+    # whole-model log densities, predictive log-likelihoods, dethlr's bias
+    "ab_ll_scratch_bytes": (sz, []),
+    "ab_lda_ll_mod": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "ab_lda_pred_ll": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp]),
+    "ab_gmm_ll_mod": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp,
+                            vp]),
+    "ab_gmm_pred_ll": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "ab_hlr_det": (i32, [vp, i32, vp, vp, vp]),
+    # model handles
+    "ab_init_lda": (i32, [C.POINTER(LdaInit), C.POINTER(vp)]),
+    "ab_init_hlr": (i32, [C.POINTER(HlrInit), C.POINTER(vp)]),
+    "ab_init_gmm": (i32, [C.POINTER(GmmInit), C.POINTER(vp)]),
+    "ab_model_kind": (i32, [vp]),
+    "ab_model_last_error": (C.c_char_p, [vp]),
+    "ab_step": (i32, [vp, i32, vp]),
+    "ab_iteration": (u32, [vp]),
+    "ab_state_bytes": (sz, [vp]),
+    "ab_get_state": (i32, [vp, vp, sz, vp]),
+    "ab_set_state": (i32, [vp, vp, sz, vp]),
+    "ab_checkpoint_bytes": (sz, [vp]),
+    "ab_checkpoint": (i32, [vp, vp, sz, vp]),
+    "ab_restore": (i32, [vp, vp, sz, vp]),
+    "ab_curr_ll_count": (i32, [vp]),
+    "ab_curr_ll": (i32, [vp, _dp, i32, vp]),
+    "ab_destroy": (i32, [vp]),
 }
 
 

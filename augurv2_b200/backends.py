@@ -85,13 +85,10 @@ class LdaBackend:
         self.s.load_state_dict(d)
 
     def curr_ll(self):
-        """Joint log density in the reference's terms (augur_dirichlet_ll has
-        no normalising constant, cbits/augur_dist.c:489-497)."""
-        theta, phi, z = self.s.state()
-        doc = np.repeat(np.arange(len(self.doc_off) - 1), np.diff(self.doc_off))
-        ll = ((self.alpha - 1.0) * np.log(theta)).sum() + ((self.beta - 1.0) * np.log(phi)).sum()
-        ll += np.log(theta[doc, z]).sum() + np.log(phi[z, self.w]).sum()
-        return float(ll)
+        """Joint log density in the reference's terms (augur_get_curr_ll,
+        CgStInit.hs:597-602; augur_dirichlet_ll has no normalising constant,
+        cbits/augur_dist.c:488-496), on the device."""
+        return self.s.ll_mod()
 
 
 # ---------------------------------------------------------------------------
@@ -172,8 +169,7 @@ class HlrBackend:
         if self.has_b:
             out[self.info["b"]] = pick(s[:, D].copy())
         if self.info["det"]:
-            t = s[:, :D] @ self.X.T + (s[:, D:D + 1] if self.has_b else 0.0)
-            out[self.info["det"]] = pick(1.0 / (1.0 + np.exp(-t)))
+            out[self.info["det"]] = pick(self.chains.det_bias().cpu().numpy())
         if self.C == 1:
             for k in (self.info["v"], self.info["b"]):
                 if k in out:
@@ -291,19 +287,9 @@ class GmmBackend:
         self.s.load_state_dict(d)
 
     def curr_ll(self):
-        from scipy.stats import multivariate_normal as mvn
-        st = self.s.state()
-        mu, z, pis = st["mu"], st["z"], st["pis"]
-        mu0 = self.s.mu0.cpu().numpy()
-        cov0 = self.s.cov0.cpu().numpy()
-        ll = sum(mvn(mu0, cov0).logpdf(m) for m in mu)
-        ll += np.log(pis[z]).sum()
-        covs = st["cov"] if self.family == "hmvgmm" else [self.s.cov.cpu().numpy()[0]] * self.K
-        for k in range(self.K):
-            m = z == k
-            if m.any():
-                ll += mvn(mu[k], covs[k]).logpdf(self.Y[m]).sum()
-        return float(ll)
+        """Joint log density in the reference's terms (augur_get_curr_ll,
+        CgStInit.hs:597-602), on the device."""
+        return self.s.ll_mod()
 
 
 def make(family, info, parsed, sched, hyp, data, opt):

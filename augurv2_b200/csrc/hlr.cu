@@ -419,12 +419,15 @@ __device__ int hmc_transition(const HlrModelDev& m, const HlrComp& cp, const int
   const double k0 = seq_dot(ws.p0, ws.p0, P, ws);
   const double k1 = seq_dot(ws.ps, ws.ps, P, ws);
   const double auxll = k0 / 2.0 - k1 / 2.0;
-  const int acc = log(u) < ll_prop - ll_curr + auxll;
+  const double dlog = ll_prop - ll_curr + auxll;   // minus the energy error
+  const int acc = log(u) < dlog;
+  // divergent: the energy error passed the bound, or is not finite
+  const int div = !(dlog > -AB_DIVERGENCE_DH);
   if (acc)
     for (int i = tid; i < m.D + 2; i += blockDim.x) ws.par[i] = ws.prop[i];
   __syncthreads();
   (void)cache_ll; (void)cache_ok;
-  return acc;
+  return acc | (div << 1);
 }
 
 // ---- NUTS: cbits/augur_mcmclib.h:575-776 (iterative restatement) ------------
@@ -448,7 +451,7 @@ __device__ int nuts_update_s(int s, const double* tp, const double* mp, const do
 
 __device__ int nuts_transition(const HlrModelDev& m, const HlrComp& cp, const int* idx, Ws& ws,
                                double* stk, uint64_t seed, uint32_t iter, uint32_t chain, uint32_t ci,
-                               int* depth_out, int* leaves_out, int* error_out) {
+                               int* depth_out, int* leaves_out, int* error_out, int* div_out) {
   const int P = cp.P;
   const int tid = threadIdx.x;
   double* tp_stk = stk;                          // theta_prop stack
@@ -483,6 +486,7 @@ __device__ int nuts_transition(const HlrModelDev& m, const HlrComp& cp, const in
     ws.ibcast[2] = -1; ws.ibcast[3] = -1; ws.ibcast[4] = -1;  // tp, ts, ms stack heads
     ws.ibcast[5] = 0;  // leaves
     ws.ibcast[6] = 0;  // overflow flag
+    ws.ibcast[7] = 0;  // divergence flag
   }
   __syncthreads();
   const double logu = ws.bcast[5];
@@ -556,6 +560,9 @@ __device__ int nuts_transition(const HlrModelDev& m, const HlrComp& cp, const in
         const double ll = llp - 0.5 * seq_dot(mom, mom, P, ws);
         rn = logu <= ll ? 1 : 0;
         rs = logu < 1000.0 + ll ? 1 : 0;
+        // a leaf outside the slice by the reference's deltaMax (1000) ends
+        // the tree: the iteration counts as divergent
+        if (tid == 0 && !rs) ws.ibcast[7] = 1;
         --sp;
         continue;
       }
@@ -625,6 +632,7 @@ __device__ int nuts_transition(const HlrModelDev& m, const HlrComp& cp, const in
     *depth_out = jd;
     *leaves_out = ws.ibcast[5];
     *error_out = ws.ibcast[6];
+    *div_out = ws.ibcast[7];
   }
   __syncthreads();
   return 0;
@@ -731,7 +739,7 @@ size_t hlr_smem_bytes(int D) {
 }
 
 // One CTA per chain: n_iter iterations of the schedule `comps`.
-// stats[c][ci][4] = {accepts, sum depth, sum leaves, errors}.
+// stats[c][ci][5] = {accepts, sum depth, sum leaves, errors, divergent iterations}.
 __global__ void __launch_bounds__(HLR_THREADS)
 hlr_chain_kernel(HlrModelDev m, const HlrComp* __restrict__ comps, int n_comps,
                  const int* __restrict__ idx_all, double* __restrict__ pars, int n_iter,
@@ -748,17 +756,15 @@ hlr_chain_kernel(HlrModelDev m, const HlrComp* __restrict__ comps, int n_comps,
     for (int ci = 0; ci < n_comps; ++ci) {
       const HlrComp cp = comps[ci];
       const int* idx = idx_all + cp.idx_off;
-      double* st = stats + ((size_t)c * n_comps + ci) * 4;
+      double* st = stats + ((size_t)c * n_comps + ci) * AB_HLR_STATS;
       if (cp.kind == COMP_HMC) {
         const int a = hmc_transition(m, cp, idx, ws, seed, iter, (uint32_t)c, (uint32_t)ci, nullptr, nullptr);
-        if (threadIdx.x == 0) st[0] += a;
+        if (threadIdx.x == 0) { st[0] += a & 1; st[4] += a >> 1; }
       } else if (cp.kind == COMP_NUTS) {
-        int depth = 0, leaves = 0, err = 0;
-        __shared__ int sh_out[3];
+        __shared__ int sh_out[4];
         nuts_transition(m, cp, idx, ws, nuts_stk + (size_t)c * 3 * HLR_STK * stk_P, seed, iter,
-                        (uint32_t)c, (uint32_t)ci, &sh_out[0], &sh_out[1], &sh_out[2]);
-        depth = sh_out[0]; leaves = sh_out[1]; err = sh_out[2];
-        if (threadIdx.x == 0) { st[1] += depth; st[2] += leaves; st[3] += err; }
+                        (uint32_t)c, (uint32_t)ci, &sh_out[0], &sh_out[1], &sh_out[2], &sh_out[3]);
+        if (threadIdx.x == 0) { st[1] += sh_out[0]; st[2] += sh_out[1]; st[3] += sh_out[2]; st[4] += sh_out[3]; }
       } else if (cp.kind == COMP_RSLICE) {
         int refl = 0;
         const int a = rslice_transition(m, cp, idx, ws, seed, iter, (uint32_t)c, (uint32_t)ci, &refl);

@@ -94,8 +94,11 @@ __global__ void __launch_bounds__(256) hmcb_final_kernel(ab_hmcb_state s, const 
     const double dH = s.H0[c] - H1;
     const bool ok = isfinite(H1) && log(u) < dH;
     acc_sh = ok;
-    s.stats[2 * c] += ok ? 1.0 : 0.0;
-    s.stats[2 * c + 1] += isfinite(dH) ? (dH >= 0.0 ? 1.0 : exp(dH)) : 0.0;
+    double* st = s.stats + (size_t)AB_HMCB_STATS * c;
+    st[0] += ok ? 1.0 : 0.0;
+    st[1] += isfinite(dH) ? (dH >= 0.0 ? 1.0 : exp(dH)) : 0.0;
+    // energy error above the divergence bound, or not finite
+    st[2] += (dH > -AB_DIVERGENCE_DH) ? 0.0 : 1.0;
     s.logp_cur[c] = ok ? logp_new[c] : s.logp0[c];
   }
   __syncthreads();

@@ -46,29 +46,77 @@ __device__ __forceinline__ uint32_t read_iter(const uint32_t* iter_dev, uint32_t
 }
 
 // ---------------------------------------------------------------------------
+// Gamma draws of one CTA with the rejection loops compacted: every thread
+// makes its cell's first Marsaglia-Tsang try (gamma_first_try, which decides
+// about 95% of draws by the squeeze); the cells it does not decide are queued
+// in shared memory and drawn afterwards by the first threads of the CTA, one
+// cell each, with the full sampler from the start of the cell's substream.
+// The draws are those of gamma_draw(make_stream(seed, elem, iter, tag),
+// shape, 1) for every cell; only the work is regrouped, so that a warp no
+// longer runs as many loop iterations as its slowest lane needs.
+// q, qshape, qelem, qout (blockDim.x entries each) and qn are shared memory;
+// the return value is the draw of the thread's own cell (when has_cell).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double gamma_draw_compacted(bool has_cell, double shape, uint32_t elem,
+                                                       uint64_t seed, uint32_t iter, uint32_t tag,
+                                                       int* q, double* qshape, uint32_t* qelem,
+                                                       double* qout, int* qn) {
+  if (threadIdx.x == 0) *qn = 0;
+  __syncthreads();
+  double g = 0.0;
+  bool queued = false;
+  if (has_cell) {
+    Stream s = make_stream(seed, elem, iter, tag);
+    if (!gamma_first_try(s, shape, 1.0, g)) {
+      const int slot = atomicAdd(qn, 1);
+      q[slot] = threadIdx.x;
+      qshape[slot] = shape;
+      qelem[slot] = elem;
+      queued = true;
+    }
+  }
+  __syncthreads();
+  const int n = *qn;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    Stream s = make_stream(seed, qelem[i], iter, tag);
+    qout[q[i]] = gamma_draw(s, qshape[i], 1.0);
+  }
+  __syncthreads();
+  if (queued) g = qout[threadIdx.x];
+  return g;
+}
+
+// ---------------------------------------------------------------------------
 // theta[d][k] = g[d][k] / sum_k g[d][k],  g ~ Gamma(alpha_k + cnt[d][k], 1)
 // (augur_dirichlet_categorical_conj, cbits/augur_dist.c:526-538).  The row
 // sum is taken sequentially over k by one thread, as the reference does, so
 // theta is bit-identical to the reference given identical gamma draws.
-// Block: R = 256 / K rows (or one row looped when K > 256).
+// Block: R = 256 / K rows of K cells, one cell per thread (K <= 256), or one
+// row looped over when K > 256.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(LDA_THREADS, 5)
+__global__ void __launch_bounds__(LDA_THREADS, 4)
 lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
                  const int* __restrict__ cnt_dk, double* __restrict__ theta,
                  uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
   extern __shared__ double sg[];  // [rows_per_block][K] gamma draws, then [rows] sums
+  __shared__ int q[LDA_THREADS];
+  __shared__ double qshape[LDA_THREADS], qout[LDA_THREADS];
+  __shared__ uint32_t qelem[LDA_THREADS];
+  __shared__ int qn;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
   const int rows = K <= LDA_THREADS ? LDA_THREADS / K : 1;
   const int row0 = blockIdx.x * rows;
   double* sums = sg + rows * K;
-  for (int e = threadIdx.x; e < rows * K; e += blockDim.x) {
+  for (int e0 = 0; e0 < rows * K; e0 += blockDim.x) {     // one pass when K <= 256
+    const int e = e0 + threadIdx.x;
     const int r = e / K, k = e - r * K;
     const int d = row0 + r;
-    if (d < D) {
-      const size_t idx = (size_t)d * K + k;
-      Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_THETA);
-      sg[e] = gamma_draw(s, __dadd_rn(alpha[k], (double)cnt_dk[idx]), 1.0);
-    }
+    const bool has = e < rows * K && d < D;
+    const size_t idx = (size_t)d * K + k;
+    const double shape = has ? __dadd_rn(alpha[k], (double)cnt_dk[idx]) : 1.0;
+    const double g = gamma_draw_compacted(has, shape, (uint32_t)idx, seed, iter, TAG_THETA, q, qshape, qelem,
+                                          qout, &qn);
+    if (has) sg[e] = g;
   }
   __syncthreads();
   if (threadIdx.x < rows && row0 + (int)threadIdx.x < D) {
@@ -98,26 +146,32 @@ lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
 // The sum is deterministic but not in the reference's sequential order, so
 // phi matches the reference to rounding, not bitwise.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(LDA_THREADS, 5)
+__global__ void __launch_bounds__(LDA_THREADS, 4)
 lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta,
                     int* __restrict__ cnt_kw, double* __restrict__ phiT, int clear_counts,
                     double* __restrict__ partial, uint32_t* __restrict__ ticket,
                     double* __restrict__ nrm, uint64_t seed, const uint32_t* iter_dev,
                     uint32_t iter_fixed) {
   __shared__ double red[33];
+  __shared__ int q[LDA_THREADS];
+  __shared__ double qshape[LDA_THREADS], qout[LDA_THREADS];
+  __shared__ uint32_t qelem[LDA_THREADS];
+  __shared__ int qn;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
   const int k = blockIdx.x / B;
   const int b = blockIdx.x - k * B;
   const int v = b * LDA_THREADS + threadIdx.x;
-  double g = 0.0;
-  if (v < V) {
-    const size_t idx = (size_t)k * V + v;
+  const bool has = v < V;
+  const size_t idx = (size_t)k * V + v;
+  double shape = 1.0;
+  if (has) {
     const int c = cnt_kw[idx];
     if (clear_counts) cnt_kw[idx] = 0;
-    Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
-    g = gamma_draw(s, __dadd_rn(beta[v], (double)c), 1.0);
-    phiT[(size_t)v * Kp + k] = g;
+    shape = __dadd_rn(beta[v], (double)c);
   }
+  const double g = gamma_draw_compacted(has, shape, (uint32_t)idx, seed, iter, TAG_PHI, q, qshape, qelem,
+                                        qout, &qn);
+  if (has) phiT[(size_t)v * Kp + k] = g;
   const double bsum = block_sum_f64(g, red);
   // The last CTA of topic k (atomic ticket) adds the topic's B partials in
   // CTA order and publishes the normaliser.
@@ -344,50 +398,58 @@ __device__ __noinline__ int lda_reference_draw(int K, const double* __restrict__
 // ---------------------------------------------------------------------------
 // z[t] for every token of document d, K <= 64 (one CTA of 128 threads per
 // document; NQ = Kp / 4 quads of topics, a compile-time constant).
-// Each warp takes LDA_ZQ_ROWS (16) consecutive tokens, one per lane.  The
-// warp copies their phi rows into shared memory with asynchronous 16-byte
-// copies, one row per copy instruction (a row is one contiguous segment, and
-// all the chunk's rows are in flight at once); the row pitch is an odd number of 16-byte units so
-// that the per-lane row reads that follow are bank-conflict free.  Each lane
-// then makes one pass over its row: p_k = theta_k * phi_k and the
-// sequential running sum c_k = c_{k-1} + p_k, written back over the row, so
-// c_{K-1} is the reference's norm bit for bit.  The draw is the first
-// k <= K - 2 with u < acc_k (acc_k the reference's running sum of p_j / norm);
-// it is found without divisions by a binary search over the nondecreasing
-// c_k for the first k with u norm <= c_k (1 + m), and is decided when also
-// u norm < c_k (1 - m).  m = (6K + 32) 2^-53 bounds the rounding of the
-// products, sums and quotients on both sides, so a decided draw equals the
+// Each warp takes LDA_ZQ_ROWS (16) consecutive tokens, two lanes per token:
+// lane j and lane j + 16 share token j, the first lane holding topics
+// [0, 2 NQ) of its row and the second topics [2 NQ, 4 NQ).  The warp copies
+// the chunk's phi rows into shared memory with asynchronous 16-byte copies,
+// one row per copy instruction (a row is one contiguous segment, and all the
+// chunk's rows are in flight at once); the row pitch is an odd number of
+// 16-byte units so that the per-lane row reads that follow are bank-conflict
+// free.  Each lane then makes one pass over its half row: p_k = theta_k *
+// phi_k and the running sum of its half, written back over the row.  With A
+// the first half's total, the running sum of the products is c_k for the
+// first half and c_k = A + s_k for the second (s_k the second half's own
+// running sum); norm = A + S (S the second half's total).  This groups the
+// additions differently from the reference's sequential sum, by at most one
+// rounding per term, which the margin below covers.
+// The draw is the first k <= K - 2 with u < acc_k (acc_k the reference's
+// running sum of p_j / norm); it is found without divisions by a binary
+// search over the nondecreasing c_k (each lane in its half) for the first k
+// with u norm <= c_k (1 + m), and is decided when also u norm < c_k (1 - m).
+// m = (6K + 32) 2^-53 bounds the rounding of the products, sums (in either
+// grouping) and quotients on both sides, so a decided draw equals the
 // reference's; a u within m of a boundary (or a zero, subnormal, infinite or
-// NaN norm) runs the reference's loop itself (lda_reference_draw).  theta and
-// phi are probabilities (nonnegative), which keeps c_k monotone.
+// NaN norm) runs the reference's loop itself (lda_reference_draw).  theta
+// and phi are probabilities (nonnegative), which keeps c_k monotone.
+// The token's uniform is read from u_pre (drawn ahead by lda_zu_kernel) when
+// given, else drawn here from the token's substream.
 // Counts of the new z: the document's row of cnt_dk is accumulated in shared
-// memory and stored whole; cnt_kw receives one atomic increment per token.
+// memory and stored whole; cnt_kw, when given, receives one atomic increment
+// per token.
 // ---------------------------------------------------------------------------
 constexpr int LDA_ZQ_MAX_K = 64;
 
-// Tokens per warp chunk: the 16 phi rows a warp stages at a time.  Lanes
-// 16..31 help copy rows but sit out the per-token work; in exchange a CTA
-// needs a third of the shared memory and 64 registers per thread, so 7 to 8
-// CTAs fit an SM instead of 4 and more rows are in flight (measured: z
-// 39.1 -> 34.9 us, sweep 88.1 -> 83.9 us at K=50; 24 and 20 rows per chunk
-// were in between or no faster).
+// Tokens per warp chunk: the 16 phi rows a warp stages at a time, two lanes
+// per token.
 constexpr int LDA_ZQ_ROWS = 16;
 
 template <int NQ>
 __global__ void __launch_bounds__(LDA_Z_THREADS, 8)
 lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
               const int* __restrict__ w, const double* __restrict__ theta,
-              const double* __restrict__ phiT, int* __restrict__ z,
-              int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
+              const double* __restrict__ phiT, const double* __restrict__ u_pre,
+              int* __restrict__ z, int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
               uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
   constexpr int KP = 4 * NQ;          // row length in doubles (= the phiT stride)
   constexpr int H2 = 2 * NQ;          // row length in 16-byte units
+  constexpr int HK = 2 * NQ;          // topics per half row
   constexpr int P2 = H2 + 1;          // row pitch in 16-byte units (odd)
-  constexpr int STEP0 = KP > 32 ? 32 : (KP > 16 ? 16 : (KP > 8 ? 8 : (KP > 4 ? 4 : 2)));
+  constexpr int STEP0 = HK > 16 ? 16 : (HK > 8 ? 8 : (HK > 4 ? 4 : (HK > 2 ? 2 : 1)));
   extern __shared__ double2 smem2[];
   double2* th2 = smem2;                                        // [H2] theta, zero padded
   int* hist = reinterpret_cast<int*>(smem2 + H2);              // [KP]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = lane & 15, half = lane >> 4;
   double2* stage = smem2 + H2 + NQ + warp * LDA_ZQ_ROWS * P2;  // [LDA_ZQ_ROWS][P2] this warp's rows
   const int d = blockIdx.x;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
@@ -401,15 +463,17 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
   const double m = (6.0 * K + 32.0) * 1.1102230246251565e-16;
   const double lo = 1.0 - m, hi = 1.0 + m;
   const double2* __restrict__ phi2 = reinterpret_cast<const double2*>(phiT);
+  // topics of this lane's half that can be a draw's answer (k <= K - 2)
+  const int n_half = min(max(K - 1 - half * HK, 0), HK);
   constexpr int STRIDE = (LDA_Z_THREADS / 32) * LDA_ZQ_ROWS;
   // word ids one chunk ahead: the load of the next chunk's ids is in flight
   // while this chunk computes, instead of preceding the next chunk's copies
   int w_next = (lane < LDA_ZQ_ROWS && t0 + warp * LDA_ZQ_ROWS + lane < t1) ? w[t0 + warp * LDA_ZQ_ROWS + lane] : 0;
   for (int tb = t0 + warp * LDA_ZQ_ROWS; tb < t1; tb += STRIDE) {
-    const int t = tb + lane;
-    const bool active = lane < LDA_ZQ_ROWS && t < t1;
+    const int t = tb + j;
+    const bool active = t < t1;
     const int wt = w_next;
-    w_next = (lane < LDA_ZQ_ROWS && t + STRIDE < t1) ? w[t + STRIDE] : 0;
+    w_next = (lane < LDA_ZQ_ROWS && tb + lane + STRIDE < t1) ? w[tb + lane + STRIDE] : 0;
     const int nrow = min(LDA_ZQ_ROWS, t1 - tb);
 #pragma unroll
     for (int r = 0; r < LDA_ZQ_ROWS; ++r) {
@@ -421,47 +485,62 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
-    int zk = 0;
     double u = 0.0;
-    if (active) {
-      Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
-      u = s.uniform();
+    if (u_pre != nullptr) {
+      if (active) u = u_pre[t];
+    } else {
+      if (active && half == 0) {
+        Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+        u = s.uniform();
+      }
+      u = __shfl_sync(0xffffffffu, u, j);
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
+    // running sum of this lane's half row, written back over it
+    double2* row = stage + j * P2 + half * NQ;
+    const double2* thh = th2 + half * NQ;
+    double c = 0.0;
     if (active) {
-      double2* row = stage + lane * P2;
-      double c = 0.0;
 #pragma unroll
-      for (int q = 0; q < H2; ++q) {
-        const double2 f = row[q], g = th2[q];
+      for (int q = 0; q < NQ; ++q) {
+        const double2 f = row[q], g = thh[q];
         const double c0 = __dadd_rn(c, __dmul_rn(g.x, f.x));
         c = __dadd_rn(c0, __dmul_rn(g.y, f.y));
         row[q] = make_double2(c0, c);
       }
-      const double norm = c;              // padding topics add exact zeros
-      bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
-      zk = K - 1;
-      if (!exact) {
-        const double un = __dmul_rn(u, norm);
-        const double* cs = reinterpret_cast<const double*>(row);
-        // pos = number of k in [0, K-2] with c_k (1 + m) < u norm (a prefix)
-        int pos = 0;
+    }
+    const double A = __shfl_sync(0xffffffffu, c, j);          // first half's total
+    const double S = __shfl_sync(0xffffffffu, c, j + 16);     // second half's total
+    const double norm = __dadd_rn(A, S);                      // padding topics add exact zeros
+    const double off = half ? A : 0.0;
+    const double un = __dmul_rn(u, norm);
+    const double* cs = reinterpret_cast<const double*>(row);
+    // pos = number of k in this half's range with c_k (1 + m) < u norm (a prefix)
+    int pos = 0;
 #pragma unroll
-        for (int step = STEP0; step >= 1; step >>= 1)
-          if (pos + step <= K - 1 && __dmul_rn(cs[pos + step - 1], hi) < un) pos += step;
-        if (pos < K - 1) {
-          if (un < __dmul_rn(cs[pos], lo)) zk = pos;
-          else exact = true;
-        }
+    for (int step = STEP0; step >= 1; step >>= 1)
+      if (pos + step <= n_half && __dmul_rn(__dadd_rn(off, cs[pos + step - 1]), hi) < un) pos += step;
+    int cand = -1, dec = 0;
+    if (pos < n_half) {
+      cand = half * HK + pos;
+      dec = un < __dmul_rn(__dadd_rn(off, cs[pos]), lo);
+    }
+    const int cand1 = __shfl_sync(0xffffffffu, cand, j + 16);
+    const int dec1 = __shfl_sync(0xffffffffu, dec, j + 16);
+    if (active && half == 0) {
+      bool exact = !(norm >= 1e-290 && norm <= 1.7976931348623157e308);
+      int zk = K - 1;
+      if (!exact) {
+        if (cand >= 0) { zk = cand; exact = !dec; }
+        else if (cand1 >= 0) { zk = cand1; exact = !dec1; }
       }
       if (exact) zk = lda_reference_draw(K, th, phiT + (size_t)wt * KP, u);
       z[t] = zk;
       atomicAdd(&hist[zk], 1);
+      // topic-word counts: one fire-and-forget atomic per token
+      if (cnt_kw != nullptr) atomicAdd(cnt_kw + (size_t)zk * V + wt, 1);
     }
-    // topic-word counts: one fire-and-forget atomic per token (measured
-    // faster than aggregating equal (z, w) keys across the warp first)
-    if (cnt_kw != nullptr && active) atomicAdd(cnt_kw + (size_t)zk * V + wt, 1);
     __syncwarp();   // the stage is rewritten by the next chunk
   }
   __syncthreads();
@@ -485,14 +564,27 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
 
 template <int NQ>
 static int launch_lda_zq(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
-                         const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
-                         uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
+                         const double* phiT, const double* u_pre, int* z, int* cnt_dk, int* cnt_kw,
+                         uint64_t seed, uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr,
+                         cudaStream_t st) {
   const size_t smem = 16 * (size_t)(2 * NQ + NQ + (LDA_Z_THREADS / 32) * LDA_ZQ_ROWS * (2 * NQ + 1));
   AB_CUDA(cudaFuncSetAttribute(lda_zq_kernel<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  lda_zq_kernel<NQ><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed,
-                                                    iter_dev, iter, done_ctr);
+  lda_zq_kernel<NQ><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, doc_off, w, theta, phiT, u_pre, z, cnt_dk, cnt_kw,
+                                                    seed, iter_dev, iter, done_ctr);
   AB_LAUNCH_CHECK("lda_zq_kernel");
   return AB_OK;
+}
+
+// The uniforms of every token's draw (substream (t, iter, TAG_Z), position
+// 0), ahead of the z kernel: drawn on the theta branch of a sweep, which runs
+// beside the phi draw, so the z kernel on the critical path reads them.
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_zu_kernel(int T, double* __restrict__ u_z, uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+    u_z[t] = s.uniform();
+  }
 }
 
 // Count statistics of a given z (conj_stat_theta / conj_stat_phi of
@@ -560,13 +652,15 @@ int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double
   return AB_OK;
 }
 
+// u_pre (the tokens' uniforms drawn ahead, or null) is used by the K <= 64
+// kernel; the kernel for larger K draws its uniforms itself.
 int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
-                 const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                 const double* phiT, const double* u_pre, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
 #define AB_ZQ(nq)                                                                                      \
   case nq:                                                                                             \
-    return launch_lda_zq<nq>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, iter_dev, iter, \
-                             done_ctr, st);
+    return launch_lda_zq<nq>(D, K, V, doc_off, w, theta, phiT, u_pre, z, cnt_dk, cnt_kw, seed, iter_dev, \
+                             iter, done_ctr, st);
   if (K <= LDA_ZQ_MAX_K) {
     switch (Kp / 4) {
       AB_ZQ(1) AB_ZQ(2) AB_ZQ(3) AB_ZQ(4) AB_ZQ(5) AB_ZQ(6) AB_ZQ(7) AB_ZQ(8)
@@ -643,8 +737,8 @@ extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int*
   AB_REQUIRE((reinterpret_cast<uintptr_t>(phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_disc_z: phiT must be 16-byte aligned");
   AB_REQUIRE((cnt_dk == nullptr) == (cnt_kw == nullptr), AB_ERR_ARG,
              "ab_lda_disc_z: pass both count tables or neither");
-  return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, nullptr,
-                      iter, nullptr, as_stream(stream));
+  return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, nullptr, z, cnt_dk, cnt_kw, seed,
+                      nullptr, iter, nullptr, as_stream(stream));
 }
 
 // ---- variant of ab_lda_conj_phi that allocates nothing ----------------------
@@ -704,25 +798,40 @@ struct ab_lda {
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 
+// Sweep scratch: the phi draw's scratch (whose first 256 bytes hold the
+// runner's iteration and completion counters), then the tokens' uniforms
+// u_z f64 [T] drawn ahead of the z kernel.
+static inline size_t lda_uz_offset(int K, int V) { return al256(lda_phi_scratch(K, V)); }
+
 static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
   const ab_lda_desc& d = h->d;
   uint32_t* iter_dev = reinterpret_cast<uint32_t*>(d.scratch);
   uint32_t* done = iter_dev + 1;
+  double* u_z = d.K <= LDA_ZQ_MAX_K
+                    ? reinterpret_cast<double*>(static_cast<char*>(d.scratch) + lda_uz_offset(d.K, d.V))
+                    : nullptr;
   AB_CUDA(cudaEventRecord(h->fork, main));
   AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
+  // theta branch: theta draws, then the z kernel's uniforms
   int rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, main);
   if (rc) return rc;
+  if (u_z != nullptr && d.T > 0) {
+    const int nb = (int)std::min<long long>((long long)ceil_div(d.T, LDA_THREADS), 148 * 8);
+    lda_zu_kernel<<<nb, LDA_THREADS, 0, main>>>(d.T, u_z, d.seed, iter_dev, 0);
+    AB_LAUNCH_CHECK("lda_zu_kernel");
+  }
+  // phi branch
   rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.scratch, d.seed, iter_dev, 0,
                       side);
   if (rc) return rc;
   AB_CUDA(cudaEventRecord(h->join, side));
   AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
-  return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, d.z, d.cnt_dk, d.cnt_kw,
+  return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, u_z, d.z, d.cnt_dk, d.cnt_kw,
                       d.seed, iter_dev, 0, done, main);
 }
 
-extern "C" size_t ab_lda_scratch_bytes(int K, int V) {
-  return (K > 0 && V > 0) ? lda_phi_scratch(K, V) : 0;
+extern "C" size_t ab_lda_scratch_bytes(int K, int V, int T) {
+  return (K > 0 && V > 0 && T >= 0) ? lda_uz_offset(K, V) + sizeof(double) * (size_t)T : 0;
 }
 
 extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
@@ -733,6 +842,7 @@ extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
                  desc->beta && desc->cnt_dk && desc->cnt_kw && desc->scratch,
              AB_ERR_ARG, "ab_lda_create: every device pointer of the descriptor is required");
   AB_REQUIRE((reinterpret_cast<uintptr_t>(desc->phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_create: phiT must be 16-byte aligned");
+  AB_REQUIRE(desc->T >= 0, AB_ERR_ARG, "ab_lda_create: T < 0");
   ab_lda* h = new ab_lda();
   h->d = *desc;
   h->Kp = lda_kp(desc->K);

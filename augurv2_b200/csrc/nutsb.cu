@@ -50,7 +50,7 @@ struct ChainState {
   int mode, sp, n, jd, s, dir, rn, rs, f_cpy, leaves, overflow;
   int tp_h, ts_h, ms_h;
   uint32_t iter, h_pos;
-  int ndraws, last_depth, last_leaves, error;
+  int ndraws, last_depth, last_leaves, error, divergences, div_flag;
   float stepsize;
   double logu, ll0, sel_ll, depth_sum;
   Frame fr[NB_FRAMES];
@@ -183,6 +183,7 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
         const double ll = llp - 0.5 * ke;
         S.rn = S.logu <= ll ? 1 : 0;
         S.rs = S.logu < 1000.0 + ll ? 1 : 0;
+        if (!S.rs) S.div_flag = 1;   // outside the slice by more than deltaMax
         S.sp -= 1;
         S.mode = M_WALK;
       }
@@ -390,6 +391,8 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
         S.last_depth = jd;
         S.last_leaves = S.leaves;
         S.depth_sum += jd;
+        S.divergences += S.div_flag;
+        S.div_flag = 0;
         S.iter += 1;
         S.mode = M_START;
       }
@@ -451,18 +454,20 @@ __global__ void nutsb_init_kernel(NutsbDev d, const float* theta, const float* g
   }
 }
 
-// Per-chain summary: [ndraws, last_depth, last_leaves, error, iter, mean depth]
+// Per-chain summary: [ndraws, last_depth, last_leaves, error, iter, mean depth,
+// divergent iterations]
 __global__ void nutsb_info_kernel(NutsbDev d, double* info) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= d.C) return;
   const ChainState& s = d.st[c];
-  double* o = info + (size_t)c * 6;
+  double* o = info + (size_t)c * AB_NUTSB_INFO;
   o[0] = s.ndraws;
   o[1] = s.last_depth;
   o[2] = s.last_leaves;
   o[3] = s.error;
   o[4] = s.iter;
   o[5] = s.ndraws > 0 ? s.depth_sum / s.ndraws : 0.0;
+  o[6] = s.divergences;
 }
 
 // Forget the recorded draws (end of warm-up): every chain keeps its position,
@@ -473,6 +478,7 @@ __global__ void nutsb_reset_history_kernel(NutsbDev d) {
   if (c >= d.C) return;
   d.st[c].ndraws = 0;
   d.st[c].depth_sum = 0.0;
+  d.st[c].divergences = 0;
 }
 }  // namespace
 }  // namespace ab

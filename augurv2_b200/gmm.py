@@ -56,9 +56,10 @@ class GmmGibbs(Checkpointable):
         self.prop_cov = f64(prop_cov if prop_cov is not None else cov0)
         Kc = 1 if self.shared else K
         self.Kc = Kc
-        # tables: component slots [0, Kc), prior slot Kc, proposal slot Kc + 1
-        self.Linv = torch.zeros((Kc + 2, d, d), dtype=torch.float64, device=dev)
-        self.hdet = torch.zeros(Kc + 2, dtype=torch.float64, device=dev)
+        # tables: component slots [0, Kc), prior slot Kc, proposal slot Kc + 1,
+        # inverse-Wishart scale slot Kc + 2 (hmvgmm)
+        self.Linv = torch.zeros((Kc + 3, d, d), dtype=torch.float64, device=dev)
+        self.hdet = torch.zeros(Kc + 3, dtype=torch.float64, device=dev)
         self.cnt = torch.zeros(K, dtype=torch.int32, device=dev)
         self.sum = torch.zeros((K, d), dtype=torch.float64, device=dev)
         self.obs = torch.zeros((K, d, d), dtype=torch.float64, device=dev)
@@ -73,6 +74,55 @@ class GmmGibbs(Checkpointable):
                 "prep")
         if self.shared:
             N.check(L.ab_gmm_prep(1, d, N.ptr(self.cov), N.ptr(self.Linv), N.ptr(self.hdet), st), "prep")
+        else:
+            N.check(L.ab_gmm_prep(1, d, N.ptr(self.scale0), N.ptr(self.Linv[Kc + 2]), N.ptr(self.hdet[Kc + 2:]),
+                                  st), "prep")
+
+    # ---- log densities -----------------------------------------------------
+    def _ll_buffers(self):
+        if getattr(self, "_ll_scratch", None) is None:
+            dev = self.Y.device
+            self._ll_scratch = torch.zeros(int(N.lib().ab_ll_scratch_bytes()), dtype=torch.uint8, device=dev)
+            self._ll_out = torch.zeros(1, dtype=torch.float64, device=dev)
+        return self._ll_scratch, self._ll_out
+
+    def _refresh_tables(self, st):
+        if not self.shared:     # the component tables of the current covariances
+            N.check(N.lib().ab_gmm_prep(self.K, self.d, N.ptr(self.cov), N.ptr(self.Linv), N.ptr(self.hdet), st),
+                    "prep")
+
+    def ll_mod(self, stream=None):
+        """The model log density of the current state, as the reference's
+        augur_get_curr_ll returns it (hmvgmm.rv or mvgmm.rv: Dirichlet
+        weights without normalising constant, normal means, inverse-Wishart
+        covariances, categorical labels, normal data), on the device."""
+        st = N.stream_ptr(stream)
+        self._refresh_tables(st)
+        sc, out = self._ll_buffers()
+        Kc = self.Kc
+        N.check(N.lib().ab_gmm_ll_mod(
+            self.N, self.d, self.K, int(self.shared), N.ptr(self.Y), N.ptr(self.z), N.ptr(self.pis), N.ptr(self.mu),
+            N.ptr(self.Linv), N.ptr(self.hdet), N.ptr(self.mu0), N.ptr(self.Linv[Kc]), N.ptr(self.hdet[Kc:]),
+            None if self.shared else N.ptr(self.alpha), 0 if self.shared else self.df,
+            None if self.shared else N.ptr(self.scale0), None if self.shared else N.ptr(self.hdet[Kc + 2:]),
+            N.ptr(out), N.ptr(sc), st), "ab_gmm_ll_mod")
+        return float(out.item())
+
+    def pred_ll(self, Y_test, stream=None):
+        """Log-likelihood of test points under the current weights, means and
+        covariances: sum_n log sum_k pis[k] N(y_n | mu_k, cov_k) (inner_ll of
+        experiments/hmvgmm/hmvgmm.py:143-178), on the device."""
+        Y_test = np.ascontiguousarray(Y_test, np.float32)
+        if Y_test.ndim != 2 or Y_test.shape[1] != self.d:
+            raise ValueError("test points must be [n, %d]" % self.d)
+        st = N.stream_ptr(stream)
+        self._refresh_tables(st)
+        sc, out = self._ll_buffers()
+        Yd = torch.as_tensor(Y_test).to(self.Y.device)
+        N.check(N.lib().ab_gmm_pred_ll(Y_test.shape[0], self.d, self.K, int(self.shared), N.ptr(Yd), N.ptr(self.pis),
+                                       N.ptr(self.mu), N.ptr(self.Linv), N.ptr(self.hdet), N.ptr(out), N.ptr(sc),
+                                       st), "ab_gmm_pred_ll")
+        return float(out.item())
 
     # ---- one augur_step ----------------------------------------------------
     @traced("gmm.sweep")

@@ -128,10 +128,24 @@ class HlrChains(Checkpointable):
             init[:, D + 1] = 1.0
         init = np.broadcast_to(np.asarray(init, np.float64), (self.C, D + 2)).copy()
         self.pars = torch.as_tensor(np.ascontiguousarray(init)).to(dev)
-        self.stats = torch.zeros((self.C, self.ncomp, 4), dtype=torch.float64, device=dev)
+        # per chain and component: accepts, NUTS depth, NUTS leaves / RSlice
+        # reflections, stack overflows, divergent iterations
+        self.stats = torch.zeros((self.C, self.ncomp, 5), dtype=torch.float64, device=dev)
         need_nuts = any(c.kind == NUTS for c in comps)
         nbytes = int(N.lib().ab_hlr_chain_scratch_bytes(self.C, D)) if need_nuts else 8
         self.scratch = torch.zeros(nbytes, dtype=torch.uint8, device=dev)
+
+    def det_bias(self, stream=None):
+        """dethlr.rv's deterministic bias[n] = sigmoid(dotprod(theta, x[n]) + b)
+        of every chain, [C, N] float64, computed on the device."""
+        out = torch.empty((self.C, self.data.N), dtype=torch.float64, device=self.pars.device)
+        N.check(N.lib().ab_hlr_det(C.byref(self.data.c), self.C, N.ptr(self.pars), N.ptr(out),
+                                   N.stream_ptr(stream)), "ab_hlr_det")
+        return out
+
+    def divergences(self):
+        """Divergent HMC / NUTS iterations per component, summed over chains."""
+        return self.stats[:, :, 4].sum(0).cpu().numpy()
 
     @traced("hlr.run_chains")
     def run(self, n_iter=1, stream=None):

@@ -145,7 +145,7 @@ class _ChainState:
         self.p, self.g_cur, self.theta0, self.g0 = z(C_, D), z(C_, D), z(C_, D), z(C_, D)
         self.logp_cur, self.logp0, self.H0 = z(C_, dt=f64), z(C_, dt=f64), z(C_, dt=f64)
         self.eps_c = z(C_)
-        self.stats = z(C_, 2, dt=f64)
+        self.stats = z(C_, 3, dt=f64)     # accepts, summed accept probability, divergences
         self.iter = torch.zeros(1, dtype=torch.int64, device=device)
         self.eps0 = torch.full((1,), float(eps), dtype=f32, device=device)
         self.c = HmcbStateC(C_, D, int(seed), self.iter.data_ptr(), self.eps0.data_ptr(), float(jitter),
@@ -239,6 +239,11 @@ class BatchedHmc(Checkpointable):
         st = self.s.stats.cpu().numpy()
         it = int(self.s.iter.item())
         return st[:, 0].sum() / max(1, it * self.C), st[:, 1].sum() / max(1, it * self.C)
+
+    def divergences(self):
+        """Divergent transitions (energy error above AB_DIVERGENCE_DH, or not
+        finite) summed over chains since the last reset_stats."""
+        return int(self.s.stats[:, 2].sum().item())
 
     def reset_stats(self):
         self.s.stats.zero_()
@@ -534,6 +539,11 @@ class SurrogateHmc(Checkpointable):
         it = int(self.s.iter.item())
         return st[:, 0].sum() / max(1, it * self.C), st[:, 1].sum() / max(1, it * self.C)
 
+    def divergences(self):
+        """Divergent transitions (energy error above AB_DIVERGENCE_DH, or not
+        finite) summed over chains since the last reset_stats."""
+        return int(self.s.stats[:, 2].sum().item())
+
     def reset_stats(self):
         self.s.stats.zero_()
         self.s.iter.zero_()
@@ -607,7 +617,7 @@ class BatchedNuts(Checkpointable):
             self.C, self.hist_cap, D)
         self.hist_depth = self.mem[off_d:off_d + 4 * self.C * self.hist_cap].view(torch.int32).view(
             self.C, self.hist_cap)
-        self.info_buf = torch.zeros((self.C, 6), dtype=torch.float64, device=dev)
+        self.info_buf = torch.zeros((self.C, 7), dtype=torch.float64, device=dev)
         self.rounds = 0
         self.graph = None
         del f32
@@ -646,6 +656,11 @@ class BatchedNuts(Checkpointable):
         N.check(N.lib().ab_nutsb_info(N.ptr(self.mem), self.C, self.D, self.hist_cap, N.ptr(self.info_buf),
                                       N.stream_ptr()), "ab_nutsb_info")
         return self.info_buf.cpu().numpy()
+
+    def divergences(self):
+        """Divergent iterations (a leaf below the slice level by more than
+        AB_DIVERGENCE_DH) summed over chains since the last reset_history."""
+        return int(self.info()[:, 6].sum())
 
     def draws(self):
         """[n, C, D]: the first n draws of every chain, n = the smallest count."""

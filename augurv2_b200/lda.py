@@ -68,7 +68,8 @@ class LdaGibbs(Checkpointable):
         self.z = torch.zeros(self.T, dtype=torch.int32, device=self.dev)
         self.cnt_dk = torch.zeros((self.D, self.K), dtype=torch.int32, device=self.dev)
         self.cnt_kw = torch.zeros((self.K, self.V), dtype=torch.int32, device=self.dev)
-        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V)), dtype=torch.uint8, device=self.dev)
+        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V, self.T)), dtype=torch.uint8,
+                                   device=self.dev)
         # defaults (uniform theta and phi, z = 0) are filled on the device;
         # given values are uploaded
         if theta is None:
@@ -79,7 +80,7 @@ class LdaGibbs(Checkpointable):
         desc = N.LdaDesc(self.D, self.K, self.V, self.doc_off.data_ptr(), self.w.data_ptr(),
                          self.alpha.data_ptr(), self.beta.data_ptr(), self.z.data_ptr(),
                          self.theta.data_ptr(), self.phiT.data_ptr(), self.cnt_dk.data_ptr(),
-                         self.cnt_kw.data_ptr(), self.scratch.data_ptr(), self.seed)
+                         self.cnt_kw.data_ptr(), self.scratch.data_ptr(), self.seed, self.T)
         h = C.c_void_p()
         N.check(L.ab_lda_create(C.byref(desc), C.byref(h)), "ab_lda_create")
         self._h = h
@@ -177,6 +178,44 @@ class LdaGibbs(Checkpointable):
         if pending is not None:
             pending[1].synchronize()
             yield tuple(t.numpy() for t in self._sample_views(pending[0]))
+
+    # ---- log densities -----------------------------------------------------
+    def _ll_buffers(self):
+        if getattr(self, "_ll_scratch", None) is None:
+            self._ll_scratch = torch.zeros(int(N.lib().ab_ll_scratch_bytes()), dtype=torch.uint8, device=self.dev)
+            self._ll_out = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        return self._ll_scratch, self._ll_out
+
+    def ll_mod(self, stream=None):
+        """The model log density of the current state, as the reference's
+        augur_get_curr_ll returns it (its Dirichlet densities carry no
+        normalising constant), computed on the device."""
+        sc, out = self._ll_buffers()
+        N.check(N.lib().ab_lda_ll_mod(self.D, self.K, self.V, N.ptr(self.doc_off), N.ptr(self.w), N.ptr(self.z),
+                                      N.ptr(self.alpha), N.ptr(self.beta), N.ptr(self.theta), N.ptr(self.phiT),
+                                      N.ptr(out), N.ptr(sc), N.stream_ptr(stream)), "ab_lda_ll_mod")
+        return float(out.item())
+
+    def pred_ll(self, w_heldout, stream=None):
+        """Log-likelihood of held-out tokens under the current theta and phi:
+        sum over tokens of log sum_k theta[d][k] phi[k][w] (the inner sum of
+        experiments/lda/lda.py:149-173).  w_heldout: one token array per
+        document (D of them), or a CSR pair (doc_off, w)."""
+        if isinstance(w_heldout, tuple):
+            off, w = (np.ascontiguousarray(a, np.int32) for a in w_heldout)
+        else:
+            off, w = flatten_docs(w_heldout)
+        if len(off) != self.D + 1:
+            raise ValueError("held-out tokens must be given for all %d documents" % self.D)
+        if len(w) and (w.min() < 0 or w.max() >= self.V):
+            raise ValueError("token ids must lie in [0, V)")
+        sc, out = self._ll_buffers()
+        off_d = torch.as_tensor(off).to(self.dev)
+        w_d = torch.as_tensor(w).to(self.dev)
+        N.check(N.lib().ab_lda_pred_ll(self.D, self.K, self.V, N.ptr(off_d), N.ptr(w_d), N.ptr(self.theta),
+                                       N.ptr(self.phiT), N.ptr(out), N.ptr(sc), N.stream_ptr(stream)),
+                "ab_lda_pred_ll")
+        return float(out.item())
 
     # ---- sampling ----------------------------------------------------------
     @traced("lda.sweep")

@@ -697,18 +697,24 @@ def run_ours(args, rank, world, local_rank):
 
 
 def time_z_kernel(s, stream, flush, reps):
+    """Average duration of the production z launch (ab_lda_disc_z with both
+    count tables, the launch the sweep makes), L2 flushed and the topic-word
+    table zeroed before each launch, outside its events."""
     import torch
     from augurv2_b200 import _native as N
     L = N.lib()
     z = s.z.clone()
+    cdk = torch.zeros_like(s.cnt_dk)
+    ckw = torch.zeros_like(s.cnt_kw)
     evs = []
     with torch.cuda.stream(stream):
         for i in range(reps + 2):
             flush.fill_(i & 0xFF)
+            ckw.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             N.check(L.ab_lda_disc_z(s.D, s.K, s.V, N.ptr(s.doc_off), N.ptr(s.w), N.ptr(s.theta),
-                                    N.ptr(s.phiT), N.ptr(z), None, None, s.seed, 0,
+                                    N.ptr(s.phiT), N.ptr(z), N.ptr(cdk), N.ptr(ckw), s.seed, 0,
                                     N.stream_ptr(stream)), "disc_z")
             b.record(stream)
             evs.append((a, b))

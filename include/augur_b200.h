@@ -41,6 +41,14 @@ enum {
   AB_ERR_STATE = 5     /* call not valid in the object's current state      */
 };
 
+/* Divergence bound of every HMC / NUTS sampler: a transition whose energy
+ * error (H_end - H_start) exceeds it, or is not finite, is counted as
+ * divergent (for NUTS, a leaf whose log density falls below the slice level
+ * by more than it: the reference's deltaMax, cbits/augur_mcmclib.h:152).
+ * Divergent transitions are rejected by the accept test in any case; the
+ * count is a diagnostic. */
+#define AB_DIVERGENCE_DH 1000.0
+
 /* Message of the calling thread's last failed call ("" if none).
  * Replaces the reference's exit()-on-error (cbits/augur_util.c:30-36). */
 const char* ab_last_error(void);
@@ -91,9 +99,12 @@ int ab_lda_conj_phi(int K, int V, const double* beta, int* cnt_kw, double* phiT,
  * ab_lda_phi_scratch_bytes(K, V) <= 1 MiB (K = 50, V = 10,000 needs 17 KB)
  * and rejects larger sizes with AB_ERR_ARG.  The first call on a device looks
  * up the array's device address; make that first call before any stream
- * capture.  All calls share the array: calls whose work overlaps on the GPU
- * (other streams, other threads) race and must be serialised by the
- * caller. */
+ * capture.  The address is cached per device for the life of the process: a
+ * cudaDeviceReset (or any other teardown of the device's primary context)
+ * leaves the cached address stale, so do not call this entry point again in
+ * a process that has reset the device.  All calls share the array: calls
+ * whose work overlaps on the GPU (other streams, other threads) race and must
+ * be serialised by the caller. */
 int ab_lda_conj_phi_noalloc(int K, int V, const double* beta, int* cnt_kw, double* phiT,
                             int clear_counts, uint64_t seed, uint32_t iter, void* stream);
 
@@ -119,12 +130,15 @@ typedef struct ab_lda_desc {
   double* phiT;         /* [V][Kp] */
   int* cnt_dk;          /* [D][K] */
   int* cnt_kw;          /* [K][V] */
-  void* scratch;        /* ab_lda_scratch_bytes(K, V) bytes of device memory */
+  void* scratch;        /* ab_lda_scratch_bytes(K, V, T) bytes of device memory */
   uint64_t seed;
+  int T;                /* tokens: doc_off[D] */
 } ab_lda_desc;
 
 typedef struct ab_lda ab_lda;
-size_t ab_lda_scratch_bytes(int K, int V);
+/* Scratch of the sweep runner: counters, the phi draw's partial sums and
+ * normalisers, and the tokens' uniforms drawn ahead of the z kernel. */
+size_t ab_lda_scratch_bytes(int K, int V, int T);
 /* Replaces augur_iface_init for the LDA model (CgStInit.hs:474-510); the
  * caller owns every buffer named by the descriptor. */
 int ab_lda_create(const ab_lda_desc* desc, ab_lda** out);
@@ -175,13 +189,14 @@ int ab_hlr_ll_grad(const ab_hlr_model* model, const int* idx_dev, const int* idx
 
 /* n_iter augur_step calls of a schedule of components for C independent
  * chains (one thread block per chain, the whole iteration on chip).
- * pars f64[C][D+2] in/out; stats f64[C][n_comps][4] accumulates {accepts
- * (moves for RSlice), NUTS depth, NUTS leaves or RSlice reflections, stack
- * overflows}.  scratch:
+ * pars f64[C][D+2] in/out; stats f64[C][n_comps][AB_HLR_STATS] accumulates
+ * {accepts (moves for RSlice), NUTS depth, NUTS leaves or RSlice
+ * reflections, stack overflows, divergent HMC / NUTS iterations}.  scratch:
  * ab_hlr_chain_scratch_bytes(C, D) bytes, needed when a NUTS component is
  * present.  Substreams: momentum (c*P+j, iter, 4|comp<<8), HMC jitter and
  * accept (c, iter, 5|comp<<8), NUTS (c, iter, 6|comp<<8), MWG (c, iter,
  * 11|comp<<8), RSlice slice level (c, iter, 14|comp<<8). */
+#define AB_HLR_STATS 5
 size_t ab_hlr_chain_scratch_bytes(int C, int D);
 int ab_hlr_run_chains(const ab_hlr_model* model, const ab_hlr_comp* comps_host, const void* comps_dev,
                       int n_comps, const int* idx_dev, const int* idx_host, int C, double* pars,
@@ -250,6 +265,54 @@ int ab_gmm_mwg(int N, int d, int K, int shared_cov, const float* Y, const int* z
                int compat, double* mu, uint64_t seed, uint32_t iter, uint32_t comp, int* accepts, void* stream);
 
 /* ======================================================================= *
+ * Whole-model log density (augur_get_curr_ll), held-out predictive
+ * log-likelihoods, and dethlr's deterministic variable.
+ * Each reduction writes one double to `out` (device memory) and needs
+ * `scratch` of ab_ll_scratch_bytes() bytes of device memory, zero before the
+ * first call (it returns to zero after each call); calls sharing a scratch
+ * must not overlap.
+ * ======================================================================= */
+size_t ab_ll_scratch_bytes(void);
+
+/* ll_mod of lda.rv: replaces the generated ll_mod behind augur_get_curr_ll
+ * (CgStInit.hs:597-602): sum of augur_dirichlet_ll (no normalising constant,
+ * cbits/augur_dist.c:488-496) over the theta rows (alpha) and phi rows
+ * (beta), and augur_categorical_ll (:96-102) of every z and w. */
+int ab_lda_ll_mod(int D, int K, int V, const int* doc_off, const int* w, const int* z, const double* alpha,
+                  const double* beta, const double* theta, const double* phiT, double* out, void* scratch,
+                  void* stream);
+
+/* Predictive log-likelihood of held-out tokens (doc_off, w) for one theta
+ * sample: sum over tokens of logsumexp_k(log theta[d][k] + log phi[k][w])
+ * (experiments/lda/lda.py:149-173, the inner sum). */
+int ab_lda_pred_ll(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                   const double* phiT, double* out, void* scratch, void* stream);
+
+/* ll_mod of hmvgmm.rv (shared_cov = 0) or mvgmm.rv (shared_cov = 1), from the
+ * component tables of ab_gmm_prep (Linv, hdet: [Kc] slots), the table of the
+ * mean prior's covariance (Linv0, hdet0 [1]) and, for hmvgmm, the Dirichlet
+ * alpha, the inverse-Wishart df and scale0 with its hdet_s0 [1] =
+ * log(det scale0)/2 (ab_gmm_prep of scale0); all pointers are device memory:
+ * augur_dirichlet_ll, augur_mvnormal_ll (:548-568), augur_invwishart_ll
+ * (:679-711, with augur_multi_lgamma's log(3.1415)), augur_categorical_ll. */
+int ab_gmm_ll_mod(int N, int d, int K, int shared_cov, const float* Y, const int* z, const double* pis,
+                  const double* mu, const double* Linv, const double* hdet, const double* mu0,
+                  const double* Linv0, const double* hdet0, const double* alpha, int df, const double* scale0,
+                  const double* hdet_s0, double* out, void* scratch, void* stream);
+
+/* Predictive log-likelihood of points Y [N][d] for one (pis, mu, cov) sample:
+ * sum_n logsumexp_k(log N(y_n | mu_k, cov_k) + log pis[k])
+ * (experiments/hmvgmm/hmvgmm.py:143-178, inner_ll). */
+int ab_gmm_pred_ll(int N, int d, int K, int shared_cov, const float* Y, const double* pis, const double* mu,
+                   const double* Linv, const double* hdet, double* out, void* scratch, void* stream);
+
+/* dethlr.rv's deterministic bias[n] = sigmoid(dotprod(theta, x[n]) + b) for
+ * C parameter vectors pars f64 [C][D+2]: out f64 [C][N] (replaces the
+ * generated deterministic-variable code, CgDet.hs, with augur_dotprod and
+ * augur_expit, cbits/augur_math.c:52-54,119-142). */
+int ab_hlr_det(const ab_hlr_model* model, int C, const double* pars, double* out, void* stream);
+
+/* ======================================================================= *
  * Batched HLR on the tensor cores: C chains against one data set.
  * The reference evaluates one chain's block log density and gradient with
  * its generated ll_/grad_ functions (compiler/augur/src/Comm/CgLike.hs:
@@ -310,6 +373,7 @@ int ab_hlrb_logp_grad_cfg(const ab_hlrb_model* m, int C, const float* theta, int
  * or surrogate) between the calls:
  *   begin; { gradient at theta; step } x (L-1); exact logp + gradient; final
  * ======================================================================= */
+#define AB_HMCB_STATS 3
 typedef struct ab_hmcb_state {
   int C, D;
   unsigned long long seed;
@@ -325,7 +389,8 @@ typedef struct ab_hmcb_state {
   double* logp0;        /* [C]                                                */
   double* H0;           /* [C] starting energy                                */
   float* eps_c;         /* [C] this iteration's step size                     */
-  double* stats;        /* [C][2] accepted count, summed acceptance prob.     */
+  double* stats;        /* [C][AB_HMCB_STATS] accepted count, summed
+                           acceptance probability, divergent transitions     */
 } ab_hmcb_state;
 
 int ab_hmcb_begin(const ab_hmcb_state* s, void* stream);
@@ -340,9 +405,10 @@ int ab_hmcb_final(const ab_hmcb_state* s, const float* g_new, const double* logp
  * leaves the leaf position in the thprop array) followed by the caller's
  * evaluation of logp [C] and grad [C][P] at thprop, passed to the next
  * advance.  Completed iterations append their draws to a per-chain history
- * of hist_cap rows.  info[c][6] = draws, last tree depth, last leaves,
- * error flag, iteration, mean depth.
+ * of hist_cap rows.  info[c][AB_NUTSB_INFO] = draws, last tree depth, last
+ * leaves, error flag, iteration, mean depth, divergent iterations.
  * ======================================================================= */
+#define AB_NUTSB_INFO 7
 size_t ab_nutsb_state_bytes(int C, int P, int hist_cap);
 int ab_nutsb_init(void* state, int C, int P, int hist_cap, const float* theta, const float* grad, const double* logp,
                   uint32_t iter0, void* stream);
@@ -463,6 +529,107 @@ enum {
 int ab_conj_scalar(int kind, int G, const int* off, const double* x, const double* aux, const double* h0,
                    const double* h1, const double* h2, int per_group, double* stat_sum, double* stat_aux,
                    double* out, uint64_t seed, uint32_t iter, void* stream);
+
+/* ======================================================================= *
+ * Model handles: the generated module's entry points (augur_iface_init,
+ * augur_step, augur_cpy, augur_set_pt, augur_get_curr_ll;
+ * compiler/augur/src/CudaC/CgStInit.hs:474-602, called from
+ * pyaugur/pyaugur/augurlib.py:445-519) as one opaque handle per model for
+ * callers with host memory only.  ab_init_* copies the HOST arrays of the
+ * descriptor into device memory the handle allocates and owns (as
+ * augur_iface_init deep-copies its inputs, cbits/augur_rtmem.c:297-303);
+ * ab_destroy frees it.  Handles share no state: several can live in one
+ * process (the reference keeps one global chain, cbits/augur_mcmclib.h:
+ * 44-45).  A failed call returns its status and its message is kept on the
+ * handle (ab_model_last_error) as well as in ab_last_error().
+ * ======================================================================= */
+typedef struct ab_model ab_model;
+enum { AB_MODEL_LDA = 1, AB_MODEL_HLR = 2, AB_MODEL_GMM = 3 };
+
+/* lda.rv.  theta [D][K], phi [K][V], z [T] are the initial point (NULL:
+ * uniform theta and phi, z = 0). */
+typedef struct ab_lda_init {
+  int D, K, V;
+  const int* doc_off;     /* [D+1], doc_off[0] = 0 */
+  const int* w;           /* [T = doc_off[D]], ids in [0, V) */
+  const double* alpha;    /* [K] */
+  const double* beta;     /* [V] */
+  const double* theta;    /* [D][K] or NULL */
+  const double* phi;      /* [K][V] or NULL */
+  const int* z;           /* [T] or NULL */
+  uint64_t seed;
+  uint32_t iter0;
+} ab_lda_init;
+int ab_init_lda(const ab_lda_init* init, ab_model** out);
+
+/* hlr.rv / dethlr.rv / the inverse-gamma variance variant: C chains of a
+ * schedule of components (ab_hlr_comp, blocks indexing idx) on the per-chain
+ * engine; X is stored in f32 on the device.  pars [C][D+2] = [theta, b, v]. */
+typedef struct ab_hlr_init {
+  int N, D, has_b, vprior, compat;
+  double lam, a0, s0;
+  const double* X;            /* [N][D] */
+  const int* y;               /* [N], 0/1 */
+  int C;
+  const double* pars;         /* [C][D+2] initial point of every chain */
+  int n_comps;
+  const ab_hlr_comp* comps;   /* [n_comps] */
+  const int* idx;             /* [n_idx] block indices */
+  int n_idx;
+  uint64_t seed;
+  uint32_t iter0;
+} ab_hlr_init;
+int ab_init_hlr(const ab_hlr_init* init, ab_model** out);
+
+/* mvgmm.rv (shared_cov = 1: fixed pis and covs [d][d]; move 0 = ConjGibbs,
+ * 1 = ESlice, 2 = MWG with proposal covariance prop_cov) or hmvgmm.rv
+ * (shared_cov = 0: pis, covs [K][d][d] initial, alpha, df, scale0; move 0).
+ * Y is stored in f32 on the device. */
+typedef struct ab_gmm_init {
+  int N, d, K, shared_cov, move, compat;
+  const double* Y;            /* [N][d] */
+  const double* mu0;          /* [d] */
+  const double* cov0;         /* [d][d] */
+  const double* pis;          /* [K] */
+  const double* covs;         /* [d][d] (mvgmm) or [K][d][d] (hmvgmm) */
+  const double* alpha;        /* [K] (hmvgmm) */
+  int df;                     /* (hmvgmm) */
+  const double* scale0;       /* [d][d] (hmvgmm) */
+  const double* prop_cov;     /* [d][d] (MWG) */
+  const double* mu;           /* [K][d] initial */
+  const int* z;               /* [N] initial */
+  uint64_t seed;
+  uint32_t iter0;
+} ab_gmm_init;
+int ab_init_gmm(const ab_gmm_init* init, ab_model** out);
+
+int ab_model_kind(const ab_model* h);
+const char* ab_model_last_error(const ab_model* h);
+/* n_iters augur_step calls (CgKern.hs:232-238) on the caller's stream. */
+int ab_step(ab_model* h, int n_iters, void* stream);
+/* Iterations taken since ab_init_* (plus iter0): the Philox iteration index
+ * of the next step. */
+uint32_t ab_iteration(const ab_model* h);
+/* The parameters in a host buffer of ab_state_bytes(h) bytes (augur_cpy /
+ * augur_set_pt).  Layouts: LDA theta f64 [D][K], phi f64 [K][V], z int32 [T];
+ * HLR pars f64 [C][D+2]; GMM pis f64 [K], mu f64 [K][d], cov f64 [K][d][d]
+ * (hmvgmm only), z int32 [N].  Both calls finish before returning. */
+size_t ab_state_bytes(const ab_model* h);
+int ab_get_state(ab_model* h, void* host, size_t bytes, void* stream);
+int ab_set_state(ab_model* h, const void* host, size_t bytes, void* stream);
+/* The complete sampler state (parameters, statistics the next step reads,
+ * iteration counter and seed) in a host buffer of ab_checkpoint_bytes(h)
+ * bytes.  ab_restore into a handle made with the same ab_init_* descriptor
+ * sizes continues the chain exactly as the uninterrupted run (every draw is
+ * addressed by the iteration in the counter-based Philox stream). */
+size_t ab_checkpoint_bytes(ab_model* h);
+int ab_checkpoint(ab_model* h, void* host, size_t bytes, void* stream);
+int ab_restore(ab_model* h, const void* host, size_t bytes, void* stream);
+/* augur_get_curr_ll: the model log density of the current state, one value
+ * per chain (ab_curr_ll_count: C for HLR, 1 otherwise), into host memory. */
+int ab_curr_ll_count(const ab_model* h);
+int ab_curr_ll(ab_model* h, double* host, int n, void* stream);
+int ab_destroy(ab_model* h);
 
 #ifdef __cplusplus
 }

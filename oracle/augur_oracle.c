@@ -825,6 +825,28 @@ void orc_gmm_disc_z(const orc_gmm* g, const double* pis, const double* mu, const
   free(pmf);
 }
 
+/* The same draw for the listed points only: z_out[i] is the assignment of
+ * point idx[i] with its own substream (idx[i], iter, Z), so a subset of a
+ * full-size pass can be checked at the cost of the subset. */
+void orc_gmm_disc_z_subset(const orc_gmm* g, const double* pis, const double* mu, const double* cov,
+                           const int* idx, int n_idx, int* z_out, uint64_t seed, uint32_t iter) {
+  const int d = g->d, K = g->K;
+  double* pmf = (double*)malloc(sizeof(double) * K);
+  for (int i = 0; i < n_idx; i++) {
+    const int n = idx[i];
+    for (int k = 0; k < K; k++) {
+      const double* ck = g->shared_cov ? cov : cov + (size_t)k * d * d;
+      double prob = 1.0;
+      prob *= pis[k];
+      prob *= exp(orc_mvnormal_ll(g->Y + (size_t)n * d, mu + (size_t)k * d, ck, d));
+      pmf[k] = prob;
+    }
+    orc_stream s = orc_make(seed, (uint32_t)n, iter, ORC_TAG_Z);
+    z_out[i] = orc_unnorm_disc(&s, pmf, K);
+  }
+  free(pmf);
+}
+
 /* Statistics of CgConj.hs:186-246 (AtomicPar over n, sequential here):
  * cnt[k], sum[k] = sum of y, obs[k] = sum of (y - mu[z])(y - mu[z])^T. */
 void orc_gmm_stats(const orc_gmm* g, const int* z, const double* mu, int* cnt, double* sum, double* obs) {
@@ -1027,4 +1049,146 @@ void orc_conj_scalar(int kind, int G, const int* off, const double* x, const dou
     }
     out[g] = r;
   }
+}
+
+/* ---- model log density (ll_mod) and predictive log-likelihoods --------- */
+
+/* augur_dirichlet_ll (augur_dist.c:488-496): no normalising constant. */
+static double orc_dirichlet_ll(const double* pt, const double* alpha, int n) {
+  double acc = 0.0;
+  for (int i = 0; i < n; i++) acc += (alpha[i] - 1.0) * log(pt[i]);
+  return acc;
+}
+
+/* ll_mod of lda.rv, the function augur_get_curr_ll returns
+ * (CgStInit.hs:597-602): the model's factors in model order, each a sum over
+ * its comprehension (CgLike.hs:128-147) - augur_dirichlet_ll of the theta
+ * rows, of the phi rows, then augur_categorical_ll (log pmf[pt],
+ * augur_dist.c:96-102) of every z and every w.  phi is [K][V]. */
+double orc_lda_ll_mod(int D, int K, int V, const int* doc_off, const int* w, const int* z,
+                      const double* alpha, const double* beta, const double* theta, const double* phi) {
+  double ll = 0.0, s = 0.0;
+  for (int d = 0; d < D; d++) s += orc_dirichlet_ll(theta + (size_t)d * K, alpha, K);
+  ll += s;
+  s = 0.0;
+  for (int k = 0; k < K; k++) s += orc_dirichlet_ll(phi + (size_t)k * V, beta, V);
+  ll += s;
+  s = 0.0;
+  for (int d = 0; d < D; d++)
+    for (int t = doc_off[d]; t < doc_off[d + 1]; t++) s += log(theta[(size_t)d * K + z[t]]);
+  ll += s;
+  s = 0.0;
+  for (int d = 0; d < D; d++)
+    for (int t = doc_off[d]; t < doc_off[d + 1]; t++) s += log(phi[(size_t)z[t] * V + w[t]]);
+  ll += s;
+  return ll;
+}
+
+/* augur_multi_lgamma (augur_math.c:80-86), with the reference's log(3.1415). */
+static double orc_multi_lgamma(int p, double x) {
+  double res = (p * (p - 1) * 0.25) * log(3.1415);
+  for (int i = 1; i < p + 1; i++) res += lgamma(x - (i - 1.0) / 2.0);
+  return res;
+}
+
+#define M_(A, i, j) (A)[(size_t)(i) * d + (j)]
+
+/* augur_invwishart_ll (augur_dist.c:679-711). */
+double orc_invwishart_ll(const double* pt, int df, const double* scale, int d) {
+  double* L = (double*)malloc(sizeof(double) * d * d);
+  double* W = (double*)malloc(sizeof(double) * d * d);
+  memcpy(L, scale, sizeof(double) * d * d);
+  orc_mat_cholesky(L, d);
+  double detPsi = 1.0;
+  for (int i = 0; i < d; i++) detPsi *= M_(L, i, i);
+  detPsi *= detPsi;
+  memcpy(W, pt, sizeof(double) * d * d);
+  orc_mat_cholesky(W, d);
+  double detX = 1.0;
+  for (int i = 0; i < d; i++) detX *= M_(W, i, i);
+  detX *= detX;
+  orc_mat_cholesky_invert(W, d);
+  double tr = 0.0;
+  for (int i = 0; i < d; i++) {
+    double tmp = 0.0;
+    for (int j = 0; j < d; j++) tmp += M_(scale, i, j) * M_(W, j, i);
+    tr += tmp;
+  }
+  double c = -df * d / 2.0 * log(2.0) - orc_multi_lgamma(d, df / 2.0);
+  free(L); free(W);
+  return c - (df + d + 1.0) / 2.0 * log(detX) + df / 2.0 * log(detPsi) - 0.5 * tr;
+}
+
+/* ll_mod of hmvgmm.rv (shared_cov = 0: pis ~ Dirichlet(alpha), mu[k] ~
+ * MvNormal(mu0, covs0), cov[k] ~ InvWishart(df, scale0), z[n] ~
+ * Categorical(pis), y[n] ~ MvNormal(mu[z[n]], cov[z[n]])) or of mvgmm.rv
+ * (shared_cov = 1: mu[k], z[n], y[n] ~ MvNormal(mu[z[n]], covs)), factors in
+ * model order as orc_lda_ll_mod. */
+double orc_gmm_ll_mod(const orc_gmm* g, const double* pis, const double* mu, const double* cov, const int* z) {
+  const int d = g->d, K = g->K;
+  double ll = 0.0, s = 0.0;
+  if (!g->shared_cov) ll += orc_dirichlet_ll(pis, g->alpha, K);
+  for (int k = 0; k < K; k++) s += orc_mvnormal_ll(mu + (size_t)k * d, g->mu0, g->cov0, d);
+  ll += s;
+  s = 0.0;
+  if (!g->shared_cov) {
+    for (int k = 0; k < K; k++) s += orc_invwishart_ll(cov + (size_t)k * d * d, g->df, g->scale0, d);
+    ll += s;
+    s = 0.0;
+  }
+  for (int n = 0; n < g->N; n++) s += log(pis[z[n]]);
+  ll += s;
+  s = 0.0;
+  for (int n = 0; n < g->N; n++) {
+    const double* ck = g->shared_cov ? cov : cov + (size_t)z[n] * d * d;
+    s += orc_mvnormal_ll(g->Y + (size_t)n * d, mu + (size_t)z[n] * d, ck, d);
+  }
+  ll += s;
+  return ll;
+}
+
+/* log sum_k exp(x_k) as scipy.misc.logsumexp: max + log(sum exp(x - max)). */
+static double orc_logsumexp(const double* x, int K) {
+  double m = x[0];
+  for (int k = 1; k < K; k++) if (x[k] > m) m = x[k];
+  if (!(m > -INFINITY)) return m;
+  double s = 0.0;
+  for (int k = 0; k < K; k++) s += exp(x[k] - m);
+  return m + log(s);
+}
+
+/* Predictive log-likelihood of held-out tokens for one theta sample
+ * (experiments/lda/lda.py:149-173, the inner sum):
+ * sum_{d,j} logsumexp_k (log theta[d][k] + log phi[k][w_dj]).  phi [K][V]. */
+double orc_lda_pred_ll(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                       const double* phi) {
+  double* tmp = (double*)malloc(sizeof(double) * K);
+  double acc = 0.0;
+  for (int d = 0; d < D; d++)
+    for (int t = doc_off[d]; t < doc_off[d + 1]; t++) {
+      for (int k = 0; k < K; k++) tmp[k] = log(theta[(size_t)d * K + k]) + log(phi[(size_t)k * V + w[t]]);
+      acc += orc_logsumexp(tmp, K);
+    }
+  free(tmp);
+  return acc;
+}
+
+/* Predictive log-likelihood of test points for one (pis, mu, cov) sample
+ * (experiments/hmvgmm/hmvgmm.py:143-178, inner_ll):
+ * sum_n logsumexp_k (log N(y_n | mu_k, cov_k) + log pis[k]), with the
+ * normal log density of augur_mvnormal_ll (the correct one; scipy's logpdf
+ * in the experiment).  cov is [K][d][d], or one [d][d] when shared_cov. */
+double orc_gmm_pred_ll(int N, int d, int K, int shared_cov, const double* Y, const double* pis,
+                       const double* mu, const double* cov) {
+  double* tmp = (double*)malloc(sizeof(double) * K);
+  double acc = 0.0;
+  for (int n = 0; n < N; n++) {
+    for (int k = 0; k < K; k++) {
+      const double* ck = shared_cov ? cov : cov + (size_t)k * d * d;
+      tmp[k] = orc_mvnormal_ll(Y + (size_t)n * d, mu + (size_t)k * d, ck, d) + log(pis[k]);
+    }
+    acc += orc_logsumexp(tmp, K);
+  }
+  free(tmp);
+  return acc;
 }

@@ -33,12 +33,18 @@ _ip = C.POINTER(C.c_int)
 _u32p = C.POINTER(C.c_uint32)
 
 
+# The reference checkout sits beside this repository unless REF_SRC names
+# its cbits directory.
+REF_SRC_DEFAULT = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "cbits")
+
+
 def build_oracle():
     """Compile the standalone oracle (and the reference build when the
     reference sources are present) with oracle/Makefile."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if os.path.isdir(os.environ.get("REF_SRC", "/root/reference/cbits")):
-        subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
+    ref_src = os.environ.get("REF_SRC", REF_SRC_DEFAULT)
+    if os.path.isdir(ref_src):
+        subprocess.check_call(["make", "-s", "-C", HERE, "ref", "REF_SRC=" + os.path.abspath(ref_src)])
 
 
 def available(kind):
@@ -149,6 +155,27 @@ class Oracle:
         f.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, C.c_uint64, C.c_uint32]
         f(K, V, dptr(beta), iptr(cnt_kw), dptr(out), seed, it)
         return out
+
+    def lda_ll_mod(self, doc_off, w, z, alpha, beta, theta, phi):
+        """The model log density augur_get_curr_ll returns for lda.rv."""
+        D, K = theta.shape
+        V = phi.shape[1]
+        f = self.fn("lda_ll_mod", C.c_double)
+        f.argtypes = [C.c_int] * 3 + [_ip, _ip, _ip, _dp, _dp, _dp, _dp]
+        c = np.ascontiguousarray
+        return f(D, K, V, iptr(c(doc_off, np.int32)), iptr(c(w, np.int32)), iptr(c(z, np.int32)),
+                 dptr(c(alpha, np.float64)), dptr(c(beta, np.float64)), dptr(c(theta, np.float64)),
+                 dptr(c(phi, np.float64)))
+
+    def lda_pred_ll(self, doc_off, w, theta, phi):
+        """Held-out log-likelihood of one theta sample (oracle only)."""
+        D, K = theta.shape
+        V = phi.shape[1]
+        f = self.fn("lda_pred_ll", C.c_double)
+        f.argtypes = [C.c_int] * 3 + [_ip, _ip, _dp, _dp]
+        c = np.ascontiguousarray
+        return f(D, K, V, iptr(c(doc_off, np.int32)), iptr(c(w, np.int32)), dptr(c(theta, np.float64)),
+                 dptr(c(phi, np.float64)))
 
     def lda_sweeps(self, doc_off, w, alpha, beta, theta, phi, z, seed, it0, n):
         D, K = theta.shape
@@ -355,6 +382,17 @@ def gmm_disc_z(o, g, pis, mu, cov, seed, it):
     return z
 
 
+def gmm_disc_z_subset(o, g, pis, mu, cov, idx, seed, it):
+    """Assignments of the points idx only, each from its own substream (the
+    values gmm_disc_z gives those points)."""
+    idx = np.ascontiguousarray(idx, np.int32)
+    z = np.zeros(len(idx), np.int32)
+    _gmm(o, "gmm_disc_z_subset", g, None, [_dp, _dp, _dp, _ip, C.c_int, _ip] + _S,
+         dptr(np.ascontiguousarray(pis, np.float64)), dptr(np.ascontiguousarray(mu, np.float64)),
+         dptr(np.ascontiguousarray(cov, np.float64)), iptr(idx), len(idx), iptr(z), seed, it)
+    return z
+
+
 def gmm_stats(o, g, z, mu):
     cnt = np.zeros(g.K, np.int32)
     s = np.zeros((g.K, g.d))
@@ -415,6 +453,23 @@ def gmm_ll_mu(o, g, muk, k, cov, z):
     return _gmm(o, "gmm_ll_mu", g, C.c_double, [_dp, C.c_int, _dp, _ip],
                 dptr(np.ascontiguousarray(muk, np.float64)), k, dptr(np.ascontiguousarray(cov, np.float64)),
                 iptr(np.ascontiguousarray(z, np.int32)))
+
+
+def gmm_ll_mod(o, g, pis, mu, cov, z):
+    """The model log density augur_get_curr_ll returns for hmvgmm.rv / mvgmm.rv."""
+    c = np.ascontiguousarray
+    return _gmm(o, "gmm_ll_mod", g, C.c_double, [_dp, _dp, _dp, _ip], dptr(c(pis, np.float64)),
+                dptr(c(mu, np.float64)), dptr(c(cov, np.float64)), iptr(c(z, np.int32)))
+
+
+def gmm_pred_ll(o, Y, pis, mu, cov, shared_cov=False):
+    """Test-point log-likelihood of one (pis, mu, cov) sample (oracle only)."""
+    c = np.ascontiguousarray
+    Y = c(Y, np.float64)
+    f = o.fn("gmm_pred_ll", C.c_double)
+    f.argtypes = [C.c_int] * 4 + [_dp, _dp, _dp, _dp]
+    return f(Y.shape[0], Y.shape[1], len(pis), int(shared_cov), dptr(Y), dptr(c(pis, np.float64)),
+             dptr(c(mu, np.float64)), dptr(c(cov, np.float64)))
 
 
 def mvnormal_ll(o, pt, mean, cov):

@@ -703,3 +703,83 @@ void ref_conj_scalar(int kind, int G, const int* off, const double* x, const dou
     }
   }
 }
+
+/* ------------------------------------------------------------------------
+ * ll_mod (the function augur_get_curr_ll returns, CgStInit.hs:597-602):
+ * the model's factors in model order, each the sum over its comprehension
+ * (CgLike.hs:128-147), with the reference's _ll functions.
+ * --------------------------------------------------------------------- */
+
+double ref_lda_ll_mod(int D, int K, int V, const int* doc_off, const int* w, const int* z,
+                      const double* alpha, const double* beta, const double* theta, const double* phi) {
+  AugurVec_t va = dvec((double*)alpha, K), vb = dvec((double*)beta, V);
+  double ll = 0.0, s = 0.0;
+  for (int d = 0; d < D; d++) {
+    AugurVec_t th = dvec((double*)theta + (size_t)d * K, K);
+    s += augur_dirichlet_ll(&th, &va);
+  }
+  ll += s;
+  s = 0.0;
+  for (int k = 0; k < K; k++) {
+    AugurVec_t ph = dvec((double*)phi + (size_t)k * V, V);
+    s += augur_dirichlet_ll(&ph, &vb);
+  }
+  ll += s;
+  s = 0.0;
+  for (int d = 0; d < D; d++) {
+    AugurVec_t th = dvec((double*)theta + (size_t)d * K, K);
+    for (int t = doc_off[d]; t < doc_off[d + 1]; t++) s += augur_categorical_ll(z[t], &th);
+  }
+  ll += s;
+  s = 0.0;
+  for (int d = 0; d < D; d++)
+    for (int t = doc_off[d]; t < doc_off[d + 1]; t++) {
+      AugurVec_t ph = dvec((double*)phi + (size_t)z[t] * V, V);
+      s += augur_categorical_ll(w[t], &ph);
+    }
+  ll += s;
+  return ll;
+}
+
+double ref_gmm_ll_mod(const ref_gmm_t* g, const double* pis, const double* mu, const double* cov, const int* z) {
+  const int d = g->d, K = g->K;
+  double* Lb = (double*)malloc(sizeof(double) * d * d);
+  double* Wb = (double*)malloc(sizeof(double) * d * d);
+  double* wb = (double*)malloc(sizeof(double) * d);
+  AugurMat_t L = dmat(Lb, d), W = dmat(Wb, d);
+  AugurVec_t work = dvec(wb, d);
+  AugurVec_t vpis = dvec((double*)pis, K), mu0 = dvec((double*)g->mu0, d);
+  AugurMat_t cov0 = dmat((double*)g->cov0, d);
+  double ll = 0.0, s = 0.0;
+  if (!g->shared_cov) {
+    AugurVec_t va = dvec((double*)g->alpha, K);
+    ll += augur_dirichlet_ll(&vpis, &va);
+  }
+  for (int k = 0; k < K; k++) {
+    AugurVec_t mk = dvec((double*)mu + (size_t)k * d, d);
+    s += augur_mvnormal_ll(&mk, &mu0, &cov0, &L, &work);
+  }
+  ll += s;
+  s = 0.0;
+  if (!g->shared_cov) {
+    AugurMat_t sc = dmat((double*)g->scale0, d);
+    for (int k = 0; k < K; k++) {
+      AugurMat_t ck = dmat((double*)cov + (size_t)k * d * d, d);
+      s += augur_invwishart_ll(&ck, g->df, &sc, &L, &W);
+    }
+    ll += s;
+    s = 0.0;
+  }
+  for (int n = 0; n < g->N; n++) s += augur_categorical_ll(z[n], &vpis);
+  ll += s;
+  s = 0.0;
+  for (int n = 0; n < g->N; n++) {
+    AugurVec_t y = dvec((double*)g->Y + (size_t)n * d, d);
+    AugurVec_t mk = dvec((double*)mu + (size_t)z[n] * d, d);
+    AugurMat_t ck = dmat((double*)(g->shared_cov ? cov : cov + (size_t)z[n] * d * d), d);
+    s += augur_mvnormal_ll(&y, &mk, &ck, &L, &work);
+  }
+  ll += s;
+  free(Lb); free(Wb); free(wb);
+  return ll;
+}

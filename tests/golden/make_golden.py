@@ -1,7 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference sources (default /root/reference,
-override with REF_ROOT):  python tests/golden/make_golden.py
+Run in a checkout that has the reference sources (by default the reference
+checkout beside this repository, override with REF_ROOT):
+python tests/golden/make_golden.py
 
 * The reference's runtime (cbits) is compiled in place with the GSL shim and
   the restated generated code (oracle/Makefile `ref`) and executed through
@@ -20,7 +21,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("REF_ROOT", os.path.join(os.path.dirname(ROOT), "reference"))
 
 from oracle import oracle as O  # noqa: E402
 

@@ -230,6 +230,16 @@ def test_gmm_oracle_vs_reference_live(orc, ref):
     np.testing.assert_array_equal(O.gmm_eslice(orc, m, mus, covs, z, 8, 2), O.gmm_eslice(ref, m, mus, covs, z, 8, 2))
 
 
+def test_gmm_disc_z_subset_equals_full_pass(orc):
+    """The subset draw gives each listed point the value of the full pass
+    (same substream per point), in the order listed."""
+    Y, z, mus, covs, pis = O.gmm_synthetic(400, 5, 6, seed=4)
+    m = O.GmmModel(Y, 5, np.zeros(6), 9 * np.eye(6), False, alpha=np.ones(5), df=8, scale0=np.eye(6))
+    full = O.gmm_disc_z(orc, m, pis, mus, covs, 6, 3)
+    idx = np.array([399, 0, 7, 7, 123, 250], np.int32)
+    np.testing.assert_array_equal(O.gmm_disc_z_subset(orc, m, pis, mus, covs, idx, 6, 3), full[idx])
+
+
 def test_mvnormal_ll_matches_scipy(orc):
     from scipy.stats import multivariate_normal
     rng = np.random.default_rng(0)
@@ -270,3 +280,69 @@ def test_conj_scalar_live(orc, ref, kind):
         b = ref.conj_scalar(kind, off, x, h0, h1, h2, aux=aux, seed=seed, it=it)
         for u, v in zip(a, b):
             np.testing.assert_array_equal(u, v)
+
+
+def test_ll_mod_oracle_vs_reference_live(orc, ref):
+    """The model log density (augur_get_curr_ll's ll_mod) of the restatement
+    equals the reference runtime's, LDA and both mixture models."""
+    from augurv2_b200.lda import synthetic_corpus
+    K, V, D = 5, 40, 12
+    off, w = synthetic_corpus(K, V, D, 20, 0.3, 0.1, seed=2)
+    rng = np.random.default_rng(2)
+    theta = rng.dirichlet(np.full(K, 0.5), size=D)
+    phi = rng.dirichlet(np.full(V, 0.2), size=K)
+    z = rng.integers(0, K, size=len(w)).astype(np.int32)
+    alpha, beta = np.full(K, 0.3), np.full(V, 0.1)
+    a = orc.lda_ll_mod(off, w, z, alpha, beta, theta, phi)
+    assert a == ref.lda_ll_mod(off, w, z, alpha, beta, theta, phi)
+    doc = np.repeat(np.arange(D), np.diff(off))
+    expect = ((alpha - 1) * np.log(theta)).sum() + ((beta - 1) * np.log(phi)).sum() + \
+        np.log(theta[doc, z]).sum() + np.log(phi[z, w]).sum()
+    assert abs(a - expect) <= 1e-10 * abs(expect)
+    Y, zg, mus, covs, pis = O.gmm_synthetic(200, 3, 4, seed=5)
+    for shared in (False, True):
+        m = O.GmmModel(Y, 3, np.zeros(4), 9 * np.eye(4), shared, alpha=np.full(3, 2.0), df=7,
+                       scale0=2 * np.eye(4))
+        cv = covs[0] if shared else covs
+        assert O.gmm_ll_mod(orc, m, pis, mus, cv, zg) == O.gmm_ll_mod(ref, m, pis, mus, cv, zg)
+
+
+def test_invwishart_ll_against_scipy(orc):
+    """The reference's inverse-Wishart log density equals scipy's up to its
+    log(3.1415) in the multivariate gamma (augur_math.c:80-86)."""
+    from scipy.stats import invwishart
+    from scipy.special import multigammaln
+    d, df = 4, 7
+    Y, zg, mus, covs, pis = O.gmm_synthetic(10, 1, d, seed=1)
+    m = O.GmmModel(Y, 1, np.zeros(d), np.eye(d), False, alpha=np.ones(1), df=df, scale0=2 * np.eye(d))
+    got = O.gmm_ll_mod(orc, m, np.ones(1), np.zeros((1, d)), covs, np.zeros(10, np.int32))
+    rest = O.mvnormal_ll(orc, np.zeros(d), np.zeros(d), np.eye(d)) + sum(
+        O.mvnormal_ll(orc, Y[n], np.zeros(d), covs[0]) for n in range(10))
+    quirk = d * (d - 1) / 4 * (np.log(np.pi) - np.log(3.1415))
+    expect = invwishart(df=df, scale=2 * np.eye(d)).logpdf(covs[0]) + quirk
+    np.testing.assert_allclose(got - rest, expect, rtol=1e-10)
+    assert abs(multigammaln(3.5, d) - (d * (d - 1) / 4 * np.log(np.pi) + sum(
+        __import__("math").lgamma(3.5 - i / 2) for i in range(d)))) < 1e-10
+
+
+def test_predictive_ll_against_scipy(orc):
+    """Held-out log-likelihoods (experiments/lda/lda.py:149-173,
+    experiments/hmvgmm/hmvgmm.py:143-178) against scipy's logsumexp and
+    multivariate normal."""
+    from scipy.special import logsumexp
+    from scipy.stats import multivariate_normal as mvn
+    rng = np.random.default_rng(7)
+    K, V, D = 6, 30, 9
+    off = np.concatenate([[0], np.cumsum(rng.integers(0, 8, size=D))]).astype(np.int32)
+    w = rng.integers(0, V, size=off[-1]).astype(np.int32)
+    theta = rng.dirichlet(np.full(K, 0.5), size=D)
+    phi = rng.dirichlet(np.full(V, 0.3), size=K)
+    doc = np.repeat(np.arange(D), np.diff(off))
+    expect = logsumexp(np.log(theta[doc]) + np.log(phi[:, w].T), axis=1).sum()
+    np.testing.assert_allclose(orc.lda_pred_ll(off, w, theta, phi), expect, rtol=1e-12)
+    Y, zg, mus, covs, pis = O.gmm_synthetic(150, 4, 3, seed=3)
+    lp = np.stack([mvn(mus[k], covs[k]).logpdf(Y) + np.log(pis[k]) for k in range(4)], 1)
+    np.testing.assert_allclose(O.gmm_pred_ll(orc, Y, pis, mus, covs), logsumexp(lp, axis=1).sum(), rtol=1e-10)
+    lp = np.stack([mvn(mus[k], covs[0]).logpdf(Y) + np.log(pis[k]) for k in range(4)], 1)
+    np.testing.assert_allclose(O.gmm_pred_ll(orc, Y, pis, mus, covs[0], shared_cov=True),
+                               logsumexp(lp, axis=1).sum(), rtol=1e-10)

@@ -37,8 +37,9 @@ def test_noalloc_matches_caller_scratch_twice():
                                           N.stream_ptr()), "ab_lda_conj_phi_noalloc")
         torch.cuda.synchronize()
         a, b = out_a.cpu().numpy()[:, :K], out_b.cpu().numpy()[:, :K]
-        np.testing.assert_allclose(b, a, rtol=RTOL, atol=0)
-        np.testing.assert_allclose(b.sum(0), 1.0, rtol=1e-12)
+        # same kernels, same seed and counts: identical bits
+        assert np.array_equal(b, a)
+        np.testing.assert_allclose(b.sum(0), 1.0, rtol=RTOL)
         assert (cnt2.cpu().numpy() == 0).all()
 
 
@@ -46,8 +47,7 @@ def test_noalloc_rejects_sizes_beyond_the_builtin_scratch():
     L = N.lib()
     K, V = 1024, 300000          # needs about 9.6 MB of scratch
     assert L.ab_lda_phi_scratch_bytes(K, V) > (1 << 20)
-    rc = L.ab_lda_conj_phi_noalloc(K, V, None, None, None, 0, 0, 0, None)
-    assert rc == 1
+    # valid pointers, so the refusal comes from the scratch-size check
     rc = L.ab_lda_conj_phi_noalloc(K, V, N.ptr(torch.zeros(1, device="cuda", dtype=torch.float64)),
                                    N.ptr(torch.zeros(1, device="cuda", dtype=torch.int32)),
                                    N.ptr(torch.zeros(1, device="cuda", dtype=torch.float64)), 0, 0, 0,
