@@ -59,7 +59,7 @@ class LdaDesc(C.Structure):
     _fields_ = [("D", i32), ("K", i32), ("V", i32),
                 ("doc_off", vp), ("w", vp), ("alpha", vp), ("beta", vp),
                 ("z", vp), ("theta", vp), ("phiT", vp), ("cnt_dk", vp), ("cnt_kw", vp),
-                ("scratch", vp), ("seed", u64), ("T", i32)]
+                ("scratch", vp), ("seed", u64)]
 
 
 _dp, _ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
@@ -101,7 +101,9 @@ _SIGS = {
     "ab_lda_conj_phi": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp, vp]),
     "ab_lda_conj_phi_noalloc": (i32, [i32, i32, vp, vp, vp, i32, u64, u32, vp]),
     "ab_lda_disc_z": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
-    "ab_lda_scratch_bytes": (sz, [i32, i32, i32]),
+    "ab_lda_scratch_bytes": (sz, [i32, i32]),
+    "ab_lda_phi32_stride": (i32, [i32]),
+    "ab_lda_disc_z_f32": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, u64, u32, vp]),
     "ab_lda_create": (i32, [C.POINTER(LdaDesc), C.POINTER(vp)]),
     "ab_lda_init_state": (i32, [vp, u32, vp]),
     "ab_lda_run": (i32, [vp, i32, i32, vp]),

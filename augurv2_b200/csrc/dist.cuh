@@ -38,35 +38,6 @@ __device__ __forceinline__ double gamma_ge1(Stream& s, double alpha) {
   return __dmul_rn(d, 1.0);  // unreachable in practice (acceptance > 95%)
 }
 
-// The first try of gamma_draw's Marsaglia-Tsang loop and, for a boosted
-// shape, its boost (substream positions 0, 1 and 2), decided by the squeeze
-// alone.  Returns true with the draw gamma_draw would return when that try
-// accepts by the squeeze (about 95% of draws at the shapes of the Gibbs
-// samplers); returns false otherwise - a rejected try, or one that needs the
-// logarithmic test - and the caller runs gamma_draw from the start of the
-// substream.  Kernels use it to run every lane's first try together and to
-// collect the few remaining draws into dense warps, instead of letting each
-// warp wait for its slowest lane's rejection loop.
-__device__ __forceinline__ bool gamma_first_try(Stream& s, double shape, double rate, double& out) {
-  const bool boost = shape < 1.0;
-  const double a = boost ? __dadd_rn(shape, 1.0) : shape;
-  const double d = __dadd_rn(a, -1.0 / 3.0);
-  const double c = 1.0 / sqrt(__dmul_rn(9.0, d));
-  const double z = s.normal();
-  const double u = s.uniform();
-  const double t = __dadd_rn(1.0, __dmul_rn(c, z));
-  const double V = __dmul_rn(__dmul_rn(t, t), t);
-  const double z2 = __dmul_rn(z, z);
-  if (!(z > -1.0 / c) || !(u < __dadd_rn(1.0, -__dmul_rn(0.0331, __dmul_rn(z2, z2))))) return false;
-  double x = __dmul_rn(d, V);
-  if (boost) {
-    const double ub = s.uniform();
-    x = __dmul_rn(x, pow(ub, 1.0 / shape));
-  }
-  out = __dmul_rn(x, 1.0 / rate);
-  return true;
-}
-
 // cbits/augur_dist.c:302-312: boost shape < 1 through Gamma(shape + 1).
 // The rejection loop is written once for both cases (its shape argument
 // selected first), so that a warp whose lanes mix shapes below and above 1

@@ -40,50 +40,10 @@ namespace ab {
 
 constexpr int LDA_THREADS = 256;
 constexpr int LDA_MAX_K = 1024;
+constexpr int LDA_PHI_MAX_B = 512;   // phi draw CTAs per topic whose partials are staged in shared memory
 
 __device__ __forceinline__ uint32_t read_iter(const uint32_t* iter_dev, uint32_t iter_fixed) {
   return iter_dev ? *(volatile const uint32_t*)iter_dev : iter_fixed;
-}
-
-// ---------------------------------------------------------------------------
-// Gamma draws of one CTA with the rejection loops compacted: every thread
-// makes its cell's first Marsaglia-Tsang try (gamma_first_try, which decides
-// about 95% of draws by the squeeze); the cells it does not decide are queued
-// in shared memory and drawn afterwards by the first threads of the CTA, one
-// cell each, with the full sampler from the start of the cell's substream.
-// The draws are those of gamma_draw(make_stream(seed, elem, iter, tag),
-// shape, 1) for every cell; only the work is regrouped, so that a warp no
-// longer runs as many loop iterations as its slowest lane needs.
-// q, qshape, qelem, qout (blockDim.x entries each) and qn are shared memory;
-// the return value is the draw of the thread's own cell (when has_cell).
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double gamma_draw_compacted(bool has_cell, double shape, uint32_t elem,
-                                                       uint64_t seed, uint32_t iter, uint32_t tag,
-                                                       int* q, double* qshape, uint32_t* qelem,
-                                                       double* qout, int* qn) {
-  if (threadIdx.x == 0) *qn = 0;
-  __syncthreads();
-  double g = 0.0;
-  bool queued = false;
-  if (has_cell) {
-    Stream s = make_stream(seed, elem, iter, tag);
-    if (!gamma_first_try(s, shape, 1.0, g)) {
-      const int slot = atomicAdd(qn, 1);
-      q[slot] = threadIdx.x;
-      qshape[slot] = shape;
-      qelem[slot] = elem;
-      queued = true;
-    }
-  }
-  __syncthreads();
-  const int n = *qn;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    Stream s = make_stream(seed, qelem[i], iter, tag);
-    qout[q[i]] = gamma_draw(s, qshape[i], 1.0);
-  }
-  __syncthreads();
-  if (queued) g = qout[threadIdx.x];
-  return g;
 }
 
 // ---------------------------------------------------------------------------
@@ -91,32 +51,25 @@ __device__ __forceinline__ double gamma_draw_compacted(bool has_cell, double sha
 // (augur_dirichlet_categorical_conj, cbits/augur_dist.c:526-538).  The row
 // sum is taken sequentially over k by one thread, as the reference does, so
 // theta is bit-identical to the reference given identical gamma draws.
-// Block: R = 256 / K rows of K cells, one cell per thread (K <= 256), or one
-// row looped over when K > 256.
+// Block: R = 256 / K rows (or one row looped when K > 256).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(LDA_THREADS, 4)
 lda_theta_kernel(int D, int K, const double* __restrict__ alpha,
                  const int* __restrict__ cnt_dk, double* __restrict__ theta,
                  uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
   extern __shared__ double sg[];  // [rows_per_block][K] gamma draws, then [rows] sums
-  __shared__ int q[LDA_THREADS];
-  __shared__ double qshape[LDA_THREADS], qout[LDA_THREADS];
-  __shared__ uint32_t qelem[LDA_THREADS];
-  __shared__ int qn;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
   const int rows = K <= LDA_THREADS ? LDA_THREADS / K : 1;
   const int row0 = blockIdx.x * rows;
   double* sums = sg + rows * K;
-  for (int e0 = 0; e0 < rows * K; e0 += blockDim.x) {     // one pass when K <= 256
-    const int e = e0 + threadIdx.x;
+  for (int e = threadIdx.x; e < rows * K; e += blockDim.x) {
     const int r = e / K, k = e - r * K;
     const int d = row0 + r;
-    const bool has = e < rows * K && d < D;
-    const size_t idx = (size_t)d * K + k;
-    const double shape = has ? __dadd_rn(alpha[k], (double)cnt_dk[idx]) : 1.0;
-    const double g = gamma_draw_compacted(has, shape, (uint32_t)idx, seed, iter, TAG_THETA, q, qshape, qelem,
-                                          qout, &qn);
-    if (has) sg[e] = g;
+    if (d < D) {
+      const size_t idx = (size_t)d * K + k;
+      Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_THETA);
+      sg[e] = gamma_draw(s, __dadd_rn(alpha[k], (double)cnt_dk[idx]), 1.0);
+    }
   }
   __syncthreads();
   if (threadIdx.x < rows && row0 + (int)threadIdx.x < D) {
@@ -153,35 +106,42 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
                     double* __restrict__ nrm, uint64_t seed, const uint32_t* iter_dev,
                     uint32_t iter_fixed) {
   __shared__ double red[33];
-  __shared__ int q[LDA_THREADS];
-  __shared__ double qshape[LDA_THREADS], qout[LDA_THREADS];
-  __shared__ uint32_t qelem[LDA_THREADS];
-  __shared__ int qn;
+  __shared__ double part_s[LDA_PHI_MAX_B];
+  __shared__ int last;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
   const int k = blockIdx.x / B;
   const int b = blockIdx.x - k * B;
   const int v = b * LDA_THREADS + threadIdx.x;
-  const bool has = v < V;
-  const size_t idx = (size_t)k * V + v;
-  double shape = 1.0;
-  if (has) {
+  double g = 0.0;
+  if (v < V) {
+    const size_t idx = (size_t)k * V + v;
     const int c = cnt_kw[idx];
     if (clear_counts) cnt_kw[idx] = 0;
-    shape = __dadd_rn(beta[v], (double)c);
+    Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
+    g = gamma_draw(s, __dadd_rn(beta[v], (double)c), 1.0);
+    phiT[(size_t)v * Kp + k] = g;
   }
-  const double g = gamma_draw_compacted(has, shape, (uint32_t)idx, seed, iter, TAG_PHI, q, qshape, qelem,
-                                        qout, &qn);
-  if (has) phiT[(size_t)v * Kp + k] = g;
   const double bsum = block_sum_f64(g, red);
   // The last CTA of topic k (atomic ticket) adds the topic's B partials in
-  // CTA order and publishes the normaliser.
+  // CTA order and publishes the normaliser.  Its threads first load the B
+  // partials together (one L2 round trip instead of B dependent ones); the
+  // additions stay sequential, in CTA order.
   if (threadIdx.x == 0) {
     partial[(size_t)k * B + b] = bsum;
     __threadfence();
-    if (atomicAdd(ticket + k, 1u) == (unsigned)(B - 1)) {
-      __threadfence();
+    last = atomicAdd(ticket + k, 1u) == (unsigned)(B - 1);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    const double* pk = partial + (size_t)k * B;
+    if (B <= LDA_PHI_MAX_B) {
+      for (int i = threadIdx.x; i < B; i += blockDim.x) part_s[i] = __ldcg(pk + i);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
       double acc = 0.0;
-      for (int i = 0; i < B; ++i) acc = __dadd_rn(acc, __ldcg(partial + (size_t)k * B + i));
+      for (int i = 0; i < B; ++i) acc = __dadd_rn(acc, B <= LDA_PHI_MAX_B ? part_s[i] : __ldcg(pk + i));
       nrm[k] = acc;
       ticket[k] = 0u;
     }
@@ -190,9 +150,12 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
 
 // phiT [V][Kp] as V * Kp / 2 pairs of doubles; pair j holds topics 2j mod Kp
 // and the next one.  Padding topics (k >= K) are left untouched (zero).
+// When phi32 is given, the normalised values are also stored rounded to
+// binary32 in phi32 [V][Kq] (the z kernel's screening copy; its padding
+// columns are left untouched and must be zero).
 __global__ void __launch_bounds__(LDA_THREADS)
 lda_phi_norm_kernel(int K, int V, int Kp, const double* __restrict__ nrm_g,
-                    double* __restrict__ phiT) {
+                    double* __restrict__ phiT, float* __restrict__ phi32, int Kq) {
   extern __shared__ double nrm[];   // [K]
   for (int k = threadIdx.x; k < K; k += blockDim.x) nrm[k] = nrm_g[k];
   __syncthreads();
@@ -206,10 +169,19 @@ lda_phi_norm_kernel(int K, int V, int Kp, const double* __restrict__ nrm_g,
     x.x = __ddiv_rn(x.x, nrm[k]);
     if (k + 1 < K) x.y = __ddiv_rn(x.y, nrm[k + 1]);
     p2[j] = x;
+    if (phi32 != nullptr) {
+      const size_t v = j / half_kp;
+      float2 f = make_float2(__double2float_rn(x.x), k + 1 < K ? __double2float_rn(x.y) : 0.0f);
+      *reinterpret_cast<float2*>(phi32 + v * Kq + k) = f;
+    }
   }
 }
 
 static inline int lda_phi_blocks(int V) { return (V + LDA_THREADS - 1) / LDA_THREADS; }
+
+// Row stride (floats) of the binary32 screening copy of phi: a multiple of 8,
+// so that each half row is whole 16-byte units.
+static inline int lda_kq(int K) { return (K + 7) & ~7; }
 
 // ---------------------------------------------------------------------------
 // z[t] for every token of document d, K > 64 (one CTA per document; the
@@ -421,8 +393,6 @@ __device__ __noinline__ int lda_reference_draw(int K, const double* __restrict__
 // reference's; a u within m of a boundary (or a zero, subnormal, infinite or
 // NaN norm) runs the reference's loop itself (lda_reference_draw).  theta
 // and phi are probabilities (nonnegative), which keeps c_k monotone.
-// The token's uniform is read from u_pre (drawn ahead by lda_zu_kernel) when
-// given, else drawn here from the token's substream.
 // Counts of the new z: the document's row of cnt_dk is accumulated in shared
 // memory and stored whole; cnt_kw, when given, receives one atomic increment
 // per token.
@@ -437,14 +407,14 @@ template <int NQ>
 __global__ void __launch_bounds__(LDA_Z_THREADS, 8)
 lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
               const int* __restrict__ w, const double* __restrict__ theta,
-              const double* __restrict__ phiT, const double* __restrict__ u_pre,
-              int* __restrict__ z, int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
+              const double* __restrict__ phiT, int* __restrict__ z, int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
               uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
   constexpr int KP = 4 * NQ;          // row length in doubles (= the phiT stride)
   constexpr int H2 = 2 * NQ;          // row length in 16-byte units
   constexpr int HK = 2 * NQ;          // topics per half row
   constexpr int P2 = H2 + 1;          // row pitch in 16-byte units (odd)
-  constexpr int STEP0 = HK > 16 ? 16 : (HK > 8 ? 8 : (HK > 4 ? 4 : (HK > 2 ? 2 : 1)));
+  // largest power of two <= HK: the search can return every count 0..HK
+  constexpr int STEP0 = HK >= 32 ? 32 : (HK >= 16 ? 16 : (HK >= 8 ? 8 : (HK >= 4 ? 4 : (HK >= 2 ? 2 : 1))));
   extern __shared__ double2 smem2[];
   double2* th2 = smem2;                                        // [H2] theta, zero padded
   int* hist = reinterpret_cast<int*>(smem2 + H2);              // [KP]
@@ -486,15 +456,11 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
     double u = 0.0;
-    if (u_pre != nullptr) {
-      if (active) u = u_pre[t];
-    } else {
-      if (active && half == 0) {
-        Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
-        u = s.uniform();
-      }
-      u = __shfl_sync(0xffffffffu, u, j);
+    if (active && half == 0) {
+      Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+      u = s.uniform();
     }
+    u = __shfl_sync(0xffffffffu, u, j);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncwarp();
     // running sum of this lane's half row, written back over it
@@ -564,27 +530,189 @@ lda_zq_kernel(int D, int K, int V, const int* __restrict__ doc_off,
 
 template <int NQ>
 static int launch_lda_zq(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
-                         const double* phiT, const double* u_pre, int* z, int* cnt_dk, int* cnt_kw,
-                         uint64_t seed, uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr,
-                         cudaStream_t st) {
+                         const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                         uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
   const size_t smem = 16 * (size_t)(2 * NQ + NQ + (LDA_Z_THREADS / 32) * LDA_ZQ_ROWS * (2 * NQ + 1));
   AB_CUDA(cudaFuncSetAttribute(lda_zq_kernel<NQ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  lda_zq_kernel<NQ><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, doc_off, w, theta, phiT, u_pre, z, cnt_dk, cnt_kw,
-                                                    seed, iter_dev, iter, done_ctr);
+  lda_zq_kernel<NQ><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed,
+                                                    iter_dev, iter, done_ctr);
   AB_LAUNCH_CHECK("lda_zq_kernel");
   return AB_OK;
 }
 
-// The uniforms of every token's draw (substream (t, iter, TAG_Z), position
-// 0), ahead of the z kernel: drawn on the theta branch of a sweep, which runs
-// beside the phi draw, so the z kernel on the critical path reads them.
-__global__ void __launch_bounds__(LDA_THREADS)
-lda_zu_kernel(int T, double* __restrict__ u_z, uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+// ---------------------------------------------------------------------------
+// The z draw screened in binary32 (K <= 64; NH = Kq / 8 16-byte units per
+// half row, Kq = lda_kq(K)).  Same structure as lda_zq_kernel - one CTA per
+// document, 16 tokens per warp chunk, two lanes per token (lane j: topics
+// [0, 4 NH), lane j + 16: [4 NH, 8 NH)), the chunk's rows staged in shared
+// memory by cp.async with an odd row pitch - but the staged rows are the
+// binary32 copy phi32 = fl32(phi) (Kq floats: 224 bytes at K = 50 against 416
+// for the binary64 rows) and the products and running sums are binary32.
+//
+// Why a decided draw is still the reference's: every theta_k, phi_k is
+// rounded once to binary32 (relative error <= u = 2^-24), each product once
+// more, and a running sum of nonnegative terms (grouped as two halves) adds
+// at most (k + 1) u relative error, so each screened running sum c_k and the
+// norm are within (K + 8) u of the exact sums C_k and N; u * norm adds 3 u.
+// Gradual underflow adds at most 2^-149 per term, below 2^-60 u of a norm
+// >= 2^-60.  The reference's running quotient sums acc_i are within 2^-50 of
+// C_i / N.  So with m = (2K + 32) u: if c_j (1 + m) < u norm for all j < k the
+// reference does not stop before k, and if also u norm < c_k (1 - m) it stops
+// at k - the draw equals the reference's.  A u within the margin of a
+// boundary (about 2 (2K + 32) u of the draws, 1e-5 at K = 50), or a norm
+// outside [2^-60, FLT_MAX], runs the reference's binary64 loop on the binary64
+// theta and phi rows (lda_reference_draw).  Counts as lda_zq_kernel.
+// ---------------------------------------------------------------------------
+template <int NH>
+__global__ void __launch_bounds__(LDA_Z_THREADS, 10)
+lda_zf_kernel(int D, int K, int V, int Kp, const int* __restrict__ doc_off,
+              const int* __restrict__ w, const double* __restrict__ theta,
+              const double* __restrict__ phiT, const float* __restrict__ phi32,
+              int* __restrict__ z, int* __restrict__ cnt_dk, int* __restrict__ cnt_kw, uint64_t seed,
+              uint32_t* iter_dev, uint32_t iter_fixed, uint32_t* done_ctr) {
+  constexpr int KQ = 8 * NH;          // row length in floats (= the phi32 stride)
+  constexpr int RU = 2 * NH;          // row length in 16-byte units
+  constexpr int HK = 4 * NH;          // topics per half row
+  constexpr int P2 = RU + 1;          // row pitch in 16-byte units (odd)
+  // largest power of two <= HK: the search can return every count 0..HK
+  constexpr int STEP0 = HK >= 32 ? 32 : (HK >= 16 ? 16 : (HK >= 8 ? 8 : 4));
+  extern __shared__ float4 smem4[];
+  float4* th4 = smem4;                                           // [RU] theta in binary32, zero padded
+  int* hist = reinterpret_cast<int*>(smem4 + RU);                // [KQ]
+  double* th64 = reinterpret_cast<double*>(smem4 + 2 * RU);      // [KQ] theta in binary64 (fallback)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int j = lane & 15, half = lane >> 4;
+  float4* stage = smem4 + 2 * RU + 2 * RU + warp * LDA_ZQ_ROWS * P2;   // [LDA_ZQ_ROWS][P2]
+  const int d = blockIdx.x;
   const uint32_t iter = read_iter(iter_dev, iter_fixed);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
-    Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
-    u_z[t] = s.uniform();
+  float* th32 = reinterpret_cast<float*>(th4);
+  for (int k = threadIdx.x; k < KQ; k += blockDim.x) {
+    const double t = k < K ? theta[(size_t)d * K + k] : 0.0;
+    th64[k] = t;
+    th32[k] = __double2float_rn(t);
+    hist[k] = 0;
   }
+  __syncthreads();
+  const int t0 = doc_off[d], t1 = doc_off[d + 1];
+  const float m = (float)(2 * K + 32) * 5.9604644775390625e-8f;
+  const float lo = 1.0f - m, hi = 1.0f + m;
+  const float4* __restrict__ phi4 = reinterpret_cast<const float4*>(phi32);
+  const int n_half = min(max(K - 1 - half * HK, 0), HK);
+  constexpr int STRIDE = (LDA_Z_THREADS / 32) * LDA_ZQ_ROWS;
+  int w_next = (lane < LDA_ZQ_ROWS && t0 + warp * LDA_ZQ_ROWS + lane < t1) ? w[t0 + warp * LDA_ZQ_ROWS + lane] : 0;
+  for (int tb = t0 + warp * LDA_ZQ_ROWS; tb < t1; tb += STRIDE) {
+    const int t = tb + j;
+    const bool active = t < t1;
+    const int wt = w_next;
+    w_next = (lane < LDA_ZQ_ROWS && tb + lane + STRIDE < t1) ? w[tb + lane + STRIDE] : 0;
+    const int nrow = min(LDA_ZQ_ROWS, t1 - tb);
+    // two rows per copy instruction: lanes 0-15 row 2r, lanes 16-31 row 2r+1
+#pragma unroll
+    for (int r = 0; r < LDA_ZQ_ROWS / 2; ++r) {
+      const int row = 2 * r + half;
+      const int wr = __shfl_sync(0xffffffffu, wt, row);
+      if (row < nrow && j < RU) {
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(stage + row * P2 + j);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst),
+                     "l"(phi4 + (size_t)wr * RU + j) : "memory");
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    double u = 0.0;
+    if (active && half == 0) {
+      Stream s = make_stream(seed, (uint32_t)t, iter, TAG_Z);
+      u = s.uniform();
+    }
+    u = __shfl_sync(0xffffffffu, u, j);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncwarp();
+    float4* row = stage + j * P2 + half * NH;
+    const float4* thh = th4 + half * NH;
+    float c = 0.0f;
+    if (active) {
+#pragma unroll
+      for (int q = 0; q < NH; ++q) {
+        const float4 f = row[q], g = thh[q];
+        const float c0 = __fadd_rn(c, __fmul_rn(g.x, f.x));
+        const float c1 = __fadd_rn(c0, __fmul_rn(g.y, f.y));
+        const float c2 = __fadd_rn(c1, __fmul_rn(g.z, f.z));
+        c = __fadd_rn(c2, __fmul_rn(g.w, f.w));
+        row[q] = make_float4(c0, c1, c2, c);
+      }
+    }
+    const float A = __shfl_sync(0xffffffffu, c, j);
+    const float S = __shfl_sync(0xffffffffu, c, j + 16);
+    const float norm = __fadd_rn(A, S);
+    const float off = half ? A : 0.0f;
+    const float un = __fmul_rn(__double2float_rn(u), norm);
+    const float* cs = reinterpret_cast<const float*>(row);
+    int pos = 0;
+#pragma unroll
+    for (int step = STEP0; step >= 1; step >>= 1)
+      if (pos + step <= n_half && __fmul_rn(__fadd_rn(off, cs[pos + step - 1]), hi) < un) pos += step;
+    int cand = -1, dec = 0;
+    if (pos < n_half) {
+      cand = half * HK + pos;
+      dec = un < __fmul_rn(__fadd_rn(off, cs[pos]), lo);
+    }
+    const int cand1 = __shfl_sync(0xffffffffu, cand, j + 16);
+    const int dec1 = __shfl_sync(0xffffffffu, dec, j + 16);
+    if (active && half == 0) {
+      bool exact = !(norm >= 8.673617379884035e-19f && norm <= 3.4028234663852886e38f);   // [2^-60, FLT_MAX]
+      int zk = K - 1;
+      if (!exact) {
+        if (cand >= 0) { zk = cand; exact = !dec; }
+        else if (cand1 >= 0) { zk = cand1; exact = !dec1; }
+      }
+      if (exact) zk = lda_reference_draw(K, th64, phiT + (size_t)wt * Kp, u);
+      z[t] = zk;
+      atomicAdd(&hist[zk], 1);
+      if (cnt_kw != nullptr) atomicAdd(cnt_kw + (size_t)zk * V + wt, 1);
+    }
+    __syncwarp();   // the stage is rewritten by the next chunk
+  }
+  __syncthreads();
+  if (cnt_dk != nullptr)
+    for (int k = threadIdx.x; k < K; k += blockDim.x) cnt_dk[(size_t)d * K + k] = hist[k];
+  if (iter_dev != nullptr && done_ctr != nullptr) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(done_ctr, 1u);
+      if (prev == (unsigned)(D - 1)) {
+        *done_ctr = 0u;
+        *iter_dev = iter + 1u;
+        __threadfence();
+      }
+    }
+  }
+}
+
+template <int NH>
+static int launch_lda_zf_t(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
+                           const double* phiT, const float* phi32, int* z, int* cnt_dk, int* cnt_kw,
+                           uint64_t seed, uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr,
+                           cudaStream_t st) {
+  // theta32 [2NH] + hist [2NH] + theta64 [2 * 2NH] + stages, in 16-byte units
+  const size_t smem = 16 * (size_t)(2 * NH + 2 * NH + 2 * (2 * NH) + (LDA_Z_THREADS / 32) * LDA_ZQ_ROWS * (2 * NH + 1));
+  AB_CUDA(cudaFuncSetAttribute(lda_zf_kernel<NH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  lda_zf_kernel<NH><<<D, LDA_Z_THREADS, smem, st>>>(D, K, V, Kp, doc_off, w, theta, phiT, phi32, z, cnt_dk,
+                                                    cnt_kw, seed, iter_dev, iter, done_ctr);
+  AB_LAUNCH_CHECK("lda_zf_kernel");
+  return AB_OK;
+}
+
+int launch_lda_zf(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
+                  const double* phiT, const float* phi32, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
+  switch (lda_kq(K) / 8) {
+#define AB_ZF(nh) \
+  case nh: return launch_lda_zf_t<nh>(D, K, V, Kp, doc_off, w, theta, phiT, phi32, z, cnt_dk, cnt_kw, seed, iter_dev, iter, done_ctr, st);
+    AB_ZF(1) AB_ZF(2) AB_ZF(3) AB_ZF(4) AB_ZF(5) AB_ZF(6) AB_ZF(7) AB_ZF(8)
+#undef AB_ZF
+    default: break;
+  }
+  return fail(AB_ERR_ARG, "lda: the binary32-screened z kernel takes K <= 64 (K=%d)", K);
 }
 
 // Count statistics of a given z (conj_stat_theta / conj_stat_phi of
@@ -636,7 +764,7 @@ size_t lda_phi_scratch(int K, int V) {
 
 int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double* phiT, int clear,
                    void* scratch, uint64_t seed, const uint32_t* iter_dev, uint32_t iter,
-                   cudaStream_t st) {
+                   cudaStream_t st, float* phi32 = nullptr) {
   const int B = lda_phi_blocks(V);
   char* base = static_cast<char*>(scratch) + 256;
   uint32_t* ticket = reinterpret_cast<uint32_t*>(base);
@@ -647,20 +775,19 @@ int launch_lda_phi(int K, int V, int Kp, const double* beta, int* cnt_kw, double
   AB_LAUNCH_CHECK("lda_phi_draw_kernel");
   const size_t n2 = (size_t)V * (Kp / 2);
   const unsigned nb = (unsigned)std::min<size_t>((n2 + LDA_THREADS - 1) / LDA_THREADS, 148u * 8u);
-  lda_phi_norm_kernel<<<nb, LDA_THREADS, sizeof(double) * K, st>>>(K, V, Kp, nrm, phiT);
+  lda_phi_norm_kernel<<<nb, LDA_THREADS, sizeof(double) * K, st>>>(K, V, Kp, nrm, phiT, phi32,
+                                                                    lda_kq(K));
   AB_LAUNCH_CHECK("lda_phi_norm_kernel");
   return AB_OK;
 }
 
-// u_pre (the tokens' uniforms drawn ahead, or null) is used by the K <= 64
-// kernel; the kernel for larger K draws its uniforms itself.
 int launch_lda_z(int D, int K, int V, int Kp, const int* doc_off, const int* w, const double* theta,
-                 const double* phiT, const double* u_pre, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                 const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                  uint32_t* iter_dev, uint32_t iter, uint32_t* done_ctr, cudaStream_t st) {
 #define AB_ZQ(nq)                                                                                      \
   case nq:                                                                                             \
-    return launch_lda_zq<nq>(D, K, V, doc_off, w, theta, phiT, u_pre, z, cnt_dk, cnt_kw, seed, iter_dev, \
-                             iter, done_ctr, st);
+    return launch_lda_zq<nq>(D, K, V, doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, iter_dev, iter, \
+                             done_ctr, st);
   if (K <= LDA_ZQ_MAX_K) {
     switch (Kp / 4) {
       AB_ZQ(1) AB_ZQ(2) AB_ZQ(3) AB_ZQ(4) AB_ZQ(5) AB_ZQ(6) AB_ZQ(7) AB_ZQ(8)
@@ -737,8 +864,25 @@ extern "C" int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int*
   AB_REQUIRE((reinterpret_cast<uintptr_t>(phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_disc_z: phiT must be 16-byte aligned");
   AB_REQUIRE((cnt_dk == nullptr) == (cnt_kw == nullptr), AB_ERR_ARG,
              "ab_lda_disc_z: pass both count tables or neither");
-  return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, nullptr, z, cnt_dk, cnt_kw, seed,
-                      nullptr, iter, nullptr, as_stream(stream));
+  return launch_lda_z(D, K, V, lda_kp(K), doc_off, w, theta, phiT, z, cnt_dk, cnt_kw, seed, nullptr, iter,
+                      nullptr, as_stream(stream));
+}
+
+extern "C" int ab_lda_phi32_stride(int K) { return lda_kq(K); }
+
+extern "C" int ab_lda_disc_z_f32(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                                 const double* phiT, const float* phi32, int* z, int* cnt_dk, int* cnt_kw,
+                                 uint64_t seed, uint32_t iter, void* stream) {
+  int rc = check_lda_dims(D, K, V);
+  if (rc) return rc;
+  AB_REQUIRE(K <= LDA_ZQ_MAX_K, AB_ERR_ARG, "ab_lda_disc_z_f32: K <= %d (got %d)", LDA_ZQ_MAX_K, K);
+  AB_REQUIRE(doc_off && w && theta && phiT && phi32 && z, AB_ERR_ARG, "ab_lda_disc_z_f32: null pointer");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(phi32) & 15) == 0, AB_ERR_ARG,
+             "ab_lda_disc_z_f32: phi32 must be 16-byte aligned");
+  AB_REQUIRE((cnt_dk == nullptr) == (cnt_kw == nullptr), AB_ERR_ARG,
+             "ab_lda_disc_z_f32: pass both count tables or neither");
+  return launch_lda_zf(D, K, V, lda_kp(K), doc_off, w, theta, phiT, phi32, z, cnt_dk, cnt_kw, seed, nullptr, iter,
+                       nullptr, as_stream(stream));
 }
 
 // ---- variant of ab_lda_conj_phi that allocates nothing ----------------------
@@ -798,40 +942,41 @@ struct ab_lda {
   cudaEvent_t fork = nullptr, join = nullptr;
 };
 
-// Sweep scratch: the phi draw's scratch (whose first 256 bytes hold the
-// runner's iteration and completion counters), then the tokens' uniforms
-// u_z f64 [T] drawn ahead of the z kernel.
-static inline size_t lda_uz_offset(int K, int V) { return al256(lda_phi_scratch(K, V)); }
+// Sweep scratch: the phi draw's scratch, whose first 256 bytes hold the
+// runner's iteration and completion counters, then (K <= 64) the binary32
+// screening copy of phi, phi32 f32 [V][Kq], zero padded.
+static inline size_t lda_phi32_offset(int K, int V) { return al256(lda_phi_scratch(K, V)); }
+static inline size_t lda_sweep_scratch(int K, int V) {
+  return lda_phi32_offset(K, V) + (K <= LDA_ZQ_MAX_K ? sizeof(float) * (size_t)V * lda_kq(K) : 0);
+}
 
 static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
   const ab_lda_desc& d = h->d;
   uint32_t* iter_dev = reinterpret_cast<uint32_t*>(d.scratch);
   uint32_t* done = iter_dev + 1;
-  double* u_z = d.K <= LDA_ZQ_MAX_K
-                    ? reinterpret_cast<double*>(static_cast<char*>(d.scratch) + lda_uz_offset(d.K, d.V))
-                    : nullptr;
+  float* phi32 = d.K <= LDA_ZQ_MAX_K
+                     ? reinterpret_cast<float*>(static_cast<char*>(d.scratch) + lda_phi32_offset(d.K, d.V))
+                     : nullptr;
   AB_CUDA(cudaEventRecord(h->fork, main));
   AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
-  // theta branch: theta draws, then the z kernel's uniforms
+  // theta branch
   int rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, main);
   if (rc) return rc;
-  if (u_z != nullptr && d.T > 0) {
-    const int nb = (int)std::min<long long>((long long)ceil_div(d.T, LDA_THREADS), 148 * 8);
-    lda_zu_kernel<<<nb, LDA_THREADS, 0, main>>>(d.T, u_z, d.seed, iter_dev, 0);
-    AB_LAUNCH_CHECK("lda_zu_kernel");
-  }
   // phi branch
   rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.scratch, d.seed, iter_dev, 0,
-                      side);
+                      side, phi32);
   if (rc) return rc;
   AB_CUDA(cudaEventRecord(h->join, side));
   AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
-  return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, u_z, d.z, d.cnt_dk, d.cnt_kw,
+  if (phi32 != nullptr)
+    return launch_lda_zf(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, phi32, d.z, d.cnt_dk,
+                         d.cnt_kw, d.seed, iter_dev, 0, done, main);
+  return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, d.z, d.cnt_dk, d.cnt_kw,
                       d.seed, iter_dev, 0, done, main);
 }
 
-extern "C" size_t ab_lda_scratch_bytes(int K, int V, int T) {
-  return (K > 0 && V > 0 && T >= 0) ? lda_uz_offset(K, V) + sizeof(double) * (size_t)T : 0;
+extern "C" size_t ab_lda_scratch_bytes(int K, int V) {
+  return (K > 0 && V > 0) ? lda_sweep_scratch(K, V) : 0;
 }
 
 extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
@@ -842,7 +987,6 @@ extern "C" int ab_lda_create(const ab_lda_desc* desc, ab_lda** out) {
                  desc->beta && desc->cnt_dk && desc->cnt_kw && desc->scratch,
              AB_ERR_ARG, "ab_lda_create: every device pointer of the descriptor is required");
   AB_REQUIRE((reinterpret_cast<uintptr_t>(desc->phiT) & 15) == 0, AB_ERR_ARG, "ab_lda_create: phiT must be 16-byte aligned");
-  AB_REQUIRE(desc->T >= 0, AB_ERR_ARG, "ab_lda_create: T < 0");
   ab_lda* h = new ab_lda();
   h->d = *desc;
   h->Kp = lda_kp(desc->K);
@@ -862,7 +1006,7 @@ extern "C" int ab_lda_init_state(ab_lda* h, uint32_t iter, void* stream) {
   AB_REQUIRE(h, AB_ERR_ARG, "ab_lda_init_state: null handle");
   const ab_lda_desc& d = h->d;
   cudaStream_t st = as_stream(stream);
-  AB_CUDA(cudaMemsetAsync(d.scratch, 0, lda_phi_scratch(d.K, d.V), st));
+  AB_CUDA(cudaMemsetAsync(d.scratch, 0, lda_sweep_scratch(d.K, d.V), st));
   AB_CUDA(cudaMemcpyAsync(d.scratch, &iter, sizeof(iter), cudaMemcpyHostToDevice, st));
   return launch_lda_count(d.D, d.K, d.V, d.doc_off, d.w, d.z, d.cnt_dk, d.cnt_kw, st);
 }

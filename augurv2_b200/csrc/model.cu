@@ -324,7 +324,7 @@ extern "C" int ab_init_lda(const ab_lda_init* in, ab_model** out) {
   chk(h->alloc(&h->theta, (size_t)D * K));
   chk(h->alloc(&h->phiT, (size_t)V * h->Kp));
   chk(h->alloc(&h->ll_out, 1));
-  chk(h->alloc(&h->scratch, ab_lda_scratch_bytes(K, V, T)));
+  chk(h->alloc(&h->scratch, ab_lda_scratch_bytes(K, V)));
   chk(h->alloc(&h->ll_scratch, ab_ll_scratch_bytes()));
   if (rc) return finish_init(h, rc, out);
   chk(h2d(h->doc_off, in->doc_off, sizeof(int) * (D + 1), st));
@@ -342,7 +342,7 @@ extern "C" int ab_init_lda(const ab_lda_init* in, ab_model** out) {
   if (in->z) chk(h2d(h->z, in->z, sizeof(int) * (size_t)T, st));
   if (rc) return finish_init(h, rc, out);
   ab_lda_desc desc{};
-  desc.D = D; desc.K = K; desc.V = V; desc.T = T;
+  desc.D = D; desc.K = K; desc.V = V;
   desc.doc_off = h->doc_off; desc.w = h->w; desc.alpha = h->alpha; desc.beta = h->beta;
   desc.z = h->z; desc.theta = h->theta; desc.phiT = h->phiT; desc.cnt_dk = h->cnt_dk; desc.cnt_kw = h->cnt_kw;
   desc.scratch = h->scratch; desc.seed = in->seed;

@@ -68,8 +68,7 @@ class LdaGibbs(Checkpointable):
         self.z = torch.zeros(self.T, dtype=torch.int32, device=self.dev)
         self.cnt_dk = torch.zeros((self.D, self.K), dtype=torch.int32, device=self.dev)
         self.cnt_kw = torch.zeros((self.K, self.V), dtype=torch.int32, device=self.dev)
-        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V, self.T)), dtype=torch.uint8,
-                                   device=self.dev)
+        self.scratch = torch.zeros(int(L.ab_lda_scratch_bytes(self.K, self.V)), dtype=torch.uint8, device=self.dev)
         # defaults (uniform theta and phi, z = 0) are filled on the device;
         # given values are uploaded
         if theta is None:
@@ -80,7 +79,7 @@ class LdaGibbs(Checkpointable):
         desc = N.LdaDesc(self.D, self.K, self.V, self.doc_off.data_ptr(), self.w.data_ptr(),
                          self.alpha.data_ptr(), self.beta.data_ptr(), self.z.data_ptr(),
                          self.theta.data_ptr(), self.phiT.data_ptr(), self.cnt_dk.data_ptr(),
-                         self.cnt_kw.data_ptr(), self.scratch.data_ptr(), self.seed, self.T)
+                         self.cnt_kw.data_ptr(), self.scratch.data_ptr(), self.seed)
         h = C.c_void_p()
         N.check(L.ab_lda_create(C.byref(desc), C.byref(h)), "ab_lda_create")
         self._h = h

@@ -284,8 +284,65 @@ def nuts_instances(n_inst=NUTS_INST, seed=0):
     return [(int(n), int(d)) for n, d in zip(Ns, Ds)]
 
 
+def nuts_cpu_baseline(per, chains, budget_s=12.0, max_nd=4_000_000):
+    """The reference's NUTS on the host, one chain per core, for every
+    instance of the run, from timed pieces of its own code: each NUTS leaf of
+    the reference (cbits/augur_mcmclib.h:305-325, h_augur_nuts_build_tree)
+    calls its gradient twice and its log density once, so the reference's
+    seconds per leaf are at least 2 t_grad + t_ll of its cbits HLR functions
+    (oracle/_ref), timed here on one core at a spread of instance sizes
+    (those with N D <= max_nd) and fitted as a + b N D.  The same algorithm
+    draws the same chain, so its leaves per draw (the GPU run's rounds per
+    draw: one leaf per chain per round) and its effective samples per draw
+    (the GPU run's min-ESS over its 512 chains' draws) carry over:
+    min-ESS/s_ref(i) = (min-ESS_i / draws_i) / (leaves per draw_i x
+    seconds per leaf_i).  A full reference NUTS iteration at these sizes runs
+    for minutes (up to 2^10 leaves of an N D product), hence the pieces."""
+    from oracle import oracle as O
+    kind = "reference" if O.available("ref") else "port"
+    o = O.Oracle("ref" if kind == "reference" else "oracle")
+    sizes = sorted({(q["N"], q["D"]) for q in per if q["N"] * q["D"] <= max_nd}, key=lambda s: s[0] * s[1])
+    if len(sizes) > 5:
+        sizes = [sizes[int(round(i * (len(sizes) - 1) / 4))] for i in range(5)]
+    rng = np.random.default_rng(5)
+    pts = []
+    t_start = time.perf_counter()
+    for (Ni, Di) in sizes:
+        X = rng.standard_normal((Ni, Di))
+        y = (rng.random(Ni) < 0.5).astype(np.int32)
+        m = O.HlrModel(X, y, has_b=False, vprior="invgamma", a0=1.0, s0=1.0)
+        par = np.concatenate([rng.standard_normal(Di) * 0.1, [0.0, 1.0]])
+        idx = list(range(Di))
+        reps, t0 = 0, time.perf_counter()
+        while reps < 3 or (time.perf_counter() - t0 < budget_s / (2 * len(sizes)) and reps < 200):
+            O.hlr_grad(o, m, par, idx)
+            O.hlr_grad(o, m, par, idx)
+            O.hlr_ll(o, m, par, idx)
+            reps += 1
+        pts.append((Ni * Di, (time.perf_counter() - t0) / reps))
+    nd = np.array([p[0] for p in pts], np.float64)
+    tl = np.array([p[1] for p in pts])
+    b, a = np.polyfit(nd, tl, 1) if len(pts) > 1 else (tl[0] / nd[0], 0.0)
+    a = max(a, 0.0)
+    rates = []
+    for q in per:
+        leaves_per_draw = q["rounds"] / max(1, q["draws_per_chain"])
+        sec_leaf = a + b * q["N"] * q["D"]
+        ess_per_draw = q["min_ess"] / (q["draws_per_chain"] * chains)
+        rates.append(ess_per_draw / (leaves_per_draw * sec_leaf))
+    worst = int(np.argmin(rates))
+    return {"value": float(rates[worst]), "unit": "min-ESS/s", "cores": 1, "kind": kind,
+            "per_instance_min_ess_per_s": [float(r) for r in rates],
+            "worst_instance": {"N": per[worst]["N"], "D": per[worst]["D"]},
+            "seconds_per_leaf_fit": {"a": float(a), "b_per_nd": float(b),
+                                     "timed": [{"ND": int(n), "s": float(t)} for n, t in pts]},
+            "sample": "the reference's cbits HLR gradient (x2) and log density per NUTS leaf, timed on one core "
+                      "at %d instance sizes (%.1f s), fitted linear in N D; leaves and min-ESS per draw from the "
+                      "GPU run of the same algorithm" % (len(pts), time.perf_counter() - t_start)}
+
+
 def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INST, chains=NUTS_C, streams=8,
-                 hist_cap=128, variants=("reference", "standard"), share="equal"):
+                 hist_cap=128, variants=("reference", "standard"), share="equal", cpu=True):
     """64 HLR instances (X ~ N(0,1) bf16, sigma^2 ~ InvGamma(1,1),
     beta ~ N(0, sigma^2 I), y ~ Bern(sigmoid(X beta)); sigma^2 held at its
     generating value), 512 NUTS chains each, max tree depth 10.  Every round
@@ -373,6 +430,9 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
                             "streams": streams,
                             "schedule": "NutsPool (%s shares): rounds until %d draws per chain, LPT streams"
                                         % (share, min_draws)}})
+    if cpu:
+        head["cpu_baseline"] = nuts_cpu_baseline(results[variants[0]]["instances"], chains)
+        head["gain_vs_cpu_core"] = head["value"] / head["cpu_baseline"]["value"]
     return head
 
 
@@ -465,7 +525,54 @@ def run_gmm(steps=10, warmup=3, cpu=True):
     return line
 
 
-def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_steps=10):
+def chain_moments(sampler, n):
+    """Runs `n` more iterations of `sampler`, accumulating every chain's sum
+    and sum of squares of theta on the device (float64).  Returns the chain
+    means [C, D] and within-chain variances [C, D] as numpy arrays."""
+    import torch
+    C_, D = sampler.theta.shape
+    s1 = torch.zeros((C_, D), dtype=torch.float64, device="cuda")
+    s2 = torch.zeros_like(s1)
+    for _ in range(n):
+        sampler.run(1)
+        t = sampler.theta.double()
+        s1 += t
+        s2 += t * t
+    m = s1 / n
+    v = (s2 / n - m * m).clamp_min(0.0) * (n / (n - 1.0))
+    return m.cpu().numpy(), v.cpu().numpy()
+
+
+def exactness_stats(mom_s, mom_p):
+    """Posterior means of two samplers of one posterior, compared in units of
+    the posterior sd per coefficient.  Each sampler's Monte-Carlo error is
+    estimated from the spread of its independent chains' means
+    (var(grand mean) = var over chains of the chain means / C).  Reports the
+    largest and median |difference|, the Monte-Carlo sd of the difference,
+    and the root-mean-square bias over coefficients with the Monte-Carlo
+    noise removed: sqrt(max(0, mean(d^2 - s^2))), with an approximate 95%
+    upper bound (mean(d^2) has standard error sqrt(2/D) mean(d^2) when the
+    difference is noise)."""
+    (m_s, v_s), (m_p, v_p) = mom_s, mom_p
+    C_, D = m_p.shape
+    sd = np.sqrt(v_p.mean(0))
+    gs, gp = m_s.mean(0), m_p.mean(0)
+    mc = np.sqrt(m_s.var(0, ddof=1) / C_ + m_p.var(0, ddof=1) / C_) / sd
+    d = (gs - gp) / sd
+    msq, nsq = float(np.mean(d * d)), float(np.mean(mc * mc))
+    bias2 = msq - nsq
+    upper2 = bias2 + 2.0 * np.sqrt(2.0 / D) * msq
+    return {"posterior_mean_diff_in_sd": float(np.max(np.abs(d))),
+            "posterior_mean_diff_in_sd_median": float(np.median(np.abs(d))),
+            "posterior_mean_mc_sd": float(np.median(mc)),
+            "posterior_mean_z_max": float(np.max(np.abs(d) / mc)),
+            "posterior_mean_bias_rms_in_sd": float(np.sqrt(max(bias2, 0.0))),
+            "posterior_mean_bias_rms_upper95_in_sd": float(np.sqrt(max(upper2, 0.0))),
+            "posterior_sd_ratio_median": float(np.median(np.sqrt(v_s.mean(0)) / sd))}
+
+
+def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_steps=10, exact_plain=1500,
+                      exact_sur=4000):
     """Surrogate-gradient HMC vs plain exact-gradient HMC on the same data,
     chains, step-size rule and iteration count; min-ESS/s of each (ESS over
     all D coefficients, Geyer initial monotone, 256 chains), device time by
@@ -522,6 +629,8 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
     draws_p = rec_p.cpu().numpy()
     ess_p = ess(draws_p)
     acc_p = plain.accept_rate()[0]
+    mom_p = chain_moments(plain, exact_plain) if exact_plain else None
+    div_p = plain.divergences()
     del plain
 
     sur = H.SurrogateHmc(d, HLR_C, L=HLR_L, eps=eps, jitter=0.1, seed=12, init=init, train_every=train_every,
@@ -535,11 +644,21 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
     draws_s = rec_s.cpu().numpy()
     ess_s = ess(draws_s)
     acc_s = sur.accept_rate()[0]
+    mom_s = chain_moments(sur, exact_sur) if exact_sur else None
+    div_s = sur.divergences()
 
-    # posterior moments: both chains target the same posterior
-    mp, ms_ = draws_p.reshape(-1, HLR_D).mean(0), draws_s.reshape(-1, HLR_D).mean(0)
-    sd = draws_p.reshape(-1, HLR_D).std(0)
-    z = (ms_ - mp) / np.sqrt(sd ** 2 / ess_p + sd ** 2 / ess_s)
+    # posterior moments: both samplers target the same posterior; compared on
+    # the long continuation runs (chain means) when they were made
+    if mom_s is not None and mom_p is not None:
+        exact = exactness_stats(mom_s, mom_p)
+        exact["iterations"] = {"plain": exact_plain, "surrogate": exact_sur}
+    else:
+        mp, ms_ = draws_p.reshape(-1, HLR_D).mean(0), draws_s.reshape(-1, HLR_D).mean(0)
+        sd = draws_p.reshape(-1, HLR_D).std(0)
+        z = (ms_ - mp) / np.sqrt(sd ** 2 / ess_p + sd ** 2 / ess_s)
+        exact = {"posterior_mean_diff_in_sd": float(np.max(np.abs(ms_ - mp) / sd)),
+                 "posterior_mean_z_max": float(np.max(np.abs(z))),
+                 "posterior_mean_mc_sd": float(np.median(np.sqrt(1.0 / ess_p + 1.0 / ess_s)))}
     v_p = ess_p.min() / (ms_p / 1e3)
     v_s = ess_s.min() / (ms_s / 1e3)
     return {
@@ -551,9 +670,9 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
         "accept": {"surrogate": float(acc_s), "plain": float(acc_p)},
         "surrogate_rel_err": sur.last_rel_err, "fallback": sur.fallback,
         "exact_passes": {"grad": sur.n_grad - g0, "logp_only": sur.n_logp - l0, "plain_grad": iters * HLR_L},
-        "posterior_mean_diff_in_sd": float(np.max(np.abs(ms_ - mp) / sd)),
-        "posterior_mean_z_max": float(np.max(np.abs(z))),
-        "posterior_mean_mc_sd": float(np.median(np.sqrt(1.0 / ess_p + 1.0 / ess_s))),
+        "exactness": exact,
+        "posterior_mean_diff_in_sd": exact["posterior_mean_diff_in_sd"],
+        "divergences": {"surrogate": div_s, "plain": div_p},
         "exact_pass_ms": pass_ms,
         "roofline": {"bound": "tensor", "kernel": "gemm_kernel (forward + backward data passes)",
                      "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
@@ -681,11 +800,14 @@ def run_ours(args, rank, world, local_rank):
             # LDA line stands on its own if one of them fails)
             for key, fn in (("hlr_surrogate", lambda: run_hlr_surrogate(iters=args.hlr_iters,
                                                                          train_every=args.train_every,
-                                                                         train_steps=args.train_steps)),
+                                                                         train_steps=args.train_steps,
+                                                                         exact_plain=args.exact_plain,
+                                                                         exact_sur=args.exact_sur)),
                             ("hlr_small", lambda: run_hlr_small(cpu=not args.no_cpu_baseline)),
                             ("gmm", lambda: run_gmm(cpu=not args.no_cpu_baseline)),
                             ("hlr_nuts", lambda: run_hlr_nuts(min_draws=args.nuts_draws,
-                                                              max_rounds=args.nuts_rounds))):
+                                                              max_rounds=args.nuts_rounds,
+                                                              cpu=not args.no_cpu_baseline))):
                 try:
                     line[key] = fn()
                 except Exception as e:
@@ -830,6 +952,10 @@ def main():
     ap.add_argument("--hlr-iters", type=int, default=100)
     ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
     ap.add_argument("--train-steps", type=int, default=10, help="surrogate: Adam steps per check")
+    ap.add_argument("--exact-plain", type=int, default=1500,
+                    help="surrogate exactness: iterations of the plain sampler's continuation (0: skip)")
+    ap.add_argument("--exact-sur", type=int, default=4000,
+                    help="surrogate exactness: iterations of the surrogate sampler's continuation")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     rank = int(os.environ.get("RANK", 0))
@@ -854,7 +980,8 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         line = run_hlr_surrogate(iters=args.hlr_iters, train_every=args.train_every,
-                                 train_steps=args.train_steps) if rank == 0 else None
+                                 train_steps=args.train_steps, exact_plain=args.exact_plain,
+                                 exact_sur=args.exact_sur) if rank == 0 else None
         if line is not None:
             line.update({"n_gpus": 1, "steps": args.hlr_iters, "warmup": 30, "higher_is_better": True,
                          "scaling": "weak", "vs_baseline": None, "dtype": "bf16 x3 parts, f32 accum, f64 energy",

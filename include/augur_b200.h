@@ -117,8 +117,22 @@ int ab_lda_disc_z(int D, int K, int V, const int* doc_off, const int* w, const d
                   const double* phiT, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
                   uint32_t iter, void* stream);
 
+/* The same draw screened in binary32 (K <= 64): phi32 f32 [V][Kq],
+ * Kq = ab_lda_phi32_stride(K), 16-byte aligned, must hold phiT's values
+ * rounded to nearest binary32 with zero padding (the sweep runner's phi
+ * normalisation writes it).  Products and running sums are binary32 with a
+ * margin that bounds their rounding, so every draw the screen decides equals
+ * the reference's; the rest (u within the margin of a boundary, about 1e-5 of
+ * the tokens at K = 50, or a degenerate norm) run the reference's binary64
+ * loop on theta and phiT.  Results equal ab_lda_disc_z's bit for bit. */
+int ab_lda_phi32_stride(int K);
+int ab_lda_disc_z_f32(int D, int K, int V, const int* doc_off, const int* w, const double* theta,
+                      const double* phiT, const float* phi32, int* z, int* cnt_dk, int* cnt_kw, uint64_t seed,
+                      uint32_t iter, void* stream);
+
 /* Sweep runner: the whole augur_step of the LDA schedule (CgKern.hs:232-238)
- * as a captured CUDA graph of four kernels. */
+ * as a captured CUDA graph of four kernels (z screened in binary32 for
+ * K <= 64). */
 typedef struct ab_lda_desc {
   int D, K, V;
   const int* doc_off;   /* [D+1] */
@@ -130,15 +144,14 @@ typedef struct ab_lda_desc {
   double* phiT;         /* [V][Kp] */
   int* cnt_dk;          /* [D][K] */
   int* cnt_kw;          /* [K][V] */
-  void* scratch;        /* ab_lda_scratch_bytes(K, V, T) bytes of device memory */
+  void* scratch;        /* ab_lda_scratch_bytes(K, V) bytes of device memory */
   uint64_t seed;
-  int T;                /* tokens: doc_off[D] */
 } ab_lda_desc;
 
 typedef struct ab_lda ab_lda;
-/* Scratch of the sweep runner: counters, the phi draw's partial sums and
- * normalisers, and the tokens' uniforms drawn ahead of the z kernel. */
-size_t ab_lda_scratch_bytes(int K, int V, int T);
+/* Scratch of the sweep runner: its counters, the phi draw's partial sums and
+ * normalisers, and the binary32 screening copy of phi (K <= 64). */
+size_t ab_lda_scratch_bytes(int K, int V);
 /* Replaces augur_iface_init for the LDA model (CgStInit.hs:474-510); the
  * caller owns every buffer named by the descriptor. */
 int ab_lda_create(const ab_lda_desc* desc, ab_lda** out);

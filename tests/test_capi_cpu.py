@@ -39,7 +39,7 @@ def test_lda_null_pointer_rejected():
 
 
 def test_lda_create_requires_every_pointer():
-    d = N.LdaDesc(4, 4, 8, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
+    d = N.LdaDesc(4, 4, 8, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0)
     h = C.c_void_p()
     assert N.lib().ab_lda_create(C.byref(d), C.byref(h)) == 1
 

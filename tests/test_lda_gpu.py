@@ -236,3 +236,65 @@ def test_full_size_properties():
     np.add.at(hist, (doc, z), 1)
     np.testing.assert_array_equal(s.cnt_dk.cpu().numpy(), hist)
     s.close()
+
+
+def _phi32_of(phi):
+    K, V = phi.shape
+    Kq = N.lib().ab_lda_phi32_stride(K)
+    out = np.zeros((V, Kq), np.float32)
+    out[:, :K] = phi.T.astype(np.float32)        # round to nearest binary32
+    return out
+
+
+@pytest.mark.parametrize("seed,K,V,degenerate", [(0, 50, 700, False), (1, 1, 30, False), (2, 2, 30, True),
+                                                 (3, 3, 40, False), (4, 4, 50, False), (5, 16, 90, True),
+                                                 (6, 32, 300, False), (7, 33, 120, False), (8, 64, 300, True),
+                                                 (9, 61, 200, False), (10, 9, 50, False), (11, 50, 700, True)])
+def test_disc_z_f32_screen_bit_exact(orc, seed, K, V, degenerate):
+    """The binary32-screened z kernel gives the reference's assignments and
+    counts bit for bit, including half rows of every length (K = 1..64) and
+    tokens the screen cannot decide (exact zeros, products that underflow
+    binary32, tiny and zero norms)."""
+    off, w, theta, phi = random_problem(seed, D=150, K=K, V=V)
+    if degenerate:
+        theta[:, ::3] = 0.0
+        theta[theta.sum(1) == 0, 0] = 1.0
+        theta[1::4] *= 1e-300                 # products below binary32 range, norm 0 in binary32
+        theta[2::4] *= 1e-25                  # norm below 2^-60 but normal in binary64
+        phi[:, 7 % V] = 0.0
+        phi[::2, 1 % V] = 1e-40               # binary32 subnormals
+    D = theta.shape[0]
+    phiT, _ = phiT_of(phi)
+    phi32 = _phi32_of(phi)
+    z = torch.zeros(len(w), dtype=torch.int32, device="cuda")
+    cdk = torch.zeros((D, K), dtype=torch.int32, device="cuda")
+    ckw = torch.zeros((K, V), dtype=torch.int32, device="cuda")
+    g = [dev(off, torch.int32), dev(w, torch.int32), dev(theta, torch.float64), dev(phiT, torch.float64),
+         torch.as_tensor(phi32).cuda()]
+    N.check(N.lib().ab_lda_disc_z_f32(D, K, V, N.ptr(g[0]), N.ptr(g[1]), N.ptr(g[2]), N.ptr(g[3]), N.ptr(g[4]),
+                                      N.ptr(z), N.ptr(cdk), N.ptr(ckw), 42, 9, N.stream_ptr()), "disc_z_f32")
+    z_ref = orc.lda_disc_z(off, w, theta, phi, np.zeros(len(w), np.int32), 42, 9)
+    np.testing.assert_array_equal(z.cpu().numpy(), z_ref)
+    c_dk, c_kw = orc.lda_conj_stat(off, w, z_ref, D, K, V)
+    np.testing.assert_array_equal(cdk.cpu().numpy(), c_dk)
+    np.testing.assert_array_equal(ckw.cpu().numpy(), c_kw)
+
+
+def test_sweep_phi32_copy_is_phi_rounded():
+    """The sweep runner's binary32 copy of phi (the z screen's input) is phi
+    rounded to nearest, with zero padding."""
+    K, V, D = 50, 600, 40
+    off, w = synthetic_corpus(K, V, D, 60, 0.1, 0.01, seed=3)
+    s = LdaGibbs(K, V, off, w, 0.1, 0.01, seed=2)
+    s.sweep(2)
+    torch.cuda.synchronize()
+    L = N.lib()
+    Kq = L.ab_lda_phi32_stride(K)
+    raw = s.scratch.cpu().numpy()
+    nbytes = 4 * V * Kq
+    phi32 = raw[len(raw) - nbytes:].view(np.float32).reshape(V, Kq)
+    phi = s.state()[1]
+    np.testing.assert_array_equal(phi32[:, :K], phi.T.astype(np.float32))
+    assert (phi32[:, K:] == 0).all()
+    s.close()
+
