@@ -148,6 +148,118 @@ lda_phi_draw_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta
   }
 }
 
+// The same draw of phi for the sweep runner, with the rejection loops taken
+// out of the draw kernel (three kernels instead of two):
+//  lda_phi_try_kernel  one cell per thread, K * B CTAs of 256 words as
+//                      lda_phi_draw_kernel: reads (and clears) the count,
+//                      makes the cell's first Marsaglia-Tsang try
+//                      (gamma_first_try) and stores the draws it decides; the
+//                      undecided cells (about 5%) go to the CTA's queue, in
+//                      thread order, with their counts; the CTA's block sum of
+//                      its decided draws (zeros for the queued) goes to
+//                      partial[cta];
+//  lda_phi_fix_kernel  one warp per try CTA: completes the CTA's queued cells
+//                      from their first try's normal and uniform
+//                      (gamma_draw_resume), adds them to partial[cta] (each
+//                      lane's draws in queue order, then a fixed butterfly),
+//                      and the last warp of a topic (atomic ticket) adds the
+//                      topic's B partials in CTA order into nrm[k];
+//  lda_phi_norm_kernel as above.
+// Every cell gets the draw gamma_draw gives it; the normaliser is a fixed-order
+// (deterministic) sum.  No warp waits for another warp's rejection loop.
+__global__ void __launch_bounds__(LDA_THREADS, 4)
+lda_phi_try_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta, int* __restrict__ cnt_kw,
+                   double* __restrict__ phiT, int clear_counts, double* __restrict__ partial,
+                   int2* __restrict__ queue, double2* __restrict__ queue_zu, int* __restrict__ qn,
+                   uint64_t seed, const uint32_t* iter_dev, uint32_t iter_fixed) {
+  __shared__ double red[33];
+  __shared__ int wcount[LDA_THREADS / 32];
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  const int k = blockIdx.x / B;
+  const int b = blockIdx.x - k * B;
+  const int v = b * LDA_THREADS + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double g = 0.0, z1 = 0.0, u1 = 0.0;
+  bool need = false;
+  int c = 0;
+  if (v < V) {
+    const size_t idx = (size_t)k * V + v;
+    c = cnt_kw[idx];
+    if (clear_counts) cnt_kw[idx] = 0;
+    Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
+    if (gamma_first_try(s, __dadd_rn(beta[v], (double)c), 1.0, g, z1, u1)) {
+      phiT[(size_t)v * Kp + k] = g;
+    } else {
+      need = true;
+      g = 0.0;
+    }
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, need);
+  if (lane == 0) wcount[warp] = __popc(bal);
+  const double bsum = block_sum_f64(g, red);     // its barriers also publish wcount
+  if (need) {
+    int base = 0;
+    for (int i = 0; i < warp; ++i) base += wcount[i];
+    const size_t slot = (size_t)blockIdx.x * LDA_THREADS + base + __popc(bal & ((1u << lane) - 1u));
+    queue[slot] = make_int2(threadIdx.x, c);
+    queue_zu[slot] = make_double2(z1, u1);
+  }
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int i = 0; i < LDA_THREADS / 32; ++i) tot += wcount[i];
+    qn[blockIdx.x] = tot;
+    partial[blockIdx.x] = bsum;
+  }
+}
+
+__global__ void __launch_bounds__(LDA_THREADS)
+lda_phi_fix_kernel(int K, int V, int Kp, int B, const double* __restrict__ beta, double* __restrict__ phiT,
+                   double* __restrict__ partial, const int2* __restrict__ queue,
+                   const double2* __restrict__ queue_zu, const int* __restrict__ qn,
+                   uint32_t* __restrict__ ticket, double* __restrict__ nrm, uint64_t seed,
+                   const uint32_t* iter_dev, uint32_t iter_fixed) {
+  const int lane = threadIdx.x & 31;
+  const int cta = blockIdx.x * (LDA_THREADS / 32) + (threadIdx.x >> 5);
+  if (cta >= K * B) return;                       // whole warps
+  const uint32_t iter = read_iter(iter_dev, iter_fixed);
+  const int k = cta / B;
+  const int b = cta - k * B;
+  const int n = qn[cta];
+  double acc = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const int2 e = queue[(size_t)cta * LDA_THREADS + i];
+    const double2 zu = queue_zu[(size_t)cta * LDA_THREADS + i];
+    const int v = b * LDA_THREADS + e.x;
+    const size_t idx = (size_t)k * V + v;
+    Stream s = make_stream(seed, (uint32_t)idx, iter, TAG_PHI);
+    s.pos = 2;                                  // after the try kernel's normal and uniform
+    const double g = gamma_draw_resume(s, __dadd_rn(beta[v], (double)e.y), 1.0, zu.x, zu.y);
+    phiT[(size_t)v * Kp + k] = g;
+    acc = __dadd_rn(acc, g);
+  }
+  acc = warp_sum_f64(acc);
+  int last = 0;
+  if (lane == 0) {
+    partial[cta] = __dadd_rn(partial[cta], acc);
+    __threadfence();
+    last = atomicAdd(ticket + k, 1u) == (unsigned)(B - 1);
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  // the topic's B partials in CTA order: the warp loads 32 at a time, lane 0 adds
+  __threadfence();
+  double tot = 0.0;
+  for (int base = 0; base < B; base += 32) {
+    const double x = base + lane < B ? __ldcg(partial + (size_t)k * B + base + lane) : 0.0;
+    const int m = min(32, B - base);
+    for (int j = 0; j < m; ++j) tot = __dadd_rn(tot, __shfl_sync(0xffffffffu, x, j));
+  }
+  if (lane == 0) {
+    nrm[k] = tot;
+    ticket[k] = 0u;
+  }
+}
+
 // phiT [V][Kp] as V * Kp / 2 pairs of doubles; pair j holds topics 2j mod Kp
 // and the next one.  Padding topics (k >= K) are left untouched (zero).
 // When phi32 is given, the normalised values are also stored rounded to
@@ -944,10 +1056,46 @@ struct ab_lda {
 
 // Sweep scratch: the phi draw's scratch, whose first 256 bytes hold the
 // runner's iteration and completion counters, then (K <= 64) the binary32
-// screening copy of phi, phi32 f32 [V][Kq], zero padded.
+// screening copy of phi, phi32 f32 [V][Kq], zero padded, ...
 static inline size_t lda_phi32_offset(int K, int V) { return al256(lda_phi_scratch(K, V)); }
+static inline size_t lda_queue_offset(int K, int V) {
+  return lda_phi32_offset(K, V) + al256(K <= LDA_ZQ_MAX_K ? sizeof(float) * (size_t)V * lda_kq(K) : 0);
+}
+// ... then the try kernel's queues: cells int2 [K * B][256], their first
+// tries' (normal, uniform) double2 [K * B][256], and lengths int [K * B]
 static inline size_t lda_sweep_scratch(int K, int V) {
-  return lda_phi32_offset(K, V) + (K <= LDA_ZQ_MAX_K ? sizeof(float) * (size_t)V * lda_kq(K) : 0);
+  const size_t nb = (size_t)K * lda_phi_blocks(V);
+  return lda_queue_offset(K, V) + (sizeof(int2) + sizeof(double2)) * nb * LDA_THREADS + sizeof(int) * nb;
+}
+
+// The sweep's phi draw: try (part 0), then fix and normalise (part 1)
+// (lda_phi_try_kernel).
+static int launch_lda_phi_sweep(int part, int K, int V, int Kp, const double* beta, int* cnt_kw, double* phiT,
+                                void* scratch, float* phi32, uint64_t seed, const uint32_t* iter_dev,
+                                cudaStream_t st) {
+  const int B = lda_phi_blocks(V);
+  char* base = static_cast<char*>(scratch) + 256;
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(base);
+  double* nrm = reinterpret_cast<double*>(base + al256(4 * (size_t)K));
+  double* partial = reinterpret_cast<double*>(base + al256(4 * (size_t)K) + al256(8 * (size_t)K));
+  double2* queue_zu = reinterpret_cast<double2*>(static_cast<char*>(scratch) + lda_queue_offset(K, V));
+  int2* queue = reinterpret_cast<int2*>(queue_zu + (size_t)K * B * LDA_THREADS);
+  int* qn = reinterpret_cast<int*>(queue + (size_t)K * B * LDA_THREADS);
+  if (part == 0) {
+    lda_phi_try_kernel<<<K * B, LDA_THREADS, 0, st>>>(K, V, Kp, B, beta, cnt_kw, phiT, 1, partial, queue,
+                                                      queue_zu, qn, seed, iter_dev, 0);
+    AB_LAUNCH_CHECK("lda_phi_try_kernel");
+    return AB_OK;
+  }
+  const int warps_per_cta = LDA_THREADS / 32;
+  lda_phi_fix_kernel<<<ceil_div((size_t)K * B, warps_per_cta), LDA_THREADS, 0, st>>>(
+      K, V, Kp, B, beta, phiT, partial, queue, queue_zu, qn, ticket, nrm, seed, iter_dev, 0);
+  AB_LAUNCH_CHECK("lda_phi_fix_kernel");
+  const size_t n2 = (size_t)V * (Kp / 2);
+  const unsigned nb = (unsigned)std::min<size_t>((n2 + LDA_THREADS - 1) / LDA_THREADS, 148u * 8u);
+  lda_phi_norm_kernel<<<nb, LDA_THREADS, sizeof(double) * K, st>>>(K, V, Kp, nrm, phiT, phi32, lda_kq(K));
+  AB_LAUNCH_CHECK("lda_phi_norm_kernel");
+  return AB_OK;
 }
 
 static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
@@ -957,20 +1105,33 @@ static int lda_enqueue_sweep(ab_lda* h, cudaStream_t main, cudaStream_t side) {
   float* phi32 = d.K <= LDA_ZQ_MAX_K
                      ? reinterpret_cast<float*>(static_cast<char*>(d.scratch) + lda_phi32_offset(d.K, d.V))
                      : nullptr;
+  if (phi32 != nullptr) {
+    // phi's first tries use the whole GPU; the theta draw then runs beside the
+    // phi fix-up and normalisation, which leave most SMs idle
+    int rc = launch_lda_phi_sweep(0, d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, d.scratch, phi32, d.seed,
+                                  iter_dev, main);
+    if (rc) return rc;
+    AB_CUDA(cudaEventRecord(h->fork, main));
+    AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
+    rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, side);
+    if (rc) return rc;
+    AB_CUDA(cudaEventRecord(h->join, side));
+    rc = launch_lda_phi_sweep(1, d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, d.scratch, phi32, d.seed, iter_dev,
+                              main);
+    if (rc) return rc;
+    AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
+    return launch_lda_zf(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, phi32, d.z, d.cnt_dk,
+                         d.cnt_kw, d.seed, iter_dev, 0, done, main);
+  }
+  // K > 64: theta beside the two-kernel phi draw, then the binary64 z kernel
   AB_CUDA(cudaEventRecord(h->fork, main));
   AB_CUDA(cudaStreamWaitEvent(side, h->fork, 0));
-  // theta branch
   int rc = launch_lda_theta(d.D, d.K, d.alpha, d.cnt_dk, d.theta, d.seed, iter_dev, 0, main);
   if (rc) return rc;
-  // phi branch
-  rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.scratch, d.seed, iter_dev, 0,
-                      side, phi32);
+  rc = launch_lda_phi(d.K, d.V, h->Kp, d.beta, d.cnt_kw, d.phiT, 1, d.scratch, d.seed, iter_dev, 0, side);
   if (rc) return rc;
   AB_CUDA(cudaEventRecord(h->join, side));
   AB_CUDA(cudaStreamWaitEvent(main, h->join, 0));
-  if (phi32 != nullptr)
-    return launch_lda_zf(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, phi32, d.z, d.cnt_dk,
-                         d.cnt_kw, d.seed, iter_dev, 0, done, main);
   return launch_lda_z(d.D, d.K, d.V, h->Kp, d.doc_off, d.w, d.theta, d.phiT, d.z, d.cnt_dk, d.cnt_kw,
                       d.seed, iter_dev, 0, done, main);
 }

@@ -42,9 +42,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 K_TOPICS, V_WORDS, D_DOCS, MEAN_LEN, ALPHA, BETA, DATA_SEED = 50, 10000, 2000, 200, 0.1, 0.01, 0
-# DRAM bytes of one z-kernel launch on this workload, from the ncu capture summarised in
-# profiles/lda_zq_kernel_k50_v10000_d2000.md (phi and the count tables stay in L2)
-Z_KERNEL_DRAM_BYTES = 6_699_264
+# DRAM bytes (read + write) of one launch of the sweep's z kernel on this
+# workload, from the ncu capture summarised with its command in profiles/
+# (phi and the count tables stay in L2)
+Z_KERNEL_DRAM_BYTES = 5_144_064
 L2_FLUSH_BYTES = 512 << 20
 
 
@@ -525,22 +526,28 @@ def run_gmm(steps=10, warmup=3, cpu=True):
     return line
 
 
-def chain_moments(sampler, n):
-    """Runs `n` more iterations of `sampler`, accumulating every chain's sum
-    and sum of squares of theta on the device (float64).  Returns the chain
-    means [C, D] and within-chain variances [C, D] as numpy arrays."""
+def chain_moments(sampler, n, burn=0):
+    """Runs `burn` iterations of `sampler` (discarded), then `n` more,
+    accumulating every chain's sum and sum of squares of theta on the device
+    (float64), separately for the two halves of the window.  Returns the chain
+    means [C, D], within-chain variances [C, D] and the two half-window chain
+    means (for a stationarity check) as numpy arrays."""
     import torch
     C_, D = sampler.theta.shape
-    s1 = torch.zeros((C_, D), dtype=torch.float64, device="cuda")
-    s2 = torch.zeros_like(s1)
-    for _ in range(n):
+    for _ in range(burn):
+        sampler.run(1)
+    s1 = torch.zeros((2, C_, D), dtype=torch.float64, device="cuda")
+    s2 = torch.zeros((C_, D), dtype=torch.float64, device="cuda")
+    for i in range(n):
         sampler.run(1)
         t = sampler.theta.double()
-        s1 += t
+        s1[int(2 * i >= n)] += t
         s2 += t * t
-    m = s1 / n
+    h = torch.tensor([(n + 1) // 2, n // 2], dtype=torch.float64, device="cuda")
+    halves = s1 / h[:, None, None]
+    m = s1.sum(0) / n
     v = (s2 / n - m * m).clamp_min(0.0) * (n / (n - 1.0))
-    return m.cpu().numpy(), v.cpu().numpy()
+    return m.cpu().numpy(), v.cpu().numpy(), halves.cpu().numpy()
 
 
 def exactness_stats(mom_s, mom_p):
@@ -553,9 +560,16 @@ def exactness_stats(mom_s, mom_p):
     noise removed: sqrt(max(0, mean(d^2 - s^2))), with an approximate 95%
     upper bound (mean(d^2) has standard error sqrt(2/D) mean(d^2) when the
     difference is noise)."""
-    (m_s, v_s), (m_p, v_p) = mom_s, mom_p
+    (m_s, v_s, h_s), (m_p, v_p, h_p) = mom_s, mom_p
     C_, D = m_p.shape
     sd = np.sqrt(v_p.mean(0))
+
+    def drift(h):
+        # second-half minus first-half grand means, in posterior sd, with the
+        # Monte-Carlo noise of the halves removed (rms over coefficients)
+        dd = (h[1].mean(0) - h[0].mean(0)) / sd
+        nn = np.sqrt(h[1].var(0, ddof=1) / C_ + h[0].var(0, ddof=1) / C_) / sd
+        return float(np.sqrt(max(0.0, np.mean(dd * dd) - np.mean(nn * nn))))
     gs, gp = m_s.mean(0), m_p.mean(0)
     mc = np.sqrt(m_s.var(0, ddof=1) / C_ + m_p.var(0, ddof=1) / C_) / sd
     d = (gs - gp) / sd
@@ -568,18 +582,34 @@ def exactness_stats(mom_s, mom_p):
             "posterior_mean_z_max": float(np.max(np.abs(d) / mc)),
             "posterior_mean_bias_rms_in_sd": float(np.sqrt(max(bias2, 0.0))),
             "posterior_mean_bias_rms_upper95_in_sd": float(np.sqrt(max(upper2, 0.0))),
-            "posterior_sd_ratio_median": float(np.median(np.sqrt(v_s.mean(0)) / sd))}
+            "posterior_sd_ratio_median": float(np.median(np.sqrt(v_s.mean(0)) / sd)),
+            "drift_rms_in_sd": {"surrogate": drift(h_s), "plain": drift(h_p)}}
 
 
-def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_steps=10, exact_plain=1500,
-                      exact_sur=4000):
+def ess_chain_means(mom):
+    """Effective sample size per coefficient of C independent chains of n
+    draws each from their chain means: var(chain mean) = sigma^2 tau / n, so
+    ESS = C n / tau = C sigma^2 / var(chain mean) (sigma^2 the mean
+    within-chain variance).  Valid when n is many autocorrelation times, which
+    the burn-in and window lengths of the caller ensure."""
+    m, v, _ = mom
+    return m.shape[0] * v.mean(0) / np.maximum(m.var(0, ddof=1), 1e-300)
+
+
+def run_hlr_surrogate(iters=100, warm=40, learn=240, train_every=8, train_steps=10, exact_plain=1000,
+                      exact_sur=3000, exact_burn=(300, 600)):
     """Surrogate-gradient HMC vs plain exact-gradient HMC on the same data,
-    chains, step-size rule and iteration count; min-ESS/s of each (ESS over
-    all D coefficients, Geyer initial monotone, 256 chains), device time by
-    CUDA events around every iteration (Python gaps included)."""
+    chains, step-size rule and trajectory length.  Per-iteration device time
+    by CUDA events over `iters` iterations of each (graph replays, the
+    surrogate's periodic exact-gradient checks included).  Each sampler then
+    runs a burn-in and a long window whose chain means give both the
+    effective sample size (ess_chain_means) and the exactness comparison
+    (posterior means of the two samplers in posterior sd, exactness_stats).
+    The surrogate learns online (replay buffer, refitted linear part, Adam)
+    for its first `learn` iterations only; afterwards its kernel is fixed and
+    its error checks decide the fallback."""
     import torch
     from augurv2_b200 import hlrb as H
-    from augurv2_b200.diagnostics import ess
 
     X, y, beta = H.synthetic(HLR_N, HLR_D, seed=HLR_SEED)
     d = H.HlrbData(X, y, prior="student_t", nu=3.0, scale=1.0)
@@ -608,68 +638,59 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
     exe = 5 * mm / (pass_ms["grad"] / 1e3) / 1e12        # executed: 3 + 2 bf16 parts
 
     def timed(sampler, n):
-        rec = torch.empty((n, HLR_C, HLR_D), dtype=torch.float32, device="cuda")
         ms = 0.0
         for i in range(n):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             sampler.run(1)
             b.record()
-            rec[i].copy_(sampler.theta)
             torch.cuda.synchronize()
             ms += a.elapsed_time(b)
-        return rec, ms
+        return ms / n
 
     plain = H.BatchedHmc(d, HLR_C, L=HLR_L, eps=2e-4, jitter=0.1, seed=11, init=init)
     eps = H.adapt_step_size(plain, warm)
-    init = plain.theta.cpu().numpy()      # both measured runs start from the warmed-up chains
+    init = plain.theta.cpu().numpy()      # both samplers start from the warmed-up chains
     plain.capture()
     plain.reset_stats()
-    rec_p, ms_p = timed(plain, iters)
-    draws_p = rec_p.cpu().numpy()
-    ess_p = ess(draws_p)
+    ms_p = timed(plain, iters)
     acc_p = plain.accept_rate()[0]
-    mom_p = chain_moments(plain, exact_plain) if exact_plain else None
+    mom_p = chain_moments(plain, exact_plain, exact_burn[0])
     div_p = plain.divergences()
     del plain
 
     sur = H.SurrogateHmc(d, HLR_C, L=HLR_L, eps=eps, jitter=0.1, seed=12, init=init, train_every=train_every,
-                         train_steps=train_steps)
-    sur.run(sur_warm)
-    H.adapt_step_size(sur, warm // 2)
+                         train_steps=train_steps, learn_iters=learn)
+    sur.run(learn)                        # online learning: the warm-up
+    eps_s = H.adapt_step_size(sur, warm // 2)
     sur.capture()
     sur.reset_stats()
     g0, l0 = sur.n_grad, sur.n_logp
-    rec_s, ms_s = timed(sur, iters)
-    draws_s = rec_s.cpu().numpy()
-    ess_s = ess(draws_s)
+    ms_s = timed(sur, iters)
     acc_s = sur.accept_rate()[0]
-    mom_s = chain_moments(sur, exact_sur) if exact_sur else None
+    passes = {"grad": sur.n_grad - g0, "logp_only": sur.n_logp - l0, "plain_grad": iters * HLR_L}
+    mom_s = chain_moments(sur, exact_sur, exact_burn[1])
     div_s = sur.divergences()
 
-    # posterior moments: both samplers target the same posterior; compared on
-    # the long continuation runs (chain means) when they were made
-    if mom_s is not None and mom_p is not None:
-        exact = exactness_stats(mom_s, mom_p)
-        exact["iterations"] = {"plain": exact_plain, "surrogate": exact_sur}
-    else:
-        mp, ms_ = draws_p.reshape(-1, HLR_D).mean(0), draws_s.reshape(-1, HLR_D).mean(0)
-        sd = draws_p.reshape(-1, HLR_D).std(0)
-        z = (ms_ - mp) / np.sqrt(sd ** 2 / ess_p + sd ** 2 / ess_s)
-        exact = {"posterior_mean_diff_in_sd": float(np.max(np.abs(ms_ - mp) / sd)),
-                 "posterior_mean_z_max": float(np.max(np.abs(z))),
-                 "posterior_mean_mc_sd": float(np.median(np.sqrt(1.0 / ess_p + 1.0 / ess_s)))}
-    v_p = ess_p.min() / (ms_p / 1e3)
-    v_s = ess_s.min() / (ms_s / 1e3)
+    exact = exactness_stats(mom_s, mom_p)
+    exact["iterations"] = {"plain": exact_plain, "surrogate": exact_sur}
+    exact["burn_in"] = {"plain": exact_burn[0], "surrogate": exact_burn[1]}
+    ess_p, ess_s = ess_chain_means(mom_p), ess_chain_means(mom_s)
+    v_p = ess_p.min() / (exact_plain * ms_p / 1e3)
+    v_s = ess_s.min() / (exact_sur * ms_s / 1e3)
     return {
-        "metric": "min-ESS/sec (surrogate-gradient HMC, HLR)", "value": v_s, "unit": "min-ESS/s",
-        "plain_hmc_value": v_p, "gain_vs_plain": v_s / v_p,
-        "iterations": iters, "chains": HLR_C, "leapfrog_steps": HLR_L, "step_size": eps,
-        "ms_per_iteration": {"surrogate": ms_s / iters, "plain": ms_p / iters},
-        "min_ess": {"surrogate": float(ess_s.min()), "plain": float(ess_p.min())},
+        "metric": "min-ESS/sec (surrogate-gradient HMC, HLR)", "value": float(v_s), "unit": "min-ESS/s",
+        "plain_hmc_value": float(v_p), "gain_vs_plain": float(v_s / v_p),
+        "iterations_timed": iters, "chains": HLR_C, "leapfrog_steps": HLR_L,
+        "step_size": {"plain": eps, "surrogate": eps_s},
+        "ms_per_iteration": {"surrogate": ms_s, "plain": ms_p},
+        "min_ess": {"surrogate": float(ess_s.min()), "plain": float(ess_p.min()),
+                    "estimator": "chain means of 256 chains over the exactness windows"},
+        "autocorrelation_time_max": {"surrogate": float(HLR_C * exact_sur / ess_s.min()),
+                                     "plain": float(HLR_C * exact_plain / ess_p.min())},
         "accept": {"surrogate": float(acc_s), "plain": float(acc_p)},
-        "surrogate_rel_err": sur.last_rel_err, "fallback": sur.fallback,
-        "exact_passes": {"grad": sur.n_grad - g0, "logp_only": sur.n_logp - l0, "plain_grad": iters * HLR_L},
+        "surrogate_rel_err": sur.last_rel_err, "fallback": sur.fallback, "max_rel_err": sur.max_rel_err,
+        "exact_passes": passes,
         "exactness": exact,
         "posterior_mean_diff_in_sd": exact["posterior_mean_diff_in_sd"],
         "divergences": {"surrogate": div_s, "plain": div_p},
@@ -682,10 +703,10 @@ def run_hlr_surrogate(iters=100, warm=40, sur_warm=60, train_every=8, train_step
                      "note": "algorithmic 2 x 2 N D C (forward and backward product); executed on the tensor "
                              "pipe 5 x 2 N D C: three bf16 parts of theta forward, two of the residual backward"},
         "config": {"workload": "hlr_surrogate_n2000000_d512_c256", "N": HLR_N, "D": HLR_D, "chains": HLR_C,
-                   "x_dtype": "bf16", "prior": "student_t(3)", "mlp": "512-256-256-512 gelu, bf16 weights",
+                   "x_dtype": "bf16", "prior": "student_t(3)",
+                   "mlp": "512-256-256-512 gelu, bf16 weights, over a dense least-squares linear part",
                    "init": "generating coefficients + N(0, 1e-6), then the plain sampler's warm-up",
-                   "launch_shape": tuned,
-                   "warmup": warm, "surrogate_warmup": sur_warm,
+                   "launch_shape": tuned, "warmup": warm, "surrogate_learning_iterations": learn,
                    "train_every": train_every, "train_steps": train_steps},
     }
 
@@ -752,7 +773,8 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- dominant kernel (z resample) timed alone for the roofline
     z_ms = time_z_kernel(s, stream, flush, reps=max(5, min(args.steps, 30)))
-    alg_bytes = T * (4 + 4 + 8 + K_TOPICS * 8) + D_DOCS * K_TOPICS * 12
+    # the screened z kernel reads a binary32 phi row (4 K bytes) per token
+    alg_bytes = T * (4 + 4 + 8 + K_TOPICS * 4) + D_DOCS * K_TOPICS * 12
     hbm, peak_kind = measured_peaks()
     achieved = alg_bytes / (z_ms / 1e3) / 1e9
 
@@ -781,16 +803,23 @@ def run_ours(args, rank, world, local_rank):
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64+int32", "data": "synthetic (LDA generative process, seed 0)",
             "config": cfg, "tokens_per_step": T,
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": 5 * args.steps,
             "clocks": clocks.summary(),
-            "roofline": {"bound": "hbm", "kernel": "lda_zq_kernel<13> (K=50)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "lda_zf_kernel<7> (K=50, binary32-screened z draw)",
+                         "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": peak_kind, "traffic": Z_KERNEL_DRAM_BYTES,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch "
-                                           "(profiles/lda_zq_kernel_k50_v10000_d2000.md)",
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of "
+                                           "this kernel on this workload (the capture summarised with its "
+                                           "command in profiles/)",
                          "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": z_ms,
-                         "note": "algorithmic bytes per token = 4 w + 4 z + 8 count RMW + 8K phi row"},
+                         "note": "algorithmic bytes per token = 4 w + 4 z + 8 count RMW + 4K binary32 phi row, "
+                                 "plus 12 D K per launch (theta rows, document counts)"},
+            # the whole sweep against the 442 B/token byte model of the
+            # binary64 formulation (4 w + 4 z + 8 (z, w) re-read + 8 count RMW
+            # + 8K phi row, plus the count tables and draws per sweep)
             "sweep_roofline_frac": (T * 442.0) / (ms_max / args.steps / 1e3) / 1e9 / hbm,
+            "sweep_critical_path": "phi first tries -> phi fix-up + normalise (theta beside them) -> z",
             "e2e": e2e,
         }
         if world == 1 and not args.no_cpu_baseline:
@@ -819,12 +848,16 @@ def run_ours(args, rank, world, local_rank):
 
 
 def time_z_kernel(s, stream, flush, reps):
-    """Average duration of the production z launch (ab_lda_disc_z with both
-    count tables, the launch the sweep makes), L2 flushed and the topic-word
-    table zeroed before each launch, outside its events."""
+    """Average duration of the production z launch - the binary32-screened
+    kernel the sweep runs (ab_lda_disc_z_f32 on the sampler's own binary32
+    copy of phi), with both count tables - L2 flushed and the topic-word table
+    zeroed before each launch, outside its events."""
     import torch
     from augurv2_b200 import _native as N
     L = N.lib()
+    Kq = L.ab_lda_phi32_stride(s.K)
+    off32 = (int(L.ab_lda_phi_scratch_bytes(s.K, s.V)) + 255) & ~255
+    phi32 = s.scratch[off32:off32 + 4 * s.V * Kq].view(torch.float32)
     z = s.z.clone()
     cdk = torch.zeros_like(s.cnt_dk)
     ckw = torch.zeros_like(s.cnt_kw)
@@ -835,9 +868,9 @@ def time_z_kernel(s, stream, flush, reps):
             ckw.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            N.check(L.ab_lda_disc_z(s.D, s.K, s.V, N.ptr(s.doc_off), N.ptr(s.w), N.ptr(s.theta),
-                                    N.ptr(s.phiT), N.ptr(z), N.ptr(cdk), N.ptr(ckw), s.seed, 0,
-                                    N.stream_ptr(stream)), "disc_z")
+            N.check(L.ab_lda_disc_z_f32(s.D, s.K, s.V, N.ptr(s.doc_off), N.ptr(s.w), N.ptr(s.theta),
+                                        N.ptr(s.phiT), N.ptr(phi32), N.ptr(z), N.ptr(cdk), N.ptr(ckw), s.seed, 0,
+                                        N.stream_ptr(stream)), "disc_z_f32")
             b.record(stream)
             evs.append((a, b))
     torch.cuda.synchronize()
@@ -952,9 +985,9 @@ def main():
     ap.add_argument("--hlr-iters", type=int, default=100)
     ap.add_argument("--train-every", type=int, default=8, help="surrogate: exact check + training period")
     ap.add_argument("--train-steps", type=int, default=10, help="surrogate: Adam steps per check")
-    ap.add_argument("--exact-plain", type=int, default=1500,
+    ap.add_argument("--exact-plain", type=int, default=1000,
                     help="surrogate exactness: iterations of the plain sampler's continuation (0: skip)")
-    ap.add_argument("--exact-sur", type=int, default=4000,
+    ap.add_argument("--exact-sur", type=int, default=3000,
                     help="surrogate exactness: iterations of the surrogate sampler's continuation")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)

@@ -173,8 +173,11 @@ def test_sweep_runner_reference_fixture(orc):
     s.close()
 
 
-def test_sweep_runner_synthetic_graph_vs_eager(orc):
-    K, V, D = 20, 500, 60
+@pytest.mark.parametrize("K", [20, 100])
+def test_sweep_runner_synthetic_graph_vs_eager(orc, K):
+    """K = 20 runs the binary32-screened z kernel and the three-kernel phi
+    draw, K = 100 the binary64 kernels; both meet the per-sweep contract."""
+    V, D = 500, 60
     off, w = synthetic_corpus(K, V, D, 50, 0.1, 0.01, seed=11)
     alpha, beta = np.full(K, 0.1), np.full(V, 0.01)
     z0 = np.random.default_rng(1).integers(0, K, size=len(w)).astype(np.int32)
@@ -291,8 +294,8 @@ def test_sweep_phi32_copy_is_phi_rounded():
     L = N.lib()
     Kq = L.ab_lda_phi32_stride(K)
     raw = s.scratch.cpu().numpy()
-    nbytes = 4 * V * Kq
-    phi32 = raw[len(raw) - nbytes:].view(np.float32).reshape(V, Kq)
+    off32 = (int(L.ab_lda_phi_scratch_bytes(K, V)) + 255) & ~255     # after the phi draw's scratch
+    phi32 = raw[off32:off32 + 4 * V * Kq].view(np.float32).reshape(V, Kq)
     phi = s.state()[1]
     np.testing.assert_array_equal(phi32[:, :K], phi.T.astype(np.float32))
     assert (phi32[:, K:] == 0).all()
