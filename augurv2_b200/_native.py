@@ -126,6 +126,16 @@ _SIGS = {
     "ab_nutsb_advance": (i32, [vp, i32, i32, i32, i32, f64, u64, u32, vp, vp, vp]),
     "ab_nutsb_advance_variant": (i32, [vp, i32, i32, i32, i32, f64, u64, u32, i32, vp, vp, vp]),
     "ab_nutsb_info": (i32, [vp, i32, i32, i32, vp, vp]),
+    "ab_hlrg_create": (i32, [i32, vp, vp, vp]),
+    "ab_hlrg_bind": (i32, [vp, i32, vp, i32, vp, vp, i32]),
+    "ab_hlrg_set_active": (i32, [vp, vp, vp]),
+    "ab_hlrg_logp_grad": (i32, [vp, vp, vp]),
+    "ab_hlrg_destroy": (i32, [vp]),
+    "ab_nutsg_create": (i32, [i32, vp, vp]),
+    "ab_nutsg_set_active": (i32, [vp, vp, vp]),
+    "ab_nutsg_advance": (i32, [vp, vp]),
+    "ab_nutsg_min_draws": (i32, [vp, vp, vp]),
+    "ab_nutsg_destroy": (i32, [vp]),
     "ab_hmcb_begin": (i32, [vp, vp]),
     "ab_hmcb_step": (i32, [vp, vp, vp]),
     "ab_hmcb_final": (i32, [vp, vp, vp, vp]),

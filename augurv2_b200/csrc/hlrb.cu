@@ -37,6 +37,7 @@
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
+#include "tc_group.cuh"
 #include "tc_host.cuh"
 
 namespace ab {
@@ -112,11 +113,6 @@ Layout layout(int N, int D, int C, const ab_hlrb_config* cfg) {
   return L;
 }
 
-__device__ __forceinline__ void split2(float x, __nv_bfloat16& h, __nv_bfloat16& m) {
-  h = __float2bfloat16_rn(x);
-  m = __float2bfloat16_rn(x - __bfloat162float(h));   // the difference is exact in FP32
-}
-
 __device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
   h = __float2bfloat16_rn(x);
   const float r1 = x - __bfloat162float(h);   // exact in FP32
@@ -126,21 +122,25 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& h, __nv_bfloat16&
 }
 
 // theta [C][ldt] f32 -> Theta3 [C][3][Dp] bf16 (hi, mid, lo; zero padding).
+__device__ __forceinline__ void split_elem(int c, int d, int D, int Dp, const float* __restrict__ theta, int ldt,
+                                          __nv_bfloat16* __restrict__ t3) {
+  __nv_bfloat16 h, m, l;
+  if (d < D) {
+    split3(theta[(size_t)c * ldt + d], h, m, l);
+  } else {
+    h = m = l = __float2bfloat16_rn(0.0f);
+  }
+  __nv_bfloat16* row = t3 + (size_t)c * 3 * Dp;
+  row[d] = h;
+  row[Dp + d] = m;
+  row[2 * Dp + d] = l;
+}
+
 __global__ void hlrb_split_kernel(int C, int D, int Dp, const float* __restrict__ theta, int ldt,
                                   __nv_bfloat16* __restrict__ t3) {
   const int c = blockIdx.y;
-  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < Dp; d += gridDim.x * blockDim.x) {
-    __nv_bfloat16 h, m, l;
-    if (d < D) {
-      split3(theta[(size_t)c * ldt + d], h, m, l);
-    } else {
-      h = m = l = __float2bfloat16_rn(0.0f);
-    }
-    __nv_bfloat16* row = t3 + (size_t)c * 3 * Dp;
-    row[d] = h;
-    row[Dp + d] = m;
-    row[2 * Dp + d] = l;
-  }
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < Dp; d += gridDim.x * blockDim.x)
+    split_elem(c, d, D, Dp, theta, ldt, t3);
 }
 
 // X [N][ldx] -> Xt [Np/64][D][64], zero for n >= N.  32x32 tiles through
@@ -164,6 +164,18 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
 // Forward epilogue: rows are chains, columns are data rows.  LL: sum the
 // log-likelihood terms; R: write the residual parts for the backward pass
 // (a leapfrog step that only needs the gradient skips the LL work).
+//
+// With s = 2y - 1 and u = s t, the Bernoulli-logit term and residual are
+//   y t - softplus(t) = min(u, 0) - log(1 + e),   e = exp(-|t|),
+//   y - sigmoid(t)    = s * (u >= 0 ? e : 1) / (1 + e),
+// one MUFU exp2, log2 and reciprocal each (hardware exp2 / log2: the
+// absolute log-density error at N = 2e6 is 0.037 nats, 4e-8 relative, and
+// its chain-to-chain differences - what an accept test sees - are 0.004).
+// The 32 terms of a column chunk are summed in four interleaved FP32
+// partials (min(u, 0) and log2(1 + e) kept apart; both parts of a term
+// have the same sign, so nothing cancels), and the chunk sums go into a
+// Kahan-compensated running sum per chain and column group.  Rows at or
+// past N carry s = 0: no term, zero residual.
 template <bool LL, bool R, int W, int BN>
 struct FwdEpi {
   static constexpr int kSmem = BN * 4;
@@ -174,64 +186,79 @@ struct FwdEpi {
   float* llpart;       // [fwd_tiles][kGroups][C]
   int N, Np, C;
   // per-thread state
-  const int* ys;
+  const float* ss;     // s = 2y - 1 of the tile's rows (0 past N), shared memory
   int n0;
   float acc, comp;
 
   __device__ void begin(int, int nt, int, char* smem, int etid) {
-    int* s = reinterpret_cast<int*>(smem);
+    float* s = reinterpret_cast<float*>(smem);
     n0 = nt * BN;
     for (int j = etid; j < BN; j += 32 * W) {
       const int n = n0 + j;
-      s[j] = n < N ? y[n] : -1;
+      s[j] = n < N ? (y[n] ? 1.0f : -1.0f) : 0.0f;
     }
-    ys = s;
+    ss = s;
     acc = 0.0f;
     comp = 0.0f;
   }
 
-  __device__ void rows(int c, int col0, const float* v, bool ok) {
-    if (!ok) return;
-    float rv[32];
+  template <bool FULL>
+  __device__ __forceinline__ void chunk(const float* v, const float* sv, float* rv) {
+    float s1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, s2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
-      const int yv = ys[col0 - n0 + i];
-      const float t = v[i];
-      float r = 0.0f;
-      if (yv >= 0) {
-        // hardware exp2 / log2 (one MUFU each): the absolute log-density
-        // error at N = 2e6 is 0.037 nats (4e-8 relative) against 0.006 for
-        // the library functions, and its chain-to-chain differences - what
-        // an accept test sees - are the same 0.004; the pass is 32 % faster
-        const float e = __expf(-fabsf(t));
-        if (LL) {
-          const float sp = fmaxf(t, 0.0f) + __logf(1.0f + e);   // softplus(t)
-          const float term = yv ? t - sp : -sp;
-          // Kahan-compensated running sum of this chain's terms
-          const float yk = term - comp;
-          const float tk = acc + yk;
-          comp = (tk - acc) - yk;
-          acc = tk;
-        }
-        if (R) {
-          const float inv = __fdividef(1.0f, 1.0f + e);   // 1/(1+e), 1+e in (1, 2]
-          const float sig = t >= 0.0f ? inv : e * inv;
-          r = (float)yv - sig;
-        }
+      const float t = v[i], sg = sv[i];
+      const float u = sg * t;
+      const float e = __expf(-fabsf(t));
+      const float ope = 1.0f + e;   // in (1, 2]
+      if (LL) {
+        s1[i & 3] += fminf(u, 0.0f);
+        const float l2 = __log2f(ope);
+        s2[i & 3] += (FULL || sg != 0.0f) ? l2 : 0.0f;
       }
-      rv[i] = r;
+      if (R) {
+        const float inv = __fdividef(1.0f, ope);
+        rv[i] = sg * (u >= 0.0f ? e * inv : inv);
+      }
     }
+    if (LL) {
+      const float part = ((s1[0] + s1[1]) + (s1[2] + s1[3])) -
+                         0.69314718055994531f * ((s2[0] + s2[1]) + (s2[2] + s2[3]));
+      const float yk = part - comp;   // Kahan-compensated running sum
+      const float tk = acc + yk;
+      comp = (tk - acc) - yk;
+      acc = tk;
+    }
+  }
+
+  __device__ void rows(int c, int col0, const float* v, bool ok) {
+    if (!ok) return;
+    float rv[32], sv[32];
+    const float4* s4 = reinterpret_cast<const float4*>(ss + (col0 - n0));
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 a = s4[q];
+      sv[4 * q] = a.x;
+      sv[4 * q + 1] = a.y;
+      sv[4 * q + 2] = a.z;
+      sv[4 * q + 3] = a.w;
+    }
+    if (col0 + 32 <= N) chunk<true>(v, sv, rv);   // uniform over the warp
+    else chunk<false>(v, sv, rv);
     if (R && col0 < Np) {
-      // K-blocked [Np/64][2][C][64]: part p of chain c for rows col0..col0+31
+      // K-blocked [Np/64][2][C][64]: part p of chain c for rows col0..col0+31;
+      // hi = bf16(r), mid = bf16(r - hi) (the difference is exact in FP32),
+      // converted two at a time
       __nv_bfloat16* base = r3 + ((size_t)(col0 >> 6) * R_PARTS * C + c) * 64 + (col0 & 63);
       uint32_t ph[16], pm[16];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        __nv_bfloat16 h0, m0, h1, m1;
-        split2(rv[2 * i], h0, m0);
-        split2(rv[2 * i + 1], h1, m1);
-        ph[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-        pm[i] = (uint32_t)__bfloat16_as_ushort(m0) | ((uint32_t)__bfloat16_as_ushort(m1) << 16);
+        const __nv_bfloat162 h = __floats2bfloat162_rn(rv[2 * i], rv[2 * i + 1]);
+        const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
+        const float h0 = __uint_as_float(hb << 16), h1 = __uint_as_float(hb & 0xffff0000u);
+        const __nv_bfloat162 m = __floats2bfloat162_rn(rv[2 * i] - h0, rv[2 * i + 1] - h1);
+        ph[i] = hb;
+        pm[i] = *reinterpret_cast<const uint32_t*>(&m);
       }
       uint4* dh = reinterpret_cast<uint4*>(base);
       uint4* dm = reinterpret_cast<uint4*>(base + (size_t)C * 64);
@@ -285,14 +312,12 @@ __device__ __forceinline__ void prior_term(int kind, double a, double b, double 
 
 // One block per chain: logp[c] (FP64) and grad[c][0..D-1] (FP32) from the
 // partials, in a fixed order; either output may be NULL.
-__global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_tiles, int splits, int ldw,
-                                                          const float* __restrict__ llpart,
-                                                          const float* __restrict__ w, const float* __restrict__ theta,
-                                                          int ldt, int prior, double pa, double pb,
-                                                          double* __restrict__ logp, float* __restrict__ grad,
-                                                          int ldg) {
+__device__ __forceinline__ void finish_chain(int c, int C, int D, int fwd_tiles, int splits, int ldw,
+                                             const float* __restrict__ llpart, const float* __restrict__ w,
+                                             const float* __restrict__ theta, int ldt, int prior, double pa,
+                                             double pb, double* __restrict__ logp, float* __restrict__ grad,
+                                             int ldg) {
   __shared__ double red[33];
-  const int c = blockIdx.x;
   double s = 0.0;
   if (logp)
     for (int t = threadIdx.x; t < fwd_tiles; t += blockDim.x) s += (double)llpart[(size_t)t * C + c];
@@ -308,6 +333,15 @@ __global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_
   }
   s = block_sum_f64(s, red);
   if (logp && threadIdx.x == 0) logp[c] = s;
+}
+
+__global__ void __launch_bounds__(256) hlrb_finish_kernel(int C, int D, int fwd_tiles, int splits, int ldw,
+                                                          const float* __restrict__ llpart,
+                                                          const float* __restrict__ w, const float* __restrict__ theta,
+                                                          int ldt, int prior, double pa, double pb,
+                                                          double* __restrict__ logp, float* __restrict__ grad,
+                                                          int ldg) {
+  finish_chain(blockIdx.x, C, D, fwd_tiles, splits, ldw, llpart, w, theta, ldt, prior, pa, pb, logp, grad, ldg);
 }
 
 }  // namespace
@@ -436,4 +470,252 @@ extern "C" int ab_hlrb_logp_grad_cfg(const ab_hlrb_model* m, int C, const float*
 extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* theta, int ldt, double* logp,
                                  float* grad, int ldg, void* work, int* err, void* stream) {
   return ab_hlrb_logp_grad_cfg(m, C, theta, ldt, logp, grad, ldg, nullptr, work, err, stream);
+}
+
+// ---- grouped pass: many instances, one launch per stage ---------------------
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace ab {
+namespace {
+
+using GFwd = FwdEpi<true, true, 8, 256>;   // the built-in forward shape, logp and gradient
+constexpr int G_BWD_BN = 128;              // widest backward tile; each instance uses its own bwd_bn(D)
+
+struct GSplit {
+  const float* theta;
+  __nv_bfloat16* t3;
+  int ldt, C, D, Dp;
+};
+
+struct GFinish {
+  const float* llpart;
+  const float* w;
+  const float* theta;
+  double* logp;
+  float* grad;
+  double pa, pb;
+  int C, D, fwd_parts, splits, ldw, ldt, prior, ldg;
+};
+
+// The launch header: problems in use and tiles of the forward and backward
+// GEMMs (the split and finish kernels read n from the forward's).
+struct GHeads {
+  tc::GHead fwd, bwd;
+};
+
+__global__ void hlrg_split_kernel(const GSplit* __restrict__ tab, const GHeads* __restrict__ head) {
+  if ((int)blockIdx.z >= head->fwd.n) return;
+  const GSplit q = tab[blockIdx.z];
+  const int c = blockIdx.y;
+  if (c >= q.C) return;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < q.Dp; d += gridDim.x * blockDim.x)
+    split_elem(c, d, q.D, q.Dp, q.theta, q.ldt, q.t3);
+}
+
+__global__ void __launch_bounds__(256) hlrg_finish_kernel(const GFinish* __restrict__ tab,
+                                                          const GHeads* __restrict__ head) {
+  if ((int)blockIdx.y >= head->fwd.n) return;
+  const GFinish q = tab[blockIdx.y];
+  if ((int)blockIdx.x >= q.C) return;
+  finish_chain(blockIdx.x, q.C, q.D, q.fwd_parts, q.splits, q.ldw, q.llpart, q.w, q.theta, q.ldt, q.prior, q.pa, q.pb,
+               q.logp, q.grad, q.ldg);
+}
+
+struct HlrgInst {
+  ab_hlrb_model m;
+  int C;
+  Layout L;
+  char* work;
+  tc::GProblem fwd, bwd;
+  GFwd fe;
+  GradEpi ge;
+  const float* theta = nullptr;
+  double* logp = nullptr;
+  float* grad = nullptr;
+  int ldt = 0, ldg = 0;
+};
+
+inline size_t al256(size_t a) { return (a + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace ab
+
+struct ab_hlrg {
+  std::vector<ab::HlrgInst> inst;
+  int C_max = 0, Dp_max = 0, grid_fwd = 0, grid_bwd = 0, n_active = 0;
+  bool ready = false;
+  char* work = nullptr;    // every instance's workspace
+  char* tab = nullptr;     // device tables
+  size_t o_fwd = 0, o_bwd = 0, o_fe = 0, o_ge = 0, o_sp = 0, o_fin = 0, bytes = 0;
+  unsigned char* stage = nullptr;   // host copy of the tables (256-byte aligned)
+  ~ab_hlrg() { std::free(stage); }
+};
+
+extern "C" int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, ab_hlrg** out) {
+  using namespace ab;
+  AB_REQUIRE(out && models && C, AB_ERR_ARG, "ab_hlrg_create: null argument");
+  *out = nullptr;
+  AB_REQUIRE(n >= 1 && n <= tc::GROUP_MAX, AB_ERR_ARG, "ab_hlrg_create: n must be 1..%d (got %d)", tc::GROUP_MAX, n);
+  std::unique_ptr<ab_hlrg> g(new ab_hlrg());
+  g->inst.resize(n);
+  size_t wtot = 0;
+  std::vector<size_t> woff(n);
+  long long fwd_tiles = 0, bwd_tiles = 0;
+  for (int i = 0; i < n; ++i) {
+    int rc = hlrb_check_model(&models[i]);
+    if (rc) return rc;
+    AB_REQUIRE(C[i] > 0 && C[i] <= 65535, AB_ERR_ARG, "ab_hlrg_create: instance %d: C must be 1..65535", i);
+    AB_REQUIRE(models[i].D % 8 == 0, AB_ERR_ARG, "ab_hlrg_create: instance %d: D must be a multiple of 8", i);
+    HlrgInst& q = g->inst[i];
+    q.m = models[i];
+    q.C = C[i];
+    q.L = layout(q.m.N, q.m.D, q.C, nullptr);
+    AB_REQUIRE(q.L.fwd_bn == 256 && q.L.groups == 2 && q.L.bn <= G_BWD_BN, AB_ERR_STATE,
+               "ab_hlrg_create: built-in launch shape changed");
+    woff[i] = wtot;
+    wtot = al256(wtot + q.L.total);
+    g->C_max = std::max(g->C_max, q.C);
+    g->Dp_max = std::max(g->Dp_max, q.L.Dp);
+  }
+  AB_CUDA(cudaMalloc(&g->work, wtot));
+  for (int i = 0; i < n; ++i) {
+    HlrgInst& q = g->inst[i];
+    const Layout& L = q.L;
+    q.work = g->work + woff[i];
+    __nv_bfloat16* t3 = reinterpret_cast<__nv_bfloat16*>(q.work + L.off_t3);
+    __nv_bfloat16* r3 = reinterpret_cast<__nv_bfloat16*>(q.work + L.off_r3);
+    float* llp = reinterpret_cast<float*>(q.work + L.off_ll);
+    float* w = reinterpret_cast<float*>(q.work + L.off_w);
+    int rc;
+    if ((rc = tc::encode_2d_bf16(&q.fwd.ta, t3, q.C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
+    if ((rc = tc::encode_2d_bf16(&q.fwd.tb, q.m.X, q.m.N, q.m.D, q.m.ldx, L.fwd_bn))) return rc;
+    q.fwd.sh = tc::make_shape(q.C, q.m.N, q.m.D, 1, tc::row_major(L.Dp), tc::row_major(0), L.fwd_bn);
+    q.fwd.bn = L.fwd_bn;
+    const int nb = L.Np / 64;
+    if ((rc = tc::encode_2d_bf16(&q.bwd.ta, r3, (uint64_t)nb * R_PARTS * q.C, 64, 64, tc::BM))) return rc;
+    if ((rc = tc::encode_2d_bf16(&q.bwd.tb, q.m.Xt, (uint64_t)nb * q.m.D, 64, 64, L.bn))) return rc;
+    q.bwd.sh = tc::make_shape(q.C, q.m.D, q.m.N, L.splits, tc::k_blocked(R_PARTS, q.C), tc::k_blocked(1, q.m.D), L.bn);
+    AB_REQUIRE(q.bwd.sh.splits == L.splits, AB_ERR_STATE, "ab_hlrg_create: split arithmetic mismatch");
+    q.bwd.bn = L.bn;
+    q.fe = GFwd{q.m.y, r3, llp, q.m.N, L.Np, q.C, nullptr, 0, 0.0f, 0.0f};
+    q.ge = GradEpi{w, q.C, q.m.D, L.ldw, 0};
+    fwd_tiles += (long long)q.fwd.sh.m_tiles * q.fwd.sh.n_tiles * q.fwd.sh.splits;
+    bwd_tiles += (long long)q.bwd.sh.m_tiles * q.bwd.sh.n_tiles * q.bwd.sh.splits;
+  }
+  AB_REQUIRE(fwd_tiles < (1LL << 31) && bwd_tiles < (1LL << 31), AB_ERR_ARG, "ab_hlrg_create: too many tiles");
+  g->grid_fwd = (int)std::min<long long>(fwd_tiles, tc::sm_count());
+  g->grid_bwd = (int)std::min<long long>(bwd_tiles, tc::sm_count());
+  size_t o = al256(sizeof(GHeads));
+  g->o_fwd = o; o = al256(o + sizeof(tc::GProblem) * n);
+  g->o_bwd = o; o = al256(o + sizeof(tc::GProblem) * n);
+  g->o_fe = o;  o = al256(o + sizeof(GFwd) * n);
+  g->o_ge = o;  o = al256(o + sizeof(GradEpi) * n);
+  g->o_sp = o;  o = al256(o + sizeof(GSplit) * n);
+  g->o_fin = o; o = al256(o + sizeof(GFinish) * n);
+  g->bytes = o;
+  AB_CUDA(cudaMalloc(&g->tab, g->bytes));
+  AB_CUDA(cudaMemset(g->tab, 0, g->bytes));
+  g->stage = static_cast<unsigned char*>(std::aligned_alloc(256, g->bytes));
+  AB_REQUIRE(g->stage, AB_ERR_CUDA, "ab_hlrg_create: host allocation failed");
+  std::memset(g->stage, 0, g->bytes);
+  using GF = tc::GCfg<256, 3, 1, GFwd>::C;
+  using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
+  static_assert(GF::SMEM_BYTES <= tc::SMEM_BUDGET && GB::SMEM_BYTES <= tc::SMEM_BUDGET, "grouped tiles exceed shared memory");
+  AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<256, 3, 1, GFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               GF::SMEM_BYTES));
+  AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, GB::SMEM_BYTES));
+  *out = g.release();
+  return AB_OK;
+}
+
+extern "C" int ab_hlrg_bind(ab_hlrg* g, int i, const float* theta, int ldt, double* logp, float* grad, int ldg) {
+  AB_REQUIRE(g, AB_ERR_ARG, "ab_hlrg_bind: null group");
+  AB_REQUIRE(i >= 0 && i < (int)g->inst.size(), AB_ERR_ARG, "ab_hlrg_bind: no instance %d", i);
+  ab::HlrgInst& q = g->inst[i];
+  AB_REQUIRE(theta && logp && grad, AB_ERR_ARG, "ab_hlrg_bind: null pointer");
+  AB_REQUIRE(ldt >= q.m.D && ldg >= q.m.D, AB_ERR_ARG, "ab_hlrg_bind: leading dimension too small");
+  q.theta = theta;
+  q.ldt = ldt;
+  q.logp = logp;
+  q.grad = grad;
+  q.ldg = ldg;
+  g->ready = false;   // takes effect at the next ab_hlrg_set_active
+  return AB_OK;
+}
+
+extern "C" int ab_hlrg_set_active(ab_hlrg* g, const int* active, void* stream) {
+  using namespace ab;
+  AB_REQUIRE(g && active, AB_ERR_ARG, "ab_hlrg_set_active: null argument");
+  const int n = (int)g->inst.size();
+  unsigned char* h = g->stage;
+  tc::GProblem* fwd = reinterpret_cast<tc::GProblem*>(h + g->o_fwd);
+  tc::GProblem* bwd = reinterpret_cast<tc::GProblem*>(h + g->o_bwd);
+  GFwd* fe = reinterpret_cast<GFwd*>(h + g->o_fe);
+  GradEpi* ge = reinterpret_cast<GradEpi*>(h + g->o_ge);
+  GSplit* sp = reinterpret_cast<GSplit*>(h + g->o_sp);
+  GFinish* fin = reinterpret_cast<GFinish*>(h + g->o_fin);
+  int k = 0, tf = 0, tb = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!active[i]) continue;
+    const HlrgInst& q = g->inst[i];
+    AB_REQUIRE(q.theta, AB_ERR_STATE, "ab_hlrg_set_active: instance %d is active but not bound", i);
+    fwd[k] = q.fwd;
+    fwd[k].tile0 = tf;
+    tf += q.fwd.sh.m_tiles * q.fwd.sh.n_tiles * q.fwd.sh.splits;
+    bwd[k] = q.bwd;
+    bwd[k].tile0 = tb;
+    tb += q.bwd.sh.m_tiles * q.bwd.sh.n_tiles * q.bwd.sh.splits;
+    fe[k] = q.fe;
+    ge[k] = q.ge;
+    sp[k] = GSplit{q.theta, reinterpret_cast<__nv_bfloat16*>(q.work + q.L.off_t3), q.ldt, q.C, q.m.D, q.L.Dp};
+    fin[k] = GFinish{reinterpret_cast<const float*>(q.work + q.L.off_ll), reinterpret_cast<const float*>(q.work + q.L.off_w),
+                     q.theta, q.logp, q.grad, q.m.prior_a, q.m.prior_b, q.C, q.m.D, q.L.fwd_tiles * q.L.groups,
+                     q.L.splits, q.L.ldw, q.ldt, q.m.prior, q.ldg};
+    ++k;
+  }
+  GHeads* hd = reinterpret_cast<GHeads*>(h);
+  hd->fwd = tc::GHead{k, tf};
+  hd->bwd = tc::GHead{k, tb};
+  g->n_active = k;
+  AB_CUDA(cudaMemcpyAsync(g->tab, h, g->bytes, cudaMemcpyHostToDevice, as_stream(stream)));
+  g->ready = true;
+  return AB_OK;
+}
+
+extern "C" int ab_hlrg_logp_grad(ab_hlrg* g, int* err, void* stream) {
+  using namespace ab;
+  AB_REQUIRE(g, AB_ERR_ARG, "ab_hlrg_logp_grad: null group");
+  AB_REQUIRE(g->ready, AB_ERR_STATE, "ab_hlrg_logp_grad: call ab_hlrg_set_active after creating or binding");
+  cudaStream_t st = as_stream(stream);
+  const int n = (int)g->inst.size();
+  const GHeads* head = reinterpret_cast<const GHeads*>(g->tab);
+  hlrg_split_kernel<<<dim3(ceil_div(g->Dp_max, 256), g->C_max, n), 256, 0, st>>>(
+      reinterpret_cast<const GSplit*>(g->tab + g->o_sp), head);
+  AB_LAUNCH_CHECK("hlrg_split_kernel");
+  using GF = tc::GCfg<256, 3, 1, GFwd>::C;
+  using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
+  tc::grouped_gemm_kernel<256, 3, 1, GFwd><<<g->grid_fwd, tc::threads_for(GFwd::kWarps), GF::SMEM_BYTES, st>>>(
+      reinterpret_cast<const tc::GProblem*>(g->tab + g->o_fwd), reinterpret_cast<const GFwd*>(g->tab + g->o_fe),
+      &head->fwd, err);
+  AB_LAUNCH_CHECK("grouped_gemm_kernel (forward)");
+  tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>
+      <<<g->grid_bwd, tc::threads_for(GradEpi::kWarps), GB::SMEM_BYTES, st>>>(
+          reinterpret_cast<const tc::GProblem*>(g->tab + g->o_bwd), reinterpret_cast<const GradEpi*>(g->tab + g->o_ge),
+          &head->bwd, err);
+  AB_LAUNCH_CHECK("grouped_gemm_kernel (backward)");
+  hlrg_finish_kernel<<<dim3(g->C_max, n), 256, 0, st>>>(reinterpret_cast<const GFinish*>(g->tab + g->o_fin), head);
+  AB_LAUNCH_CHECK("hlrg_finish_kernel");
+  return AB_OK;
+}
+
+extern "C" int ab_hlrg_destroy(ab_hlrg* g) {
+  if (!g) return AB_OK;
+  cudaFree(g->work);
+  cudaFree(g->tab);
+  delete g;
+  return AB_OK;
 }

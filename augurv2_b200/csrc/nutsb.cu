@@ -29,6 +29,10 @@
 // stream (seed, chain, iteration, NUTS | comp << 8).
 #include <math.h>
 
+#include <algorithm>
+#include <memory>
+#include <vector>
+
 #include "common.cuh"
 #include "philox.cuh"
 
@@ -94,11 +98,13 @@ struct NutsbDev {
 
 namespace {
 
-__global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) {
+// One chain's walk to its next leaf (one CTA of NB_THREADS threads), shared
+// by the per-sampler and the grouped launch.
+__device__ __forceinline__ void advance_chain(const NutsbDev& dv, const int c) {
   __shared__ ChainState S;
   __shared__ double red[33];
   __shared__ double dsh[2];
-  const int c = blockIdx.x, P = dv.P, tid = threadIdx.x;
+  const int P = dv.P, tid = threadIdx.x;
   if (tid == 0) S = dv.st[c];
   __syncthreads();
   const size_t o = (size_t)c * P;
@@ -406,6 +412,18 @@ __global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) 
   }
 }
 
+__global__ void __launch_bounds__(NB_THREADS) nutsb_advance_kernel(NutsbDev dv) { advance_chain(dv, blockIdx.x); }
+
+// Grouped advance: instance blockIdx.y of the first *n entries of tab, chain
+// blockIdx.x (the grid covers the largest chain count of the group).
+__global__ void __launch_bounds__(NB_THREADS) nutsg_advance_kernel(const NutsbDev* __restrict__ tab,
+                                                                   const int* __restrict__ n) {
+  if ((int)blockIdx.y >= *n) return;
+  const NutsbDev dv = tab[blockIdx.y];
+  if ((int)blockIdx.x >= dv.C) return;
+  advance_chain(dv, blockIdx.x);
+}
+
 }  // namespace
 }  // namespace ab
 
@@ -560,5 +578,115 @@ extern "C" int ab_nutsb_reset_history(void* mem, int C, int P, int hist_cap, voi
   NutsbDev d = layout(mem, C, P, hist_cap);
   nutsb_reset_history_kernel<<<ceil_div(C, 128), 128, 0, as_stream(stream)>>>(d);
   AB_LAUNCH_CHECK("nutsb_reset_history_kernel");
+  return AB_OK;
+}
+
+// ---- grouped NUTS: many samplers, one advance launch per round --------------
+namespace ab {
+namespace {
+// Per instance, over its chains: [2i] = the smallest draw count, [2i+1] = 1
+// if any chain reported an error.
+__global__ void nutsg_min_draws_kernel(const NutsbDev* __restrict__ tab, int* __restrict__ out) {
+  __shared__ int mn, bad;
+  const NutsbDev& d = tab[blockIdx.x];
+  if (threadIdx.x == 0) { mn = 0x7fffffff; bad = 0; }
+  __syncthreads();
+  int m = 0x7fffffff, e = 0;
+  for (int c = threadIdx.x; c < d.C; c += blockDim.x) {
+    m = min(m, d.st[c].ndraws);
+    e |= d.st[c].error;
+  }
+  atomicMin(&mn, m);
+  if (e) atomicOr(&bad, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = mn;
+    out[2 * blockIdx.x + 1] = bad;
+  }
+}
+}  // namespace
+}  // namespace ab
+
+struct ab_nutsg {
+  int n = 0, C_max = 0, n_active = 0;
+  std::vector<ab::NutsbDev> all;   // every instance, in creation order
+  ab::NutsbDev* d_all = nullptr;   // the same, on the device (min-draws queries)
+  ab::NutsbDev* d_act = nullptr;   // the active instances, compacted
+  int* d_n = nullptr;              // number of active instances
+};
+
+extern "C" int ab_nutsg_create(int n, const ab_nutsg_inst* insts, ab_nutsg** out) {
+  AB_REQUIRE(out && insts && n >= 1 && n <= 65535, AB_ERR_ARG, "ab_nutsg_create: bad arguments");
+  *out = nullptr;
+  std::unique_ptr<ab_nutsg> g(new ab_nutsg());
+  g->n = n;
+  for (int i = 0; i < n; ++i) {
+    const ab_nutsg_inst& q = insts[i];
+    AB_REQUIRE(q.state && q.logp_new && q.g_new && q.C > 0 && q.P > 0 && q.hist_cap >= 0, AB_ERR_ARG,
+               "ab_nutsg_create: instance %d: bad arguments", i);
+    AB_REQUIRE((reinterpret_cast<uintptr_t>(q.state) & 255) == 0, AB_ERR_ARG,
+               "ab_nutsg_create: instance %d: state must be 256-byte aligned", i);
+    AB_REQUIRE(q.variant == AB_NUTS_REFERENCE || q.variant == AB_NUTS_STANDARD, AB_ERR_ARG,
+               "ab_nutsg_create: instance %d: unknown variant %d", i, q.variant);
+    AB_REQUIRE(q.max_depth >= 1 && q.max_depth <= 14, AB_ERR_ARG,
+               "ab_nutsg_create: instance %d: max_depth must be 1..14", i);
+    AB_REQUIRE(q.eps > 0.0 && q.eps < 1e5, AB_ERR_ARG, "ab_nutsg_create: instance %d: bad step size", i);
+    NutsbDev d = layout(q.state, q.C, q.P, q.hist_cap);
+    d.max_depth = q.max_depth;
+    d.eps = (float)q.eps;
+    d.seed = q.seed;
+    d.comp = q.comp;
+    d.logp_new = q.logp_new;
+    d.g_new = q.g_new;
+    d.standard = q.variant == AB_NUTS_STANDARD;
+    g->all.push_back(d);
+    g->C_max = std::max(g->C_max, q.C);
+  }
+  const size_t tb = sizeof(NutsbDev) * (size_t)n;
+  AB_CUDA(cudaMalloc(&g->d_all, tb));
+  AB_CUDA(cudaMalloc(&g->d_act, tb));
+  AB_CUDA(cudaMalloc(&g->d_n, sizeof(int)));
+  AB_CUDA(cudaMemcpy(g->d_all, g->all.data(), tb, cudaMemcpyHostToDevice));
+  AB_CUDA(cudaMemcpy(g->d_act, g->all.data(), tb, cudaMemcpyHostToDevice));
+  g->n_active = n;
+  AB_CUDA(cudaMemcpy(g->d_n, &g->n_active, sizeof(int), cudaMemcpyHostToDevice));
+  *out = g.release();
+  return AB_OK;
+}
+
+extern "C" int ab_nutsg_set_active(ab_nutsg* g, const int* active, void* stream) {
+  AB_REQUIRE(g && active, AB_ERR_ARG, "ab_nutsg_set_active: null argument");
+  std::vector<NutsbDev> act;
+  for (int i = 0; i < g->n; ++i)
+    if (active[i]) act.push_back(g->all[i]);
+  g->n_active = (int)act.size();
+  cudaStream_t st = as_stream(stream);
+  if (!act.empty())
+    AB_CUDA(cudaMemcpyAsync(g->d_act, act.data(), sizeof(NutsbDev) * act.size(), cudaMemcpyHostToDevice, st));
+  AB_CUDA(cudaMemcpyAsync(g->d_n, &g->n_active, sizeof(int), cudaMemcpyHostToDevice, st));
+  // the host vectors are pageable: the copies have left them when the calls return
+  return AB_OK;
+}
+
+extern "C" int ab_nutsg_advance(ab_nutsg* g, void* stream) {
+  AB_REQUIRE(g, AB_ERR_ARG, "ab_nutsg_advance: null group");
+  nutsg_advance_kernel<<<dim3(g->C_max, g->n), NB_THREADS, 0, as_stream(stream)>>>(g->d_act, g->d_n);
+  AB_LAUNCH_CHECK("nutsg_advance_kernel");
+  return AB_OK;
+}
+
+extern "C" int ab_nutsg_min_draws(ab_nutsg* g, int* out, void* stream) {
+  AB_REQUIRE(g && out, AB_ERR_ARG, "ab_nutsg_min_draws: null argument");
+  nutsg_min_draws_kernel<<<g->n, 128, 0, as_stream(stream)>>>(g->d_all, out);
+  AB_LAUNCH_CHECK("nutsg_min_draws_kernel");
+  return AB_OK;
+}
+
+extern "C" int ab_nutsg_destroy(ab_nutsg* g) {
+  if (!g) return AB_OK;
+  cudaFree(g->d_all);
+  cudaFree(g->d_act);
+  cudaFree(g->d_n);
+  delete g;
   return AB_OK;
 }

@@ -145,6 +145,67 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// The same load in two halves: issue (the registers fill asynchronously) and
+// wait (tcgen05.wait::ld, with the registers passed through so that every
+// use of them comes after it).  At most one load per thread is outstanding
+// where these are used.
+#define AB_R32(r) "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), \
+    "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]),      \
+    "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),    \
+    "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait32(uint32_t* r) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : AB_R32(r) : : "memory");
+}
+#undef AB_R32
+
+// The epilogue's walk over the 32-column chunks [cbeg, cend) of one
+// accumulator (taddr: this warp's lane quarter at column 0): the next
+// chunk's tensor-memory load is issued before the current chunk goes to the
+// epilogue functor, so its latency hides behind that work.  have = false
+// hands zeros to the functor (an empty split or a failed wait); all
+// conditions are uniform over the warp, as tcgen05.ld requires.
+template <class Epi>
+__device__ __forceinline__ void epi_columns(Epi& e, uint32_t taddr, int cbeg, int cend, bool have, int row,
+                                            int col_base, bool row_ok) {
+  if (cbeg >= cend) return;
+  float v[32];
+  if (!have) {
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = 0.0f;
+    for (int c0 = cbeg; c0 < cend; c0 += 32) e.rows(row, col_base + c0, v, row_ok);
+    return;
+  }
+  uint32_t a[32], b[32];
+  tmem_ld32_issue(taddr + (uint32_t)cbeg, a);
+  tmem_wait32(a);
+  for (int c0 = cbeg;; c0 += 64) {
+    const bool m1 = c0 + 32 < cend, m2 = c0 + 64 < cend;
+    if (m1) tmem_ld32_issue(taddr + (uint32_t)(c0 + 32), b);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(a[k]);
+    e.rows(row, col_base + c0, v, row_ok);
+    if (!m1) break;
+    tmem_wait32(b);
+    if (m2) tmem_ld32_issue(taddr + (uint32_t)(c0 + 64), a);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(b[k]);
+    e.rows(row, col_base + c0 + 32, v, row_ok);
+    if (!m2) break;
+    tmem_wait32(a);
+  }
+}
+
 struct Addr {
   int x_kb, x_p, y_kb, y_p;
 };
@@ -319,16 +380,8 @@ gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUte
       const bool have = __all_sync(0xffffffffu, ok && kb1 > kb0 && !*(volatile int*)fail);
       const int row = mt * BM + q * 32 + lane;
       const bool row_ok = row < sh.M;
-      for (int c0 = cg * GCOLS; c0 < (cg + 1) * GCOLS; c0 += 32) {
-        float v[32];
-        if (have) {
-          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * C::ACC_COLS + c0), v);
-        } else {
-#pragma unroll
-          for (int k = 0; k < 32; ++k) v[k] = 0.0f;
-        }
-        e.rows(row, nt * BN + c0, v, row_ok);
-      }
+      epi_columns(e, tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * C::ACC_COLS), cg * GCOLS,
+                  (cg + 1) * GCOLS, have, row, nt * BN, row_ok);
       fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&acc_empty[ab]);

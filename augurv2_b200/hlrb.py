@@ -853,3 +853,141 @@ class NutsPool:
                 if ran(i) >= max_rounds or counts[i] >= min(min_draws, s.hist_cap):
                     self.done[i] = True
         return [ran(i) for i in range(len(self.samplers))]
+
+
+class NutsgInstC(C.Structure):
+    _fields_ = [("state", C.c_void_p), ("C", C.c_int), ("P", C.c_int), ("hist_cap", C.c_int),
+                ("max_depth", C.c_int), ("variant", C.c_int), ("eps", C.c_double), ("seed", C.c_uint64),
+                ("comp", C.c_uint32), ("logp_new", C.c_void_p), ("g_new", C.c_void_p)]
+
+
+class NutsGroup:
+    """Many BatchedNuts samplers of uneven size (model instances with their
+    own N and D) advanced together with ONE launch per stage: a round is one
+    grouped advance launch (every running instance's chains walk to their
+    next leaf, ab_nutsg_advance) and one grouped tensor-core pass over all of
+    their data sets (ab_hlrg_logp_grad: split, forward, backward and finish,
+    one launch each, the tiles of every instance sharing one persistent
+    grid), captured as one CUDA graph.  The pass uses the built-in launch
+    shape: results equal each sampler's own rounds with `data.config` None,
+    bit for bit.  An instance leaves the launches once every one of its
+    chains has `min_draws` draws (or its history is full, or it ran
+    `max_rounds` rounds in this call); the instance table lives in device
+    memory, so the captured graph follows the shrinking set without being
+    captured again."""
+
+    def __init__(self, samplers):
+        L = N.lib()
+        self.samplers = list(samplers)
+        n = len(self.samplers)
+        if n == 0:
+            raise ValueError("NutsGroup needs at least one sampler")
+        dev = self.samplers[0].data.device
+        models = (HlrbModelC * n)(*[s.data.c for s in self.samplers])
+        cs = (C.c_int * n)(*[s.C for s in self.samplers])
+        self._pass = C.c_void_p()
+        N.check(L.ab_hlrg_create(n, models, cs, C.byref(self._pass)), "ab_hlrg_create")
+        self._adv = C.c_void_p()
+        try:
+            for i, s in enumerate(self.samplers):
+                N.check(L.ab_hlrg_bind(self._pass, i, N.ptr(s.thprop), s.D, N.ptr(s.logp_new), N.ptr(s.g_new), s.D),
+                        "ab_hlrg_bind")
+            insts = (NutsgInstC * n)(*[NutsgInstC(s.mem.data_ptr(), s.C, s.D, s.hist_cap, s.max_depth,
+                                                  BatchedNuts.VARIANTS[s.variant], s.eps, s.seed, s.comp,
+                                                  s.logp_new.data_ptr(), s.g_new.data_ptr())
+                                       for s in self.samplers])
+            N.check(L.ab_nutsg_create(n, insts, C.byref(self._adv)), "ab_nutsg_create")
+        except Exception:
+            self.close()
+            raise
+        self.err = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.draw_buf = torch.zeros(2 * n, dtype=torch.int32, device=dev)
+        self.active = [True] * n
+        self.rounds = [s.rounds for s in self.samplers]
+        self.graph = None
+        self._set_active(self.active)
+
+    def _set_active(self, active, stream=None):
+        n = len(self.samplers)
+        a = (C.c_int * n)(*[1 if x else 0 for x in active])
+        N.check(N.lib().ab_hlrg_set_active(self._pass, a, N.stream_ptr(stream)), "ab_hlrg_set_active")
+        N.check(N.lib().ab_nutsg_set_active(self._adv, a, N.stream_ptr(stream)), "ab_nutsg_set_active")
+        self.active = list(active)
+
+    def _round(self, stream=None):
+        N.check(N.lib().ab_nutsg_advance(self._adv, N.stream_ptr(stream)), "ab_nutsg_advance")
+        N.check(N.lib().ab_hlrg_logp_grad(self._pass, N.ptr(self.err), N.stream_ptr(stream)), "ab_hlrg_logp_grad")
+
+    def _count(self, reps):
+        for i, a in enumerate(self.active):
+            if a:
+                self.rounds[i] += reps
+                self.samplers[i].rounds = self.rounds[i]
+
+    def capture(self):
+        """Run one round, then capture a round as a CUDA graph."""
+        self._round()
+        self._count(1)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._round(torch.cuda.current_stream())
+
+    def step(self, rounds=1):
+        """`rounds` rounds of every active instance."""
+        for _ in range(int(rounds)):
+            if self.graph is not None:
+                self.graph.replay()
+            else:
+                self._round()
+        self._count(int(rounds))
+
+    def min_draws(self):
+        """[n] smallest draw count over each instance's chains (raises if a
+        chain reported an error or the pass timed out)."""
+        N.check(N.lib().ab_nutsg_min_draws(self._adv, N.ptr(self.draw_buf), N.stream_ptr()), "ab_nutsg_min_draws")
+        d = self.draw_buf.cpu().numpy().reshape(-1, 2)
+        if d[:, 1].any() or int(self.err.item()):
+            raise N.AugurError("grouped NUTS: a chain reported an error or the pass timed out")
+        return d[:, 0]
+
+    def reset(self):
+        """Start a new phase: every instance runs again and its recorded
+        draws are forgotten (the chains keep their states)."""
+        for s in self.samplers:
+            s.reset_history()
+        self._set_active([True] * len(self.samplers))
+
+    @traced("nuts_group.run")
+    def run(self, min_draws, max_rounds, block=25):
+        """Rounds until every instance has min_draws draws per chain; returns
+        the rounds each instance ran in this call."""
+        start = list(self.rounds)
+        ran = lambda i: self.rounds[i] - start[i]
+        if self.graph is None:
+            self.capture()
+        self._set_active([True] * len(self.samplers))
+        while any(self.active):
+            reps = min(block, min(max_rounds - ran(i) for i, a in enumerate(self.active) if a))
+            if reps > 0:
+                self.step(reps)
+            d = self.min_draws()
+            act = [a and not (ran(i) >= max_rounds or d[i] >= min(min_draws, self.samplers[i].hist_cap))
+                   for i, a in enumerate(self.active)]
+            if act != self.active:
+                self._set_active(act)
+        return [ran(i) for i in range(len(self.samplers))]
+
+    def close(self):
+        self.graph = None
+        if getattr(self, "_adv", None):
+            N.lib().ab_nutsg_destroy(self._adv)
+            self._adv = None
+        if getattr(self, "_pass", None):
+            N.lib().ab_hlrg_destroy(self._pass)
+            self._pass = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

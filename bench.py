@@ -342,17 +342,19 @@ def nuts_cpu_baseline(per, chains, budget_s=12.0, max_nd=4_000_000):
                       "GPU run of the same algorithm" % (len(pts), time.perf_counter() - t_start)}
 
 
-def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INST, chains=NUTS_C, streams=8,
-                 hist_cap=128, variants=("reference", "standard"), share="equal", cpu=True):
+def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INST, chains=NUTS_C,
+                 hist_cap=128, variants=("reference", "standard"), cpu=True):
     """64 HLR instances (X ~ N(0,1) bf16, sigma^2 ~ InvGamma(1,1),
     beta ~ N(0, sigma^2 I), y ~ Bern(sigmoid(X beta)); sigma^2 held at its
     generating value), 512 NUTS chains each, max tree depth 10.  Every round
-    each instance advances all its chains to their next leaf and evaluates
-    one batched tensor-core pass; an instance's round is one CUDA graph, and
-    a NutsPool replays the instances' rounds over `streams` streams until
-    every chain of every instance has `min_draws` draws (instances with deep
-    trees run more rounds), after an untimed warm-up of `warmup_draws` draws
-    per chain whose draws are discarded.  min-ESS/s per instance = min-ESS
+    every running instance advances all its chains to their next leaf and
+    evaluates its log density and gradient there; a NutsGroup does this for
+    all instances with one advance launch and one grouped tensor-core pass
+    (one launch per stage, the tiles of every instance sharing one
+    persistent grid), captured as one CUDA graph, until every chain of every
+    instance has `min_draws` draws (instances with deep trees run more
+    rounds; finished instances leave the launches), after an untimed warm-up
+    of `warmup_draws` draws per chain whose draws are discarded.  min-ESS/s per instance = min-ESS
     of its draws / the whole run's device time; the line reports the minimum
     over instances.  Each selection rule in `variants` runs on the same data
     and starting points; the first is the line's value (the reference's
@@ -375,7 +377,6 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
         w = (torch.sigmoid(t) * (1 - torch.sigmoid(t))).mean().item()
         eps = 0.6 / np.sqrt(Ni * w + 1.0 / s2)       # ~ 0.6 of the posterior scale
         d = H.HlrbData(X, y, prior="normal", var=s2)
-        d.autotune(chains, tuner=bench_tuner())
         init = beta[None] + (0.1 * eps) * rng.standard_normal((chains, Di)).astype(np.float32)
         datas.append((d, eps, init))
         flops_round_i.append(4.0 * Ni * Di * chains)   # algorithmic: forward + backward product
@@ -384,14 +385,14 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
     for variant in variants:
         insts = [H.BatchedNuts(d, chains, eps=eps, max_depth=NUTS_DEPTH, seed=7 + i, init=init, hist_cap=hist_cap,
                                variant=variant) for i, (d, eps, init) in enumerate(datas)]
-        pool = H.NutsPool(insts, streams=streams)
+        pool = H.NutsGroup(insts)
         # warm-up (untimed, draws discarded): the chains leave their common start
-        pool.run(warmup_draws, max_rounds, share=share)
+        pool.run(warmup_draws, max_rounds)
         pool.reset()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        rounds = pool.run(min_draws, max_rounds, share=share)
+        rounds = pool.run(min_draws, max_rounds)
         b.record()
         torch.cuda.synchronize()
         ms = a.elapsed_time(b)
@@ -410,11 +411,13 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
             "seconds": ms / 1e3, "worst_instance": worst,
             "median_instance_min_ess_per_s": float(np.median([q["min_ess_per_s"] for q in per])),
             "total_draws": int(sum(q["draws_per_chain"] for q in per) * chains),
-            "roofline": {"bound": "tensor", "kernel": "gemm_kernel (batched passes, all instances)", "achieved": ach,
+            "roofline": {"bound": "tensor", "kernel": "grouped_gemm_kernel (forward + backward, all instances)",
+                         "achieved": ach,
                          "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "peak_source": kind + " (sustained)",
                          "note": "algorithmic 4 N D C per chain-round (forward and backward product); the tensor "
                                  "pipe executes 2.5x that (3 bf16 parts forward, 2 backward)"},
             "instances": per}
+        pool.close()
         del pool, insts
         torch.cuda.empty_cache()
     head = dict(results[variants[0]])
@@ -428,9 +431,9 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
                             "max_depth": NUTS_DEPTH, "x_dtype": "bf16", "N": "log-uniform [1e3, 1e6]",
                             "D": "{16, 64, 256}", "prior": "normal(0, sigma^2), sigma^2 at its generating value",
                             "step_size": "0.6 / sqrt(N E[w] + 1/sigma^2) at the generating coefficients",
-                            "streams": streams,
-                            "schedule": "NutsPool (%s shares): rounds until %d draws per chain, LPT streams"
-                                        % (share, min_draws)}})
+                            "schedule": "NutsGroup: one advance + one grouped pass (4 launches) per round for "
+                                        "all running instances, one CUDA graph; rounds until %d draws per chain"
+                                        % min_draws}})
     if cpu:
         head["cpu_baseline"] = nuts_cpu_baseline(results[variants[0]]["instances"], chains)
         head["gain_vs_cpu_core"] = head["value"] / head["cpu_baseline"]["value"]

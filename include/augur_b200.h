@@ -449,6 +449,56 @@ int ab_nutsb_info(void* state, int C, int P, int hist_cap, double* info, void* s
 int ab_nutsb_reset_history(void* state, int C, int P, int hist_cap, void* stream);
 
 /* ======================================================================= *
+ * Many instances in one launch per stage.  The reference runs one chain of
+ * one model per loaded library (process-global MCMC state,
+ * cbits/augur_mcmclib.h:44-45), so it has no counterpart for grouping; each
+ * instance's arithmetic is that of the single-instance calls above.
+ *
+ * ab_hlrg: the batched HLR pass (ab_hlrb_logp_grad with the built-in launch
+ * shape) for n instances, each with its own data set and C_i chains: one
+ * split, one forward, one backward and one finishing launch cover every
+ * active instance, the tensor-core tiles of all instances sharing one
+ * persistent grid.  Results equal each instance's own ab_hlrb_logp_grad
+ * (default launch shape) bit for bit.  The group owns the workspaces; bind
+ * each instance's theta [C_i][ldt] f32 input and logp [C_i] f64 / grad
+ * [C_i][ldg] f32 outputs, then ab_hlrg_set_active (active[i] != 0 takes part)
+ * before the first pass and after any change.  The tables live in device
+ * memory, so a CUDA graph captured around ab_hlrg_logp_grad follows later
+ * ab_hlrg_set_active calls.  D_i must be a multiple of 8; n <= 256.
+ * ======================================================================= */
+typedef struct ab_hlrg ab_hlrg;
+int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, ab_hlrg** out);
+int ab_hlrg_bind(ab_hlrg* g, int i, const float* theta, int ldt, double* logp, float* grad, int ldg);
+int ab_hlrg_set_active(ab_hlrg* g, const int* active, void* stream);
+int ab_hlrg_logp_grad(ab_hlrg* g, int* err, void* stream);
+int ab_hlrg_destroy(ab_hlrg* g);
+
+/* ab_nutsg: n batched-NUTS samplers advanced by one launch per round (each
+ * instance's chains walk to their next leaf exactly as
+ * ab_nutsb_advance_variant does, h_augur_mcmc_nuts,
+ * cbits/augur_mcmclib.h:575-776).  A round is ab_nutsg_advance followed by
+ * the caller's evaluation at every active instance's thprop (ab_hlrg for
+ * HLR), written to the instance's logp_new / g_new.  ab_nutsg_min_draws
+ * writes, for every instance (active or not), out[2i] = the smallest draw
+ * count over its chains and out[2i+1] = 1 if any chain reported an error
+ * (device int [2n]). */
+typedef struct ab_nutsg_inst {
+  void* state;              /* ab_nutsb_state_bytes buffer after ab_nutsb_init */
+  int C, P, hist_cap, max_depth, variant;
+  double eps;
+  uint64_t seed;
+  uint32_t comp;
+  const double* logp_new;   /* [C] at thprop, from the caller's evaluation */
+  const float* g_new;       /* [C][P] */
+} ab_nutsg_inst;
+typedef struct ab_nutsg ab_nutsg;
+int ab_nutsg_create(int n, const ab_nutsg_inst* insts, ab_nutsg** out);
+int ab_nutsg_set_active(ab_nutsg* g, const int* active, void* stream);
+int ab_nutsg_advance(ab_nutsg* g, void* stream);
+int ab_nutsg_min_draws(ab_nutsg* g, int* out, void* stream);
+int ab_nutsg_destroy(ab_nutsg* g);
+
+/* ======================================================================= *
  * Gradient-surrogate MLP (no counterpart in the reference): d_in -> h1 ->
  * h2 -> d_out, GELU hidden layers, flat FP32 master parameters w with a bf16
  * copy wb of the same layout [W1, b1, W2, b2, W3, b3]; forward passes use
