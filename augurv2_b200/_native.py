@@ -130,6 +130,7 @@ _SIGS = {
     "ab_hlrg_bind": (i32, [vp, i32, vp, i32, vp, vp, i32]),
     "ab_hlrg_set_active": (i32, [vp, vp, vp]),
     "ab_hlrg_logp_grad": (i32, [vp, vp, vp]),
+    "ab_hlrg_fused": (i32, [vp]),
     "ab_hlrg_destroy": (i32, [vp]),
     "ab_nutsg_create": (i32, [i32, vp, vp]),
     "ab_nutsg_set_active": (i32, [vp, vp, vp]),

@@ -176,6 +176,67 @@ __global__ void hlrb_transpose_kernel(int N, int D, int Np, const __nv_bfloat16*
 // have the same sign, so nothing cancels), and the chunk sums go into a
 // Kahan-compensated running sum per chain and column group.  Rows at or
 // past N carry s = 0: no term, zero residual.
+// The hardware approximations (one MUFU operation each, subnormals flushed):
+// 2^x, log2 x and 1/x.
+__device__ __forceinline__ float ex2_ftz(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float lg2_ftz(float x) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// One chunk of NW columns of the forward epilogue for one chain: t = v[i] at
+// rows with s = sv[i] (2y - 1, or 0 past N; FULL: no such rows), residual
+// into rv, the chunk's log-likelihood terms added to the Kahan pair
+// (acc, comp).
+template <bool LL, bool R, bool FULL, int NW = 32>
+__device__ __forceinline__ void ll_resid_chunk(const float* v, const float* sv, float* rv, float& acc, float& comp) {
+  float s1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, s2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int i = 0; i < NW; ++i) {
+    const float t = v[i], sg = sv[i];
+    const float u = sg * t;
+    const float e = ex2_ftz(-1.4426950408889634f * fabsf(t));   // exp(-|t|), 0 below 2^-126
+    const float ope = 1.0f + e;                                  // in [1, 2]
+    if (LL) {
+      s1[i & 3] += fminf(u, 0.0f);
+      const float l2 = lg2_ftz(ope);
+      s2[i & 3] += (FULL || sg != 0.0f) ? l2 : 0.0f;
+    }
+    if (R) {
+      const float inv = rcp_ftz(ope);
+      rv[i] = sg * (u >= 0.0f ? e * inv : inv);
+    }
+  }
+  if (LL) {
+    const float part = ((s1[0] + s1[1]) + (s1[2] + s1[3])) -
+                       0.69314718055994531f * ((s2[0] + s2[1]) + (s2[2] + s2[3]));
+    const float yk = part - comp;   // Kahan-compensated running sum
+    const float tk = acc + yk;
+    comp = (tk - acc) - yk;
+    acc = tk;
+  }
+}
+
+// hi = bf16(r), mid = bf16(r - hi) of two values, each pair packed in one
+// 32-bit word (the difference r - hi is exact in FP32).
+__device__ __forceinline__ void split_pair(float r0, float r1, uint32_t& hi, uint32_t& mid) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(r0, r1);
+  hi = *reinterpret_cast<const uint32_t*>(&h);
+  const float h0 = __uint_as_float(hi << 16), h1 = __uint_as_float(hi & 0xffff0000u);
+  const __nv_bfloat162 m = __floats2bfloat162_rn(r0 - h0, r1 - h1);
+  mid = *reinterpret_cast<const uint32_t*>(&m);
+}
+
 template <bool LL, bool R, int W, int BN>
 struct FwdEpi {
   static constexpr int kSmem = BN * 4;
@@ -202,35 +263,6 @@ struct FwdEpi {
     comp = 0.0f;
   }
 
-  template <bool FULL>
-  __device__ __forceinline__ void chunk(const float* v, const float* sv, float* rv) {
-    float s1[4] = {0.0f, 0.0f, 0.0f, 0.0f}, s2[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      const float t = v[i], sg = sv[i];
-      const float u = sg * t;
-      const float e = __expf(-fabsf(t));
-      const float ope = 1.0f + e;   // in (1, 2]
-      if (LL) {
-        s1[i & 3] += fminf(u, 0.0f);
-        const float l2 = __log2f(ope);
-        s2[i & 3] += (FULL || sg != 0.0f) ? l2 : 0.0f;
-      }
-      if (R) {
-        const float inv = __fdividef(1.0f, ope);
-        rv[i] = sg * (u >= 0.0f ? e * inv : inv);
-      }
-    }
-    if (LL) {
-      const float part = ((s1[0] + s1[1]) + (s1[2] + s1[3])) -
-                         0.69314718055994531f * ((s2[0] + s2[1]) + (s2[2] + s2[3]));
-      const float yk = part - comp;   // Kahan-compensated running sum
-      const float tk = acc + yk;
-      comp = (tk - acc) - yk;
-      acc = tk;
-    }
-  }
-
   __device__ void rows(int c, int col0, const float* v, bool ok) {
     if (!ok) return;
     float rv[32], sv[32];
@@ -243,8 +275,8 @@ struct FwdEpi {
       sv[4 * q + 2] = a.z;
       sv[4 * q + 3] = a.w;
     }
-    if (col0 + 32 <= N) chunk<true>(v, sv, rv);   // uniform over the warp
-    else chunk<false>(v, sv, rv);
+    if (col0 + 32 <= N) ll_resid_chunk<LL, R, true>(v, sv, rv, acc, comp);   // uniform over the warp
+    else ll_resid_chunk<LL, R, false>(v, sv, rv, acc, comp);
     if (R && col0 < Np) {
       // K-blocked [Np/64][2][C][64]: part p of chain c for rows col0..col0+31;
       // hi = bf16(r), mid = bf16(r - hi) (the difference is exact in FP32),
@@ -252,14 +284,7 @@ struct FwdEpi {
       __nv_bfloat16* base = r3 + ((size_t)(col0 >> 6) * R_PARTS * C + c) * 64 + (col0 & 63);
       uint32_t ph[16], pm[16];
 #pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(rv[2 * i], rv[2 * i + 1]);
-        const uint32_t hb = *reinterpret_cast<const uint32_t*>(&h);
-        const float h0 = __uint_as_float(hb << 16), h1 = __uint_as_float(hb & 0xffff0000u);
-        const __nv_bfloat162 m = __floats2bfloat162_rn(rv[2 * i] - h0, rv[2 * i + 1] - h1);
-        ph[i] = hb;
-        pm[i] = *reinterpret_cast<const uint32_t*>(&m);
-      }
+      for (int i = 0; i < 16; ++i) split_pair(rv[2 * i], rv[2 * i + 1], ph[i], pm[i]);
       uint4* dh = reinterpret_cast<uint4*>(base);
       uint4* dm = reinterpret_cast<uint4*>(base + (size_t)C * 64);
 #pragma unroll
@@ -473,6 +498,7 @@ extern "C" int ab_hlrb_logp_grad(const ab_hlrb_model* m, int C, const float* the
 }
 
 // ---- grouped pass: many instances, one launch per stage ---------------------
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -527,11 +553,14 @@ __global__ void __launch_bounds__(256) hlrg_finish_kernel(const GFinish* __restr
 struct HlrgInst {
   ab_hlrb_model m;
   int C;
-  Layout L;
+  Layout L;          // unfused pass: the built-in launch shape
   char* work;
   tc::GProblem fwd, bwd;
   GFwd fe;
   GradEpi ge;
+  // fused pass (every instance D <= 256): theta parts, partial sums, maps
+  int Dp = 0, Dn = 0, rtiles = 0, nseg = 0;
+  size_t f_t3 = 0, f_llp = 0, f_gw = 0, f_total = 0;
   const float* theta = nullptr;
   double* logp = nullptr;
   float* grad = nullptr;
@@ -540,19 +569,413 @@ struct HlrgInst {
 
 inline size_t al256(size_t a) { return (a + 255) & ~size_t(255); }
 
+// ---- fused pass (D <= 256): forward, residual and backward in one kernel ----
+//
+// One persistent CTA per SM walks a list of work units; a unit is one
+// instance's chain tile (128 chains) over a segment of up to F_SEG_TILES
+// row tiles of 128 data rows.  Per row tile:
+//   forward   T[128 chains x 128 rows] = Theta3 . X_tile^T into one of two
+//             tensor-memory accumulators (3 bf16 parts of theta, K = D);
+//   epilogue  log-likelihood terms (Kahan sum per chain over the unit) and
+//             the residual r = y - sigmoid(t) as two bf16 parts, written to
+//             shared memory in the 128-byte-swizzled K-major layout the MMA
+//             reads (no global scratch);
+//   backward  G[128 chains x Dn] += R_p . Xt_block^T, the transposed X block
+//             [D rows x 64] fetched by TMA from the K-blocked copy of X; G
+//             stays in tensor memory (columns 256..511) for the whole unit.
+// The MMA issue order F(0) F(1) B(0) F(2) B(1) ... B(n-1) lets the forward
+// of the next row tile run while the epilogue works on the current one.  At
+// the end of a unit the epilogue writes the unit's partial log likelihood
+// [seg][2 column groups][C] and gradient [seg][C][Dn]; the finishing kernel
+// adds the segments in a fixed order.  A unit's results depend only on its
+// instance and rows, never on which CTA ran it or what else is in the
+// launch, so a group of instances gives each instance the numbers it gets
+// alone.  Roles: warp 0 lane 0 TMA producer, warp 1 lane 0 MMA issuer,
+// warps 2..17 epilogue (column group g = 32 columns, taken 16 at a time;
+// lane quarter = warp % 4).  Every wait is bounded as in gemm_kernel.
+constexpr int F_ROWS = 128;
+constexpr int F_SEG_TILES = 64;                            // row tiles per unit (8192 rows)
+constexpr int F_MAX_D = 256;
+constexpr int F_EPI_WARPS = 16;
+constexpr int F_GROUPS = F_EPI_WARPS / 4;                 // column groups of 32
+constexpr int F_THREADS = 64 + 32 * F_EPI_WARPS;
+constexpr int F_STAGES = 2;
+constexpr int F_A_BYTES = 128 * 64 * 2;                    // one 128 x 64 bf16 box
+constexpr int F_STAGE_BYTES = 3 * F_A_BYTES + F_ROWS * 128; // theta parts + X tile; an Xt block uses Dn * 128
+constexpr int F_ROFF = F_STAGES * F_STAGE_BYTES;           // residual parts: [2 parts][2 K-blocks] boxes
+constexpr int F_YOFF = F_ROFF + 4 * F_A_BYTES;             // s values [2][128] f32
+constexpr int F_BAROFF = F_YOFF + 2 * F_ROWS * 4;
+constexpr int F_SMEM = F_BAROFF + 256 + 1024;
+constexpr int F_TMEM_COLS = 512;                           // T0 | T1 | G
+static_assert(F_SMEM <= tc::SMEM_BUDGET, "fused pass exceeds shared memory");
+
+struct alignas(64) FInst {
+  CUtensorMap t3, x, xt;
+  const int* y;
+  float* llp;   // [nseg][F_GROUPS][C]
+  float* gw;    // [nseg][C][Dn]
+  int N, D, Dp, Dn, C;
+};
+
+struct FUnit {
+  int inst, m, r0, r1, seg;
+};
+
+__global__ void __launch_bounds__(F_THREADS, 1)
+hlrf_kernel(const FInst* __restrict__ insts, const FUnit* __restrict__ units, const int* __restrict__ cta_off,
+            int* __restrict__ err) {
+  using namespace tc;
+  const int u_beg = cta_off[blockIdx.x], u_end = cta_off[blockIdx.x + 1];
+  if (u_beg >= u_end) return;   // uniform over the CTA
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* ring = base;
+  unsigned char* rbuf = base + F_ROFF;
+  float* ys = reinterpret_cast<float*>(base + F_YOFF);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + F_BAROFF);
+  uint64_t* empty = full + F_STAGES;
+  uint64_t* acc_full = empty + F_STAGES;
+  uint64_t* acc_empty = acc_full + 2;
+  uint64_t* r_full = acc_empty + 2;
+  uint64_t* r_empty = r_full + 1;
+  uint64_t* g_full = r_empty + 1;
+  uint64_t* g_empty = g_full + 1;
+  uint64_t* drain = g_empty + 1;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  int* fail = reinterpret_cast<int*>(tmem_slot + 1);
+  int* epi_fail = fail + 1;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < F_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    for (int b = 0; b < 2; ++b) { mbar_init(&acc_full[b], 1); mbar_init(&acc_empty[b], F_EPI_WARPS); }
+    mbar_init(r_full, F_EPI_WARPS);
+    mbar_init(r_empty, 1);
+    mbar_init(g_full, 1);
+    mbar_init(g_empty, F_EPI_WARPS);
+    mbar_init(drain, 1);
+    *fail = 0;
+    *epi_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"((uint32_t)F_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  int issued = 0;
+  if (warp == 0) {
+    if (lane == 0) {
+      int g = 0, last = -1;
+      for (int u = u_beg; u < u_end && !*(volatile int*)fail; ++u) {
+        const FUnit U = units[u];
+        const FInst* I = insts + U.inst;
+        if (U.inst != last) {
+          tensormap_acquire(&I->t3);
+          tensormap_acquire(&I->x);
+          tensormap_acquire(&I->xt);
+          last = U.inst;
+        }
+        const int n = U.r1 - U.r0, ksteps = I->Dp / BK, D = I->D, Dp = I->Dp;
+        const uint32_t bbytes = (uint32_t)(I->Dn * 128);
+        bool bad = false;
+        for (int k = 0; k <= n && !bad; ++k) {
+          if (k < n) {
+            for (int kb = 0; kb < ksteps; ++kb, ++g) {
+              const int s = g % F_STAGES;
+              if (g >= F_STAGES && !mbar_wait(&empty[s], ((g / F_STAGES) & 1) ^ 1)) { *fail = 1; bad = true; break; }
+              if (*(volatile int*)fail) { bad = true; break; }
+              unsigned char* a = ring + s * F_STAGE_BYTES;
+              mbar_expect_tx(&full[s], (uint32_t)F_STAGE_BYTES);
+#pragma unroll
+              for (int p = 0; p < 3; ++p) tma_load_2d(a + p * F_A_BYTES, &I->t3, &full[s], kb * BK + p * Dp, U.m * BM);
+              tma_load_2d(a + 3 * F_A_BYTES, &I->x, &full[s], kb * BK, (U.r0 + k) * F_ROWS);
+              ++issued;
+            }
+          }
+          if (k >= 1 && !bad) {
+            for (int j = 0; j < 2; ++j, ++g) {
+              const int s = g % F_STAGES;
+              if (g >= F_STAGES && !mbar_wait(&empty[s], ((g / F_STAGES) & 1) ^ 1)) { *fail = 1; bad = true; break; }
+              if (*(volatile int*)fail) { bad = true; break; }
+              unsigned char* a = ring + s * F_STAGE_BYTES;
+              mbar_expect_tx(&full[s], bbytes);
+              tma_load_2d(a, &I->xt, &full[s], 0, (2 * (U.r0 + k - 1) + j) * D);
+              ++issued;
+            }
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc_t = make_idesc(F_ROWS);
+      int g = 0, it = 0, rb = 0, gu = 0;
+      bool bad = false;
+      for (int u = u_beg; u < u_end && !bad; ++u) {
+        const FUnit U = units[u];
+        const FInst* I = insts + U.inst;
+        const int n = U.r1 - U.r0, ksteps = I->Dp / BK;
+        const uint32_t idesc_g = make_idesc(I->Dn);
+        for (int k = 0; k <= n && !bad; ++k) {
+          if (k < n) {
+            const int buf = it & 1;
+            if (it >= 2 && !mbar_wait(&acc_empty[buf], ((it >> 1) - 1) & 1)) { *fail = 1; bad = true; break; }
+            if (*(volatile int*)fail) { bad = true; break; }
+            fence_after();
+            const uint32_t d = tmem + (uint32_t)(buf * F_ROWS);
+            for (int kb = 0; kb < ksteps; ++kb, ++g) {
+              const int s = g % F_STAGES;
+              if (!mbar_wait(&full[s], (g / F_STAGES) & 1)) { *fail = 1; bad = true; break; }
+              if (*(volatile int*)fail) { bad = true; break; }
+              fence_after();
+              unsigned char* a = ring + s * F_STAGE_BYTES;
+#pragma unroll
+              for (int kk = 0; kk < BK / 16; ++kk)
+#pragma unroll
+                for (int p = 0; p < 3; ++p)
+                  mma_bf16(d, make_desc(a + p * F_A_BYTES) + 2 * kk, make_desc(a + 3 * F_A_BYTES) + 2 * kk, idesc_t,
+                           (kb > 0 || kk > 0 || p > 0) ? 1u : 0u);
+              mma_commit(&empty[s]);
+            }
+            if (bad) break;
+            mma_commit(&acc_full[buf]);
+            ++it;
+          }
+          if (k >= 1) {
+            if (!mbar_wait(r_full, rb & 1)) { *fail = 1; bad = true; break; }
+            if (k == 1 && gu >= 1 && !mbar_wait(g_empty, (gu - 1) & 1)) { *fail = 1; bad = true; break; }
+            if (*(volatile int*)fail) { bad = true; break; }
+            fence_after();
+            const uint32_t dg = tmem + 2u * F_ROWS;
+            for (int j = 0; j < 2; ++j, ++g) {
+              const int s = g % F_STAGES;
+              if (!mbar_wait(&full[s], (g / F_STAGES) & 1)) { *fail = 1; bad = true; break; }
+              if (*(volatile int*)fail) { bad = true; break; }
+              fence_after();
+              unsigned char* b = ring + s * F_STAGE_BYTES;
+#pragma unroll
+              for (int kk = 0; kk < BK / 16; ++kk)
+#pragma unroll
+                for (int p = 0; p < 2; ++p)
+                  mma_bf16(dg, make_desc(rbuf + (p * 2 + j) * F_A_BYTES) + 2 * kk, make_desc(b) + 2 * kk, idesc_g,
+                           (k > 1 || j > 0 || kk > 0 || p > 0) ? 1u : 0u);
+              mma_commit(&empty[s]);
+            }
+            if (bad) break;
+            mma_commit(r_empty);
+            ++rb;
+          }
+        }
+        if (bad) break;
+        mma_commit(g_full);
+        ++gu;
+      }
+      mma_commit(drain);
+      if (!mbar_wait(drain, 0)) *fail = 1;
+    }
+  } else {
+    const int qw = warp & 3;                 // TMEM lane quarter
+    const int grp = (warp - 2) >> 2;         // column group: columns [32 grp, 32 grp + 32)
+    const int etid = (warp - 2) * 32 + lane;
+    const int cl = qw * 32 + lane;           // chain within the tile
+    const uint32_t lane_base = tmem + ((uint32_t)(qw * 32) << 16);
+    int it = 0, gu = 0;
+    bool bad = false;   // this thread's failure so far (uniform over the warp)
+    // y of row etid of the next tile, loaded one tile ahead (threads etid < 128)
+    int pf_y = 0;
+    bool pf_v = false;
+    auto prefetch = [&](int uu, int kk) {
+      if (etid < F_ROWS && uu < u_end) {
+        const FUnit V = units[uu];
+        const FInst* J = insts + V.inst;
+        const int nn = (V.r0 + kk) * F_ROWS + etid;
+        pf_v = nn < J->N;
+        pf_y = pf_v ? J->y[nn] : 0;
+      }
+    };
+    prefetch(u_beg, 0);
+    for (int u = u_beg; u < u_end; ++u) {
+      const FUnit U = units[u];
+      const FInst* I = insts + U.inst;
+      const int n = U.r1 - U.r0, N = I->N, C = I->C, Dn = I->Dn;
+      const int chain = U.m * BM + cl;
+      const bool ok = chain < C;
+      float acc = 0.0f, comp = 0.0f;
+      bool stop = false;
+      for (int k = 0; k < n; ++k) {
+        const int buf = it & 1;
+        const int row0 = (U.r0 + k) * F_ROWS;
+        if (etid < F_ROWS) ys[buf * F_ROWS + etid] = pf_v ? (pf_y ? 1.0f : -1.0f) : 0.0f;
+        if (k + 1 < n) prefetch(u, k + 1);
+        else prefetch(u + 1, 0);
+        // the barrier ORs every epilogue thread's failure flag: all stop together
+        if (epi_sync_or(32 * F_EPI_WARPS, bad)) { stop = true; break; }
+        bool okw = __all_sync(0xffffffffu, mbar_wait(&acc_full[buf], (it >> 1) & 1));
+        if (it >= 1) okw = __all_sync(0xffffffffu, okw && mbar_wait(r_empty, (it - 1) & 1));
+        fence_after();
+        const bool have = __all_sync(0xffffffffu, okw && !*(volatile int*)fail);
+        const uint32_t tcol = (uint32_t)(buf * F_ROWS + grp * 32);
+        const float* sv0 = ys + buf * F_ROWS + grp * 32;
+        // the group's 32 columns lie in residual K-block grp / 2, 16-byte
+        // chunks 4 (grp % 2) .. +3 of each chain row
+        unsigned char* rowh = rbuf + (0 * 2 + (grp >> 1)) * F_A_BYTES + cl * 128;
+        unsigned char* rowm = rbuf + (1 * 2 + (grp >> 1)) * F_A_BYTES + cl * 128;
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+          float v[16], sv[16], rv[16];
+          if (have) {
+            uint32_t r[16];
+            tmem_ld16_issue(lane_base + tcol + cc * 16, r);
+            tmem_wait16(r);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+          }
+          const float4* s4 = reinterpret_cast<const float4*>(sv0 + cc * 16);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float4 a = s4[i];
+            sv[4 * i] = a.x;
+            sv[4 * i + 1] = a.y;
+            sv[4 * i + 2] = a.z;
+            sv[4 * i + 3] = a.w;
+          }
+          if (row0 + grp * 32 + cc * 16 + 16 <= N) ll_resid_chunk<true, true, true, 16>(v, sv, rv, acc, comp);
+          else ll_resid_chunk<true, true, false, 16>(v, sv, rv, acc, comp);
+          // residual parts into the swizzled K-major boxes: chain row cl,
+          // 16-byte chunk c16 of the row stored at c16 ^ (cl & 7)
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            uint32_t h[4], m[4];
+#pragma unroll
+            for (int e2 = 0; e2 < 4; ++e2) split_pair(rv[8 * q + 2 * e2], rv[8 * q + 2 * e2 + 1], h[e2], m[e2]);
+            const int c16 = ((grp & 1) * 4 + cc * 2 + q) ^ (cl & 7);
+            *reinterpret_cast<uint4*>(rowh + c16 * 16) = make_uint4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<uint4*>(rowm + c16 * 16) = make_uint4(m[0], m[1], m[2], m[3]);
+          }
+        }
+        fence_before();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // residual writes -> tensor core
+        __syncwarp();
+        if (lane == 0) {
+          mbar_arrive(&acc_empty[buf]);
+          mbar_arrive(r_full);
+        }
+        if (!have) bad = true;
+        ++it;
+      }
+      if (stop) break;
+      if (ok) I->llp[((size_t)U.seg * F_GROUPS + grp) * C + chain] = acc;
+      // the unit's gradient: columns [64 grp, 64 grp + 64) of G
+      const bool okg = __all_sync(0xffffffffu, mbar_wait(g_full, gu & 1) && !*(volatile int*)fail);
+      fence_after();
+      const int c_end = min(Dn, grp * 64 + 64);
+      for (int c0 = grp * 64; c0 < c_end; c0 += 32) {
+        if (!okg) break;
+        uint32_t r[32];
+        tmem_ld32_issue(lane_base + 2u * F_ROWS + (uint32_t)c0, r);
+        tmem_wait32(r);
+        if (ok) {
+          float4* o = reinterpret_cast<float4*>(I->gw + ((size_t)U.seg * C + chain) * Dn + c0);
+          const int lim = min(32, Dn - c0);   // Dn is a multiple of 16
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+            if (4 * i < lim)
+              o[i] = make_float4(__uint_as_float(r[4 * i]), __uint_as_float(r[4 * i + 1]), __uint_as_float(r[4 * i + 2]),
+                                 __uint_as_float(r[4 * i + 3]));
+        }
+      }
+      fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(g_empty);
+      if (!okg) bad = true;
+      ++gu;
+    }
+    if (bad) *(volatile int*)epi_fail = 1;
+  }
+  __syncwarp();
+  if (threadIdx.x == 0 && *(volatile int*)fail) {
+    for (int g = max(0, issued - F_STAGES); g < issued; ++g) mbar_wait(&full[g % F_STAGES], (g / F_STAGES) & 1);
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)F_TMEM_COLS)
+                 : "memory");
+  }
+  if (threadIdx.x == 0 && (*(volatile int*)fail || *(volatile int*)epi_fail) && err) atomicExch(err, AB_ERR_TIMEOUT);
+}
+
 }  // namespace
 }  // namespace ab
 
 struct ab_hlrg {
   std::vector<ab::HlrgInst> inst;
-  int C_max = 0, Dp_max = 0, grid_fwd = 0, grid_bwd = 0, n_active = 0;
+  std::vector<ab::FInst> finst;   // fused pass: per instance (maps, pointers, sizes)
+  bool fused = false;             // every instance has D <= 256: one fused kernel per pass
+  int C_max = 0, Dp_max = 0, grid_fwd = 0, grid_bwd = 0, grid_f = 0, n_active = 0, units_max = 0;
   bool ready = false;
   char* work = nullptr;    // every instance's workspace
   char* tab = nullptr;     // device tables
-  size_t o_fwd = 0, o_bwd = 0, o_fe = 0, o_ge = 0, o_sp = 0, o_fin = 0, bytes = 0;
+  size_t o_fwd = 0, o_bwd = 0, o_fe = 0, o_ge = 0, o_sp = 0, o_fin = 0, o_fi = 0, o_fu = 0, o_off = 0, bytes = 0;
   unsigned char* stage = nullptr;   // host copy of the tables (256-byte aligned)
-  ~ab_hlrg() { std::free(stage); }
+  ~ab_hlrg() {
+    std::free(stage);
+    cudaFree(work);
+    cudaFree(tab);
+  }
 };
+
+namespace ab {
+namespace {
+// Fused pass: the work units of one instance (chain tile, row segment).
+void fused_units(const HlrgInst& q, int inst, std::vector<FUnit>& out) {
+  const int mt = (q.C + tc::BM - 1) / tc::BM;
+  for (int m = 0; m < mt; ++m)
+    for (int sg = 0; sg < q.nseg; ++sg)
+      out.push_back(FUnit{inst, m, sg * F_SEG_TILES, std::min(q.rtiles, (sg + 1) * F_SEG_TILES), sg});
+}
+
+// Longest-processing-time-first assignment of units to CTAs; writes the
+// units grouped by CTA and the CTA offsets.
+void assign_units(const std::vector<FUnit>& u, const std::vector<HlrgInst>& inst, const std::vector<int>& act,
+                  int ctas, FUnit* out, int* off) {
+  std::vector<std::pair<double, int>> cost(u.size());
+  for (size_t i = 0; i < u.size(); ++i) {
+    const HlrgInst& q = inst[act[u[i].inst]];
+    cost[i] = {(double)(u[i].r1 - u[i].r0) * (2.0 + q.Dp / 64), (int)i};
+  }
+  std::stable_sort(cost.begin(), cost.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+    return a.first > b.first;
+  });
+  std::vector<double> load(ctas, 0.0);
+  std::vector<std::vector<int>> lists(ctas);
+  for (const auto& c : cost) {
+    int best = 0;
+    for (int j = 1; j < ctas; ++j)
+      if (load[j] < load[best]) best = j;
+    load[best] += c.first;
+    lists[best].push_back(c.second);
+  }
+  int k = 0;
+  for (int j = 0; j < ctas; ++j) {
+    off[j] = k;
+    for (int i : lists[j]) out[k++] = u[i];
+  }
+  off[ctas] = k;
+}
+}  // namespace
+}  // namespace ab
 
 extern "C" int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, ab_hlrg** out) {
   using namespace ab;
@@ -561,35 +984,68 @@ extern "C" int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, 
   AB_REQUIRE(n >= 1 && n <= tc::GROUP_MAX, AB_ERR_ARG, "ab_hlrg_create: n must be 1..%d (got %d)", tc::GROUP_MAX, n);
   std::unique_ptr<ab_hlrg> g(new ab_hlrg());
   g->inst.resize(n);
-  size_t wtot = 0;
-  std::vector<size_t> woff(n);
-  long long fwd_tiles = 0, bwd_tiles = 0;
+  g->fused = true;
   for (int i = 0; i < n; ++i) {
     int rc = hlrb_check_model(&models[i]);
     if (rc) return rc;
     AB_REQUIRE(C[i] > 0 && C[i] <= 65535, AB_ERR_ARG, "ab_hlrg_create: instance %d: C must be 1..65535", i);
     AB_REQUIRE(models[i].D % 8 == 0, AB_ERR_ARG, "ab_hlrg_create: instance %d: D must be a multiple of 8", i);
+    if (models[i].D > F_MAX_D) g->fused = false;
+  }
+  size_t wtot = 0;
+  std::vector<size_t> woff(n);
+  long long fwd_tiles = 0, bwd_tiles = 0;
+  for (int i = 0; i < n; ++i) {
     HlrgInst& q = g->inst[i];
     q.m = models[i];
     q.C = C[i];
     q.L = layout(q.m.N, q.m.D, q.C, nullptr);
     AB_REQUIRE(q.L.fwd_bn == 256 && q.L.groups == 2 && q.L.bn <= G_BWD_BN, AB_ERR_STATE,
                "ab_hlrg_create: built-in launch shape changed");
+    q.Dp = q.L.Dp;
+    q.Dn = (q.m.D + 15) / 16 * 16;
+    q.rtiles = (q.m.N + F_ROWS - 1) / F_ROWS;
+    q.nseg = (q.rtiles + F_SEG_TILES - 1) / F_SEG_TILES;
+    size_t o = 0;
+    q.f_t3 = o;  o = al256(o + (size_t)q.C * 3 * q.Dp * 2);
+    q.f_llp = o; o = al256(o + (size_t)q.nseg * F_GROUPS * q.C * 4);
+    q.f_gw = o;  o = al256(o + (size_t)q.nseg * q.C * q.Dn * 4);
+    q.f_total = o;
     woff[i] = wtot;
-    wtot = al256(wtot + q.L.total);
+    wtot = al256(wtot + (g->fused ? q.f_total : q.L.total));
     g->C_max = std::max(g->C_max, q.C);
     g->Dp_max = std::max(g->Dp_max, q.L.Dp);
+    g->units_max += ((q.C + tc::BM - 1) / tc::BM) * q.nseg;
   }
   AB_CUDA(cudaMalloc(&g->work, wtot));
+  if (g->fused) g->finst.resize(n);
   for (int i = 0; i < n; ++i) {
     HlrgInst& q = g->inst[i];
     const Layout& L = q.L;
     q.work = g->work + woff[i];
+    int rc;
+    if (g->fused) {
+      FInst& f = g->finst[i];
+      std::memset(&f, 0, sizeof(f));
+      __nv_bfloat16* t3 = reinterpret_cast<__nv_bfloat16*>(q.work + q.f_t3);
+      const int nb = L.Np / 64;
+      if ((rc = tc::encode_2d_bf16(&f.t3, t3, q.C, 3 * q.Dp, 3 * q.Dp, tc::BM))) return rc;
+      if ((rc = tc::encode_2d_bf16(&f.x, q.m.X, q.m.N, q.m.D, q.m.ldx, F_ROWS))) return rc;
+      if ((rc = tc::encode_2d_bf16(&f.xt, q.m.Xt, (uint64_t)nb * q.m.D, 64, 64, q.Dn))) return rc;
+      f.y = q.m.y;
+      f.llp = reinterpret_cast<float*>(q.work + q.f_llp);
+      f.gw = reinterpret_cast<float*>(q.work + q.f_gw);
+      f.N = q.m.N;
+      f.D = q.m.D;
+      f.Dp = q.Dp;
+      f.Dn = q.Dn;
+      f.C = q.C;
+      continue;
+    }
     __nv_bfloat16* t3 = reinterpret_cast<__nv_bfloat16*>(q.work + L.off_t3);
     __nv_bfloat16* r3 = reinterpret_cast<__nv_bfloat16*>(q.work + L.off_r3);
     float* llp = reinterpret_cast<float*>(q.work + L.off_ll);
     float* w = reinterpret_cast<float*>(q.work + L.off_w);
-    int rc;
     if ((rc = tc::encode_2d_bf16(&q.fwd.ta, t3, q.C, 3 * L.Dp, 3 * L.Dp, tc::BM))) return rc;
     if ((rc = tc::encode_2d_bf16(&q.fwd.tb, q.m.X, q.m.N, q.m.D, q.m.ldx, L.fwd_bn))) return rc;
     q.fwd.sh = tc::make_shape(q.C, q.m.N, q.m.D, 1, tc::row_major(L.Dp), tc::row_major(0), L.fwd_bn);
@@ -606,8 +1062,9 @@ extern "C" int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, 
     bwd_tiles += (long long)q.bwd.sh.m_tiles * q.bwd.sh.n_tiles * q.bwd.sh.splits;
   }
   AB_REQUIRE(fwd_tiles < (1LL << 31) && bwd_tiles < (1LL << 31), AB_ERR_ARG, "ab_hlrg_create: too many tiles");
-  g->grid_fwd = (int)std::min<long long>(fwd_tiles, tc::sm_count());
-  g->grid_bwd = (int)std::min<long long>(bwd_tiles, tc::sm_count());
+  g->grid_fwd = (int)std::max<long long>(1, std::min<long long>(fwd_tiles, tc::sm_count()));
+  g->grid_bwd = (int)std::max<long long>(1, std::min<long long>(bwd_tiles, tc::sm_count()));
+  g->grid_f = tc::sm_count();
   size_t o = al256(sizeof(GHeads));
   g->o_fwd = o; o = al256(o + sizeof(tc::GProblem) * n);
   g->o_bwd = o; o = al256(o + sizeof(tc::GProblem) * n);
@@ -615,19 +1072,27 @@ extern "C" int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, 
   g->o_ge = o;  o = al256(o + sizeof(GradEpi) * n);
   g->o_sp = o;  o = al256(o + sizeof(GSplit) * n);
   g->o_fin = o; o = al256(o + sizeof(GFinish) * n);
+  g->o_fi = o;  o = al256(o + sizeof(FInst) * n);
+  g->o_fu = o;  o = al256(o + sizeof(FUnit) * (size_t)g->units_max);
+  g->o_off = o; o = al256(o + sizeof(int) * (size_t)(g->grid_f + 1));
   g->bytes = o;
   AB_CUDA(cudaMalloc(&g->tab, g->bytes));
   AB_CUDA(cudaMemset(g->tab, 0, g->bytes));
   g->stage = static_cast<unsigned char*>(std::aligned_alloc(256, g->bytes));
   AB_REQUIRE(g->stage, AB_ERR_CUDA, "ab_hlrg_create: host allocation failed");
   std::memset(g->stage, 0, g->bytes);
-  using GF = tc::GCfg<256, 3, 1, GFwd>::C;
-  using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
-  static_assert(GF::SMEM_BYTES <= tc::SMEM_BUDGET && GB::SMEM_BYTES <= tc::SMEM_BUDGET, "grouped tiles exceed shared memory");
-  AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<256, 3, 1, GFwd>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               GF::SMEM_BYTES));
-  AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, GB::SMEM_BYTES));
+  if (g->fused) {
+    AB_CUDA(cudaFuncSetAttribute(hlrf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, F_SMEM));
+  } else {
+    using GF = tc::GCfg<256, 3, 1, GFwd>::C;
+    using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
+    static_assert(GF::SMEM_BYTES <= tc::SMEM_BUDGET && GB::SMEM_BYTES <= tc::SMEM_BUDGET,
+                  "grouped tiles exceed shared memory");
+    AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<256, 3, 1, GFwd>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, GF::SMEM_BYTES));
+    AB_CUDA(cudaFuncSetAttribute(tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, GB::SMEM_BYTES));
+  }
   *out = g.release();
   return AB_OK;
 }
@@ -658,25 +1123,42 @@ extern "C" int ab_hlrg_set_active(ab_hlrg* g, const int* active, void* stream) {
   GradEpi* ge = reinterpret_cast<GradEpi*>(h + g->o_ge);
   GSplit* sp = reinterpret_cast<GSplit*>(h + g->o_sp);
   GFinish* fin = reinterpret_cast<GFinish*>(h + g->o_fin);
+  FInst* fi = reinterpret_cast<FInst*>(h + g->o_fi);
   int k = 0, tf = 0, tb = 0;
+  std::vector<int> act;
+  std::vector<FUnit> units;
   for (int i = 0; i < n; ++i) {
     if (!active[i]) continue;
     const HlrgInst& q = g->inst[i];
     AB_REQUIRE(q.theta, AB_ERR_STATE, "ab_hlrg_set_active: instance %d is active but not bound", i);
-    fwd[k] = q.fwd;
-    fwd[k].tile0 = tf;
-    tf += q.fwd.sh.m_tiles * q.fwd.sh.n_tiles * q.fwd.sh.splits;
-    bwd[k] = q.bwd;
-    bwd[k].tile0 = tb;
-    tb += q.bwd.sh.m_tiles * q.bwd.sh.n_tiles * q.bwd.sh.splits;
-    fe[k] = q.fe;
-    ge[k] = q.ge;
-    sp[k] = GSplit{q.theta, reinterpret_cast<__nv_bfloat16*>(q.work + q.L.off_t3), q.ldt, q.C, q.m.D, q.L.Dp};
-    fin[k] = GFinish{reinterpret_cast<const float*>(q.work + q.L.off_ll), reinterpret_cast<const float*>(q.work + q.L.off_w),
-                     q.theta, q.logp, q.grad, q.m.prior_a, q.m.prior_b, q.C, q.m.D, q.L.fwd_tiles * q.L.groups,
-                     q.L.splits, q.L.ldw, q.ldt, q.m.prior, q.ldg};
+    if (g->fused) {
+      fi[k] = g->finst[i];
+      fused_units(q, k, units);
+      sp[k] = GSplit{q.theta, reinterpret_cast<__nv_bfloat16*>(q.work + q.f_t3), q.ldt, q.C, q.m.D, q.Dp};
+      fin[k] = GFinish{reinterpret_cast<const float*>(q.work + q.f_llp), reinterpret_cast<const float*>(q.work + q.f_gw),
+                       q.theta, q.logp, q.grad, q.m.prior_a, q.m.prior_b, q.C, q.m.D, F_GROUPS * q.nseg, q.nseg, q.Dn, q.ldt,
+                       q.m.prior, q.ldg};
+    } else {
+      fwd[k] = q.fwd;
+      fwd[k].tile0 = tf;
+      tf += q.fwd.sh.m_tiles * q.fwd.sh.n_tiles * q.fwd.sh.splits;
+      bwd[k] = q.bwd;
+      bwd[k].tile0 = tb;
+      tb += q.bwd.sh.m_tiles * q.bwd.sh.n_tiles * q.bwd.sh.splits;
+      fe[k] = q.fe;
+      ge[k] = q.ge;
+      sp[k] = GSplit{q.theta, reinterpret_cast<__nv_bfloat16*>(q.work + q.L.off_t3), q.ldt, q.C, q.m.D, q.L.Dp};
+      fin[k] = GFinish{reinterpret_cast<const float*>(q.work + q.L.off_ll),
+                       reinterpret_cast<const float*>(q.work + q.L.off_w), q.theta, q.logp, q.grad, q.m.prior_a,
+                       q.m.prior_b, q.C, q.m.D, q.L.fwd_tiles * q.L.groups, q.L.splits, q.L.ldw, q.ldt, q.m.prior,
+                       q.ldg};
+    }
+    act.push_back(i);
     ++k;
   }
+  if (g->fused)
+    assign_units(units, g->inst, act, g->grid_f, reinterpret_cast<FUnit*>(h + g->o_fu),
+                 reinterpret_cast<int*>(h + g->o_off));
   GHeads* hd = reinterpret_cast<GHeads*>(h);
   hd->fwd = tc::GHead{k, tf};
   hd->bwd = tc::GHead{k, tb};
@@ -696,26 +1178,32 @@ extern "C" int ab_hlrg_logp_grad(ab_hlrg* g, int* err, void* stream) {
   hlrg_split_kernel<<<dim3(ceil_div(g->Dp_max, 256), g->C_max, n), 256, 0, st>>>(
       reinterpret_cast<const GSplit*>(g->tab + g->o_sp), head);
   AB_LAUNCH_CHECK("hlrg_split_kernel");
-  using GF = tc::GCfg<256, 3, 1, GFwd>::C;
-  using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
-  tc::grouped_gemm_kernel<256, 3, 1, GFwd><<<g->grid_fwd, tc::threads_for(GFwd::kWarps), GF::SMEM_BYTES, st>>>(
-      reinterpret_cast<const tc::GProblem*>(g->tab + g->o_fwd), reinterpret_cast<const GFwd*>(g->tab + g->o_fe),
-      &head->fwd, err);
-  AB_LAUNCH_CHECK("grouped_gemm_kernel (forward)");
-  tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>
-      <<<g->grid_bwd, tc::threads_for(GradEpi::kWarps), GB::SMEM_BYTES, st>>>(
-          reinterpret_cast<const tc::GProblem*>(g->tab + g->o_bwd), reinterpret_cast<const GradEpi*>(g->tab + g->o_ge),
-          &head->bwd, err);
-  AB_LAUNCH_CHECK("grouped_gemm_kernel (backward)");
+  if (g->fused) {
+    hlrf_kernel<<<g->grid_f, F_THREADS, F_SMEM, st>>>(reinterpret_cast<const FInst*>(g->tab + g->o_fi),
+                                                      reinterpret_cast<const FUnit*>(g->tab + g->o_fu),
+                                                      reinterpret_cast<const int*>(g->tab + g->o_off), err);
+    AB_LAUNCH_CHECK("hlrf_kernel");
+  } else {
+    using GF = tc::GCfg<256, 3, 1, GFwd>::C;
+    using GB = tc::GCfg<G_BWD_BN, R_PARTS, 1, GradEpi>::C;
+    tc::grouped_gemm_kernel<256, 3, 1, GFwd><<<g->grid_fwd, tc::threads_for(GFwd::kWarps), GF::SMEM_BYTES, st>>>(
+        reinterpret_cast<const tc::GProblem*>(g->tab + g->o_fwd), reinterpret_cast<const GFwd*>(g->tab + g->o_fe),
+        &head->fwd, err);
+    AB_LAUNCH_CHECK("grouped_gemm_kernel (forward)");
+    tc::grouped_gemm_kernel<G_BWD_BN, R_PARTS, 1, GradEpi>
+        <<<g->grid_bwd, tc::threads_for(GradEpi::kWarps), GB::SMEM_BYTES, st>>>(
+            reinterpret_cast<const tc::GProblem*>(g->tab + g->o_bwd),
+            reinterpret_cast<const GradEpi*>(g->tab + g->o_ge), &head->bwd, err);
+    AB_LAUNCH_CHECK("grouped_gemm_kernel (backward)");
+  }
   hlrg_finish_kernel<<<dim3(g->C_max, n), 256, 0, st>>>(reinterpret_cast<const GFinish*>(g->tab + g->o_fin), head);
   AB_LAUNCH_CHECK("hlrg_finish_kernel");
   return AB_OK;
 }
 
+extern "C" int ab_hlrg_fused(const ab_hlrg* g) { return g && g->fused ? 1 : 0; }
+
 extern "C" int ab_hlrg_destroy(ab_hlrg* g) {
-  if (!g) return AB_OK;
-  cudaFree(g->work);
-  cudaFree(g->tab);
   delete g;
   return AB_OK;
 }

@@ -127,6 +127,19 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 
 // Named barrier over the epilogue warps.
 __device__ __forceinline__ void epi_sync(int nthreads) { asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory"); }
+// The same barrier returning the OR of every participating thread's flag.
+__device__ __forceinline__ bool epi_sync_or(int nthreads, bool flag) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)flag), "r"(nthreads)
+      : "memory");
+  return r != 0;
+}
 
 // 32 consecutive fp32 columns of this warp's 32 TMEM lanes.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
@@ -168,6 +181,21 @@ __device__ __forceinline__ void tmem_wait32(uint32_t* r) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" : AB_R32(r) : : "memory");
 }
 #undef AB_R32
+#define AB_R16(r) "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]), \
+    "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+// 16 columns: the same pair of halves.
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait16(uint32_t* r) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : AB_R16(r) : : "memory");
+}
+#undef AB_R16
 
 // The epilogue's walk over the 32-column chunks [cbeg, cend) of one
 // accumulator (taddr: this warp's lane quarter at column 0): the next

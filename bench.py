@@ -350,8 +350,9 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
     every running instance advances all its chains to their next leaf and
     evaluates its log density and gradient there; a NutsGroup does this for
     all instances with one advance launch and one grouped tensor-core pass
-    (one launch per stage, the tiles of every instance sharing one
-    persistent grid), captured as one CUDA graph, until every chain of every
+    (theta split, the fused forward + residual + backward kernel whose work
+    units of every instance share one persistent grid, and the finishing
+    sums), captured as one CUDA graph, until every chain of every
     instance has `min_draws` draws (instances with deep trees run more
     rounds; finished instances leave the launches), after an untimed warm-up
     of `warmup_draws` draws per chain whose draws are discarded.  min-ESS/s per instance = min-ESS
@@ -411,8 +412,8 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
             "seconds": ms / 1e3, "worst_instance": worst,
             "median_instance_min_ess_per_s": float(np.median([q["min_ess_per_s"] for q in per])),
             "total_draws": int(sum(q["draws_per_chain"] for q in per) * chains),
-            "roofline": {"bound": "tensor", "kernel": "grouped_gemm_kernel (forward + backward, all instances)",
-                         "achieved": ach,
+            "roofline": {"bound": "tensor", "kernel": "hlrf_kernel (fused forward + residual + backward, all "
+                                                     "instances)", "achieved": ach,
                          "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "peak_source": kind + " (sustained)",
                          "note": "algorithmic 4 N D C per chain-round (forward and backward product); the tensor "
                                  "pipe executes 2.5x that (3 bf16 parts forward, 2 backward)"},
@@ -431,8 +432,8 @@ def run_hlr_nuts(min_draws=48, max_rounds=2400, warmup_draws=16, n_inst=NUTS_INS
                             "max_depth": NUTS_DEPTH, "x_dtype": "bf16", "N": "log-uniform [1e3, 1e6]",
                             "D": "{16, 64, 256}", "prior": "normal(0, sigma^2), sigma^2 at its generating value",
                             "step_size": "0.6 / sqrt(N E[w] + 1/sigma^2) at the generating coefficients",
-                            "schedule": "NutsGroup: one advance + one grouped pass (4 launches) per round for "
-                                        "all running instances, one CUDA graph; rounds until %d draws per chain"
+                            "schedule": "NutsGroup: one advance + one grouped fused pass (3 launches) per round "
+                                        "for all running instances, one CUDA graph; rounds until %d draws per chain"
                                         % min_draws}})
     if cpu:
         head["cpu_baseline"] = nuts_cpu_baseline(results[variants[0]]["instances"], chains)

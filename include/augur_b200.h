@@ -454,23 +454,30 @@ int ab_nutsb_reset_history(void* state, int C, int P, int hist_cap, void* stream
  * cbits/augur_mcmclib.h:44-45), so it has no counterpart for grouping; each
  * instance's arithmetic is that of the single-instance calls above.
  *
- * ab_hlrg: the batched HLR pass (ab_hlrb_logp_grad with the built-in launch
- * shape) for n instances, each with its own data set and C_i chains: one
- * split, one forward, one backward and one finishing launch cover every
- * active instance, the tensor-core tiles of all instances sharing one
- * persistent grid.  Results equal each instance's own ab_hlrb_logp_grad
- * (default launch shape) bit for bit.  The group owns the workspaces; bind
- * each instance's theta [C_i][ldt] f32 input and logp [C_i] f64 / grad
- * [C_i][ldg] f32 outputs, then ab_hlrg_set_active (active[i] != 0 takes part)
- * before the first pass and after any change.  The tables live in device
- * memory, so a CUDA graph captured around ab_hlrg_logp_grad follows later
- * ab_hlrg_set_active calls.  D_i must be a multiple of 8; n <= 256.
+ * ab_hlrg: the batched HLR pass (log density and gradient, the contract of
+ * ab_hlrb_logp_grad) for n instances, each with its own data set and C_i
+ * chains, one launch per stage covering every active instance.  When every
+ * instance has D <= 256 the pass is FUSED: one persistent tensor-core kernel
+ * runs forward, residual and backward per 128-row tile with the residual
+ * kept in shared memory (no N x C scratch in HBM), the work units (chain
+ * tile x 8192-row segment) of all instances balanced over the SMs; an
+ * instance's results depend only on its own data, so they are the same
+ * alone or in any group.  Otherwise the group runs the two-GEMM pass of
+ * ab_hlrb_logp_grad (built-in launch shape) over all instances' tiles, equal
+ * to each instance's own ab_hlrb_logp_grad bit for bit.  ab_hlrg_fused tells
+ * which.  The group owns the workspaces; bind each instance's theta
+ * [C_i][ldt] f32 input and logp [C_i] f64 / grad [C_i][ldg] f32 outputs,
+ * then ab_hlrg_set_active (active[i] != 0 takes part) before the first pass
+ * and after any change.  The tables live in device memory, so a CUDA graph
+ * captured around ab_hlrg_logp_grad follows later ab_hlrg_set_active calls.
+ * D_i must be a multiple of 8; n <= 256.
  * ======================================================================= */
 typedef struct ab_hlrg ab_hlrg;
 int ab_hlrg_create(int n, const ab_hlrb_model* models, const int* C, ab_hlrg** out);
 int ab_hlrg_bind(ab_hlrg* g, int i, const float* theta, int ldt, double* logp, float* grad, int ldg);
 int ab_hlrg_set_active(ab_hlrg* g, const int* active, void* stream);
 int ab_hlrg_logp_grad(ab_hlrg* g, int* err, void* stream);
+int ab_hlrg_fused(const ab_hlrg* g);
 int ab_hlrg_destroy(ab_hlrg* g);
 
 /* ab_nutsg: n batched-NUTS samplers advanced by one launch per round (each

@@ -1,13 +1,16 @@
 """Many model instances in one launch per stage: the grouped HLR pass
 (ab_hlrg_*) and the grouped NUTS advance (ab_nutsg_*, NutsGroup).
 
-The grouped launches change only which CTA computes which tile, not the
-arithmetic, so the contract is bit equality with each instance's own calls:
-  pass   logp and grad equal ab_hlrb_logp_grad's (built-in launch shape);
-  NUTS   every instance's draws, depths and proposals equal its own
-         BatchedNuts run for the same number of rounds;
-and through those, the FP64 oracle's NUTS draws (the per-instance sampler's
-contract, tests/test_hlrb_gpu.py)."""
+Contracts:
+  fused pass (every D <= 256)  logp and grad within the FP64-oracle
+         tolerance of the batched pass (log density 1e-5 of sum_n |term_n|,
+         gradient 1e-5 of |g| + sum_n |r_n x_nd|), and an instance's numbers
+         identical alone and in any group;
+  two-GEMM grouped pass (some D > 256)  equal to each instance's own
+         ab_hlrb_logp_grad bit for bit;
+  NUTS   every instance's draws, depths and proposals equal a group of that
+         instance alone run for the same number of rounds, and the FP64
+         oracle's NUTS draws (cbits/augur_mcmclib.h:575-776)."""
 import ctypes as C
 
 import numpy as np
@@ -16,6 +19,7 @@ import torch
 
 from augurv2_b200 import _native as N
 from augurv2_b200 import hlrb as H
+from oracle import batched as B
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -52,11 +56,68 @@ class _Group:
     def run(self, err):
         N.check(N.lib().ab_hlrg_logp_grad(self.h, N.ptr(err), N.stream_ptr()), "ab_hlrg_logp_grad")
 
+    def fused(self):
+        return N.lib().ab_hlrg_fused(self.h) == 1
+
     def close(self):
         N.lib().ab_hlrg_destroy(self.h)
 
 
-def test_grouped_pass_equals_each_instance_bit_for_bit():
+def _fp64_check(X64, y, d, th, lp, g):
+    lp64, g64, scale = B.hlr_logp_grad(X64, y, th.double().cpu().numpy(), d.prior, d.pa, d.pb)
+    t = th.double().cpu().numpy() @ X64.T
+    term_scale = (np.abs(y * t) + np.logaddexp(0, t)).sum(-1)
+    e_lp = np.abs(lp.cpu().numpy() - lp64) / term_scale
+    gd = g.cpu().numpy().astype(np.float64)
+    e_g = np.abs(gd - g64) / (np.abs(g64) + scale)
+    assert e_lp.max() <= 1e-5 and e_g.max() <= 1e-5, (e_lp.max(), e_g.max())
+
+
+FUSED = [(3000, 64, 40, "student_t"), (1000, 16, 3, "normal"), (2500, 200, 130, "student_t"),
+         (64, 8, 1, "student_t"), (20000, 128, 256, "student_t"), (1498, 256, 512, "normal"),
+         (50, 24, 7, "normal"), (70000, 256, 129, "student_t")]
+
+
+def _run_group(datas, ths, mask=None):
+    g = _Group(datas, [t.shape[0] for t in ths])
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lps = [torch.full((t.shape[0],), float("nan"), dtype=torch.float64, device="cuda") for t in ths]
+    gs = [torch.full(t.shape, float("nan"), dtype=torch.float32, device="cuda") for t in ths]
+    for i, t in enumerate(ths):
+        g.bind(i, t, lps[i], gs[i])
+    g.active(mask if mask is not None else [1] * len(ths))
+    g.run(err)
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    fused = g.fused()
+    g.close()
+    return lps, gs, fused
+
+
+def test_fused_pass_matches_fp64_and_is_independent_of_the_group():
+    raw = [_data(n, d, seed=7 * n + d + c, prior=p) for n, d, c, p in FUSED]
+    datas = [r[0] for r in raw]
+    rs = np.random.default_rng(3)
+    ths = [torch.as_tensor(rs.standard_normal((c, d.D)) * 0.3, dtype=torch.float32, device="cuda")
+           for d, (_, _, c, _) in zip(datas, FUSED)]
+    lps, gs, fused = _run_group(datas, ths)
+    assert fused
+    for (d, X64, y), th, lp, g in zip(raw, ths, lps, gs):
+        _fp64_check(X64, y, d, th, lp, g)
+    # each instance alone gives the same bits, and so does a subset
+    for i in (0, 5, 7):
+        lp1, g1, _ = _run_group([datas[i]], [ths[i]])
+        assert torch.equal(lp1[0], lps[i]) and torch.equal(g1[0], gs[i])
+    mask = [i % 3 != 1 for i in range(len(datas))]
+    lp2, g2, _ = _run_group(datas, ths, mask)
+    for m, a, b, ga, gb in zip(mask, lp2, lps, g2, gs):
+        if m:
+            assert torch.equal(a, b) and torch.equal(ga, gb)
+        else:
+            assert torch.isnan(a).all() and torch.isnan(ga).all()
+
+
+def test_two_gemm_grouped_pass_equals_each_instance_bit_for_bit():
     datas = [_data(n, d, seed=n + d + c, prior=p)[0] for n, d, c, p in SHAPES]
     Cs = [c for _, _, c, _ in SHAPES]
     rs = np.random.default_rng(0)
@@ -72,6 +133,7 @@ def test_grouped_pass_equals_each_instance_bit_for_bit():
     g.run(err)
     torch.cuda.synchronize()
     assert int(err.item()) == 0
+    assert not g.fused()          # D = 520: the two-GEMM grouped pass
     for d, th, lp, gr in zip(datas, ths, lps, gs):
         lp0, g0 = d.logp_grad(th)
         assert torch.equal(lp, lp0) and torch.equal(gr, g0)
@@ -132,7 +194,9 @@ def test_nuts_group_equals_each_instance_run_alone():
     assert len(set(ran)) > 1
     for (d, eps, init, seed), s, r in zip(raw, insts, grp.rounds):
         solo = H.BatchedNuts(d, 6, eps=eps, max_depth=5, seed=seed, init=init, hist_cap=24)
-        solo.run(r)
+        alone = H.NutsGroup([solo])
+        alone.step(r)
+        alone.close()
         assert torch.equal(solo.thprop, s.thprop)
         assert torch.equal(solo.hist, s.hist) and torch.equal(solo.hist_depth, s.hist_depth)
         np.testing.assert_array_equal(solo.info(), s.info())
