@@ -861,18 +861,63 @@ class NutsgInstC(C.Structure):
                 ("comp", C.c_uint32), ("logp_new", C.c_void_p), ("g_new", C.c_void_p)]
 
 
+class HlrGroup:
+    """Log density and gradient of many HlrbData instances, each with its own
+    chains, with one launch per stage (ab_hlrg_*): when every D <= 256 the
+    fused tensor-core kernel (forward, residual and backward per 128-row
+    tile, the residual kept on chip, the work units of all instances on one
+    persistent grid); otherwise the two-GEMM pass over all instances' tiles.
+    Bind each instance's theta [C_i, D_i] f32 and logp [C_i] f64 / grad
+    [C_i, D_i] f32 outputs (device tensors that outlive the group), then
+    choose the active instances; the tables live in device memory, so a CUDA
+    graph captured around logp_grad() follows later set_active() calls."""
+
+    def __init__(self, datas, chains):
+        L = N.lib()
+        self.datas = list(datas)
+        n = len(self.datas)
+        if n == 0:
+            raise ValueError("HlrGroup needs at least one data set")
+        models = (HlrbModelC * n)(*[d.c for d in self.datas])
+        cs = (C.c_int * n)(*[int(c) for c in chains])
+        self._h = C.c_void_p()
+        N.check(L.ab_hlrg_create(n, models, cs, C.byref(self._h)), "ab_hlrg_create")
+        self.fused = bool(L.ab_hlrg_fused(self._h))
+
+    def bind(self, i, theta, logp, grad):
+        N.check(N.lib().ab_hlrg_bind(self._h, i, N.ptr(theta), theta.stride(0), N.ptr(logp), N.ptr(grad),
+                                     grad.stride(0)), "ab_hlrg_bind")
+
+    def set_active(self, active, stream=None):
+        a = (C.c_int * len(self.datas))(*[1 if x else 0 for x in active])
+        N.check(N.lib().ab_hlrg_set_active(self._h, a, N.stream_ptr(stream)), "ab_hlrg_set_active")
+
+    def logp_grad(self, err=None, stream=None):
+        N.check(N.lib().ab_hlrg_logp_grad(self._h, N.ptr(err) if err is not None else None, N.stream_ptr(stream)),
+                "ab_hlrg_logp_grad")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            N.lib().ab_hlrg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class NutsGroup:
     """Many BatchedNuts samplers of uneven size (model instances with their
     own N and D) advanced together with ONE launch per stage: a round is one
     grouped advance launch (every running instance's chains walk to their
-    next leaf, ab_nutsg_advance) and one grouped tensor-core pass over all of
-    their data sets (ab_hlrg_logp_grad: split, forward, backward and finish,
-    one launch each, the tiles of every instance sharing one persistent
-    grid), captured as one CUDA graph.  The pass uses the built-in launch
-    shape: results equal each sampler's own rounds with `data.config` None,
-    bit for bit.  An instance leaves the launches once every one of its
+    next leaf, ab_nutsg_advance) and one HlrGroup pass over all of their
+    data sets (theta split, the fused tensor-core kernel, finishing sums),
+    captured as one CUDA graph.  An instance's results are the same alone or
+    in any group.  An instance leaves the launches once every one of its
     chains has `min_draws` draws (or its history is full, or it ran
-    `max_rounds` rounds in this call); the instance table lives in device
+    `max_rounds` rounds in this call); the instance tables live in device
     memory, so the captured graph follows the shrinking set without being
     captured again."""
 
@@ -883,15 +928,11 @@ class NutsGroup:
         if n == 0:
             raise ValueError("NutsGroup needs at least one sampler")
         dev = self.samplers[0].data.device
-        models = (HlrbModelC * n)(*[s.data.c for s in self.samplers])
-        cs = (C.c_int * n)(*[s.C for s in self.samplers])
-        self._pass = C.c_void_p()
-        N.check(L.ab_hlrg_create(n, models, cs, C.byref(self._pass)), "ab_hlrg_create")
+        self._pass = HlrGroup([s.data for s in self.samplers], [s.C for s in self.samplers])
         self._adv = C.c_void_p()
         try:
             for i, s in enumerate(self.samplers):
-                N.check(L.ab_hlrg_bind(self._pass, i, N.ptr(s.thprop), s.D, N.ptr(s.logp_new), N.ptr(s.g_new), s.D),
-                        "ab_hlrg_bind")
+                self._pass.bind(i, s.thprop, s.logp_new, s.g_new)
             insts = (NutsgInstC * n)(*[NutsgInstC(s.mem.data_ptr(), s.C, s.D, s.hist_cap, s.max_depth,
                                                   BatchedNuts.VARIANTS[s.variant], s.eps, s.seed, s.comp,
                                                   s.logp_new.data_ptr(), s.g_new.data_ptr())
@@ -910,13 +951,13 @@ class NutsGroup:
     def _set_active(self, active, stream=None):
         n = len(self.samplers)
         a = (C.c_int * n)(*[1 if x else 0 for x in active])
-        N.check(N.lib().ab_hlrg_set_active(self._pass, a, N.stream_ptr(stream)), "ab_hlrg_set_active")
+        self._pass.set_active(active, stream)
         N.check(N.lib().ab_nutsg_set_active(self._adv, a, N.stream_ptr(stream)), "ab_nutsg_set_active")
         self.active = list(active)
 
     def _round(self, stream=None):
         N.check(N.lib().ab_nutsg_advance(self._adv, N.stream_ptr(stream)), "ab_nutsg_advance")
-        N.check(N.lib().ab_hlrg_logp_grad(self._pass, N.ptr(self.err), N.stream_ptr(stream)), "ab_hlrg_logp_grad")
+        self._pass.logp_grad(self.err, stream)
 
     def _count(self, reps):
         for i, a in enumerate(self.active):
@@ -983,7 +1024,7 @@ class NutsGroup:
             N.lib().ab_nutsg_destroy(self._adv)
             self._adv = None
         if getattr(self, "_pass", None):
-            N.lib().ab_hlrg_destroy(self._pass)
+            self._pass.close()
             self._pass = None
 
     def __del__(self):

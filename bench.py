@@ -285,6 +285,63 @@ def nuts_instances(n_inst=NUTS_INST, seed=0):
     return [(int(n), int(d)) for n, d in zip(Ns, Ds)]
 
 
+def run_hlr_group(scale=1.0, steps=10, warmup=3, n_inst=NUTS_INST, chains=NUTS_C):
+    """The grouped HLR pass alone on the 64 config-4 instances with every N_i
+    scaled by `scale` (scale 1: the NUTS workload's data, X ~ N(0,1) bf16):
+    log density and gradient of 512 chains per instance at theta = the
+    generating coefficients plus noise, one HlrGroup pass (theta split, the
+    fused tensor-core kernel, finishing sums) for all instances; device time
+    per pass and tensor-pipe throughput."""
+    import torch
+    from augurv2_b200 import hlrb as H
+    specs = [(max(64, int(n * scale)), d) for n, d in nuts_instances(n_inst)]
+    rng = np.random.default_rng(42)
+    datas, ths, lps, gs = [], [], [], []
+    for i, (Ni, Di) in enumerate(specs):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(1000 + i)
+        X = torch.randn((Ni, Di), generator=g, device="cuda").to(torch.bfloat16)
+        beta = rng.standard_normal(Di).astype(np.float32) * 0.5
+        t = X.float() @ torch.as_tensor(beta, device="cuda")
+        y = (torch.rand(Ni, generator=g, device="cuda") < torch.sigmoid(t)).to(torch.int32)
+        datas.append(H.HlrbData(X, y, prior="normal", var=1.0))
+        ths.append(torch.as_tensor(beta[None] + 0.01 * rng.standard_normal((chains, Di)).astype(np.float32),
+                                   device="cuda").contiguous())
+        lps.append(torch.empty(chains, dtype=torch.float64, device="cuda"))
+        gs.append(torch.empty((chains, Di), dtype=torch.float32, device="cuda"))
+    grp = H.HlrGroup(datas, [chains] * len(datas))
+    for i in range(len(datas)):
+        grp.bind(i, ths[i], lps[i], gs[i])
+    grp.set_active([True] * len(datas))
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for _ in range(warmup):
+        grp.logp_grad(err)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        grp.logp_grad(err)
+    e1.record()
+    torch.cuda.synchronize()
+    if int(err.item()) != 0:
+        raise RuntimeError("device wait timed out in the grouped HLR pass")
+    ms = e0.elapsed_time(e1) / steps
+    nd = float(sum(n * d for n, d in specs))
+    alg = 4.0 * nd * chains                      # forward + backward products
+    peak, kind = measured_tensor_peak(sustained=True)
+    out = {"metric": "grouped HLR pass (logp + grad, 512 chains per instance, all instances)", "value": ms,
+           "unit": "ms", "higher_is_better": False, "fused": grp.fused,
+           "roofline": {"bound": "tensor", "kernel": "hlrf_kernel" if grp.fused else "grouped_gemm_kernel",
+                        "achieved": alg / (ms / 1e3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                        "frac": alg / (ms / 1e3) / 1e12 / peak, "peak_source": kind + " (sustained)",
+                        "executed_tflops": 2.5 * alg / (ms / 1e3) / 1e12,
+                        "note": "algorithmic 4 N D C per instance (forward and backward product); the pipe "
+                                "executes 2.5x (3 bf16 parts of theta forward, 2 of the residual backward)"},
+           "config": {"workload": "hlr_group_64_instances_c512", "scale": scale, "sum_N": int(sum(n for n, _ in specs)),
+                      "sum_ND": int(nd), "D": "{16, 64, 256}", "chains": chains}}
+    grp.close()
+    return out
+
+
 def nuts_cpu_baseline(per, chains, budget_s=12.0, max_nd=4_000_000):
     """The reference's NUTS on the host, one chain per core, for every
     instance of the run, from timed pieces of its own code: each NUTS leaf of
@@ -982,7 +1039,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-secondary", action="store_true", help="skip the surrogate HLR measurement")
     ap.add_argument("--workload", default="lda",
-                    choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm", "hlr_nuts"])
+                    choices=["lda", "hlr_surrogate", "hlr_pass", "hlr_small", "gmm", "hlr_nuts", "hlr_group"])
+    ap.add_argument("--group-scale", type=float, default=1.0, help="hlr_group: factor on every instance's N")
     ap.add_argument("--nuts-rounds", type=int, default=2400, help="batched NUTS: round cap per instance")
     ap.add_argument("--nuts-draws", type=int, default=48, help="batched NUTS: draws per chain per instance")
     ap.add_argument("--hlr-n", type=int, default=HLR_N, help="rows for --workload hlr_pass")
@@ -1009,6 +1067,10 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         line = run_hlr_nuts(min_draws=args.nuts_draws, max_rounds=args.nuts_rounds) if rank == 0 else None
+    elif args.workload == "hlr_group":
+        import torch
+        torch.cuda.set_device(local_rank)
+        line = run_hlr_group(args.group_scale, args.steps, args.warmup) if rank == 0 else None
     elif args.workload == "hlr_pass":
         import torch
         torch.cuda.set_device(local_rank)
