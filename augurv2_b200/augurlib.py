@@ -84,7 +84,7 @@ def recognise(model):
         raise Unsupported("models with exactly one data declaration are supported")
     y = datas[0]
     fn = y.dist.fn
-    if fn == "Bernoulli":
+    if fn in ("Bernoulli", "Poisson", "Normal"):
         return "hlr", _rec_hlr(model, params, dets, y)
     if fn == "Categorical":
         return "lda", _rec_lda(model, params, dets, y)
@@ -94,6 +94,11 @@ def recognise(model):
 
 
 def _rec_hlr(model, params, dets, y):
+    """Regressions on a linear predictor t = dotprod(theta, x[n]) [+ b] with
+    theta[k] ~ Normal(0, v), b ~ Normal(0, v), v ~ Exponential | InvGamma:
+    y[n] ~ Bernoulli(sigmoid(t)) (hlr.rv, dethlr.rv), Poisson(exp(t)) or
+    Normal(t, s2) with s2 a hyper-parameter or a number."""
+    fn = y.dist.fn
     arg = y.dist.args[0]
     det = None
     if _is_idx(arg) and len(dets) == 1 and arg.base.name == dets[0].name:
@@ -101,9 +106,21 @@ def _rec_hlr(model, params, dets, y):
         arg = det.expr
     elif dets:
         raise Unsupported("deterministic declarations other than the bias of hlr")
-    if not (isinstance(arg, rv.Call) and arg.fn == "sigmoid"):
-        raise Unsupported("Bernoulli(sigmoid(...)) expected")
-    lin = arg.args[0]
+    obs_var = None
+    if fn == "Bernoulli":
+        if not (isinstance(arg, rv.Call) and arg.fn == "sigmoid"):
+            raise Unsupported("Bernoulli(sigmoid(...)) expected")
+        lin = arg.args[0]
+    elif fn == "Poisson":
+        if det is not None or not (isinstance(arg, rv.Call) and arg.fn == "exp"):
+            raise Unsupported("Poisson(exp(...)) expected")
+        lin = arg.args[0]
+    else:
+        if det is not None or len(y.dist.args) != 2:
+            raise Unsupported("Normal(dotprod(theta, x[n]) [+ b], s2) expected")
+        lin, obs_var = arg, y.dist.args[1]
+        if _is_var(obs_var) and obs_var.name in {d.name for d in params}:
+            raise Unsupported("the observation variance of a Normal likelihood must be a hyper-parameter")
     bias = None
     if isinstance(lin, rv.BinOp) and lin.op == "+":
         lin, bias = lin.lhs, lin.rhs
@@ -132,7 +149,8 @@ def _rec_hlr(model, params, dets, y):
     if set(byname) != names:
         raise Unsupported("unexpected parameters %s" % sorted(set(byname) - names))
     return {"theta": theta.name, "b": b.name if b else None, "v": v.name, "x": xn.base.name,
-            "y": y.name, "vprior": v.dist, "det": det.name if det else None, "order": [d.name for d in params]}
+            "y": y.name, "vprior": v.dist, "det": det.name if det else None, "order": [d.name for d in params],
+            "lik": {"Bernoulli": "bernoulli", "Poisson": "poisson", "Normal": "normal"}[fn], "obs_var": obs_var}
 
 
 def _rec_lda(model, params, dets, w):

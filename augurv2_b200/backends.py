@@ -99,7 +99,9 @@ class HlrBackend:
         X = np.asarray(hyp[info["x"]], np.float64)
         if X.dtype == object:
             X = np.array([np.asarray(r, np.float64) for r in X])
-        y = np.asarray(data[0], np.int32)
+        lik = info.get("lik", "bernoulli")
+        y = np.asarray(data[0], np.float64 if lik == "normal" else np.int32)
+        obs_var = float(_val(info["obs_var"], hyp)) if lik == "normal" else 1.0
         vp = info["vprior"]
         if vp.fn == "Exponential":
             pri = dict(vprior="exponential", lam=_val(vp.args[0], hyp))
@@ -108,7 +110,7 @@ class HlrBackend:
         self.has_b = info["b"] is not None
         self.X = X
         self.data = HlrData(X, y, has_b=self.has_b, compat=opt.compat, x_dtype=opt.x_dtype,
-                            device=opt.device, **pri)
+                            device=opt.device, lik=lik, obs_var=obs_var, **pri)
         role = {info["theta"]: "theta", info["v"]: "v"}
         if self.has_b:
             role[info["b"]] = "b"

@@ -21,6 +21,7 @@
 // deterministic.  Priors, momenta, energies and the accept tests are binary64
 // in the reference's operation order (cbits/augur_dist.c, augur_mcmclib.h).
 #include <cuda_bf16.h>
+#include <math.h>
 
 #include "common.cuh"
 #include "philox.cuh"
@@ -41,6 +42,10 @@ struct HlrModelDev {
   double lam, a0, s0;
   const void* X;
   const int* y;
+  int lik;              // AB_LIK_*
+  float inv_var;        // AB_LIK_NORMAL: 1 / obs_var
+  double ll_add;        // AB_LIK_NORMAL: N times the per-row normaliser, added once
+  const float* yr;
 };
 
 struct HlrComp {
@@ -66,6 +71,26 @@ __device__ __forceinline__ void bern_terms(int y, float t, float& ll, float& r) 
   ll = y ? t - sp : -sp;
   const float sg = 1.0f / (1.0f + __expf(-t));
   r = (float)y - sg;
+}
+
+// Data factor of row n at t and its derivative in t, FP32: the logistic
+// terms above, Poisson(exp(t)): y t - exp(t) - lgamma(y + 1) and y - exp(t)
+// (the reference's y log(rate) - rate - sum_{k <= y} log k and its adjoint
+// through exp), Normal(t, obs_var): -(y - t)^2 / (2 var) and (y - t) / var
+// (the normaliser is added once per pass, ll_add).
+__device__ __forceinline__ void lik_terms(const HlrModelDev& m, int n, float t, float& ll, float& r) {
+  if (m.lik == AB_LIK_POISSON) {
+    const int y = m.y[n];
+    const float rate = expf(t);
+    ll = (float)y * t - rate - lgammaf((float)y + 1.0f);
+    r = (float)y - rate;
+  } else if (m.lik == AB_LIK_NORMAL) {
+    const float d = m.yr[n] - t;
+    ll = -0.5f * d * d * m.inv_var;
+    r = d * m.inv_var;
+  } else {
+    bern_terms(m.y[n], t, ll, r);
+  }
 }
 
 // Shared-memory workspace of one chain CTA (sizes fixed by D).
@@ -145,7 +170,7 @@ __device__ double data_pass_small(const HlrModelDev& m, const double* par, Ws& w
       t += x[k] * th[k];
     }
     float llv, rv;
-    bern_terms(m.y[n], t + bias, llv, rv);
+    lik_terms(m, n, t + bias, llv, rv);
     kahan_add(s[COLS - 1], c[COLS - 1], llv);
     if (want_grad) {
 #pragma unroll
@@ -216,7 +241,7 @@ __device__ double data_pass(const HlrModelDev& m, const double* par, Ws& ws, boo
       for (int o = S >> 1; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
       if (ls == 0 && i < nc) {
         float llv, rv;
-        bern_terms(m.y[n], part + bias, llv, rv);
+        lik_terms(m, n, part + bias, llv, rv);
         kahan_add(lls, llc, llv);
         ws.r[i] = rv;
       }
@@ -305,7 +330,7 @@ __device__ double block_ll_grad(const HlrModelDev& m, const double* par, const i
   const int D = m.D;
   const BlockInfo bi = block_info(m, idx, P);
   double data_ll = 0.0;
-  if (bi.th || bi.b) data_ll = data_pass(m, par, ws, want_grad);
+  if (bi.th || bi.b) data_ll = data_pass(m, par, ws, want_grad) + m.ll_add;
   const double b = m.has_b ? par[D] : 0.0, v = par[D + 1];
   // prior terms of the coefficients, one per thread; thread 0 then adds
   // them in the reference's (sequential) order
@@ -800,13 +825,23 @@ static int make_model(HlrModelDev& m, const ab_hlr_model* d) {
   AB_REQUIRE(d != nullptr, AB_ERR_ARG, "hlr: null model");
   AB_REQUIRE(d->N > 0 && d->D > 0 && d->D <= HLR_MAX_D, AB_ERR_ARG,
              "hlr: need N > 0 and 0 < D <= %d (N=%d D=%d)", HLR_MAX_D, d->N, d->D);
-  AB_REQUIRE(d->X && d->y, AB_ERR_ARG, "hlr: null data pointer");
+  AB_REQUIRE(d->lik == AB_LIK_BERNOULLI || d->lik == AB_LIK_POISSON || d->lik == AB_LIK_NORMAL, AB_ERR_ARG,
+             "hlr: unknown likelihood %d", d->lik);
+  AB_REQUIRE(d->X && (d->lik == AB_LIK_NORMAL ? d->yr != nullptr : d->y != nullptr), AB_ERR_ARG,
+             "hlr: null data pointer");
+  AB_REQUIRE(d->lik != AB_LIK_NORMAL || d->obs_var > 0.0, AB_ERR_ARG, "hlr: the observation variance must be > 0");
   AB_REQUIRE(d->x_dtype == AB_F32 || d->x_dtype == AB_BF16, AB_ERR_ARG, "hlr: X must be f32 or bf16");
   AB_REQUIRE(d->ldx >= d->D, AB_ERR_ARG, "hlr: ldx < D");
   AB_REQUIRE(d->vprior == 0 || d->vprior == 1, AB_ERR_ARG, "hlr: vprior must be 0 or 1");
   m.N = d->N; m.D = d->D; m.ldx = d->ldx; m.has_b = d->has_b != 0; m.vprior = d->vprior;
   m.compat = d->compat != 0; m.x_bf16 = d->x_dtype == AB_BF16;
   m.lam = d->lam; m.a0 = d->a0; m.s0 = d->s0; m.X = d->X; m.y = d->y;
+  m.lik = d->lik;
+  m.yr = d->yr;
+  m.inv_var = d->lik == AB_LIK_NORMAL ? (float)(1.0 / d->obs_var) : 0.0f;
+  // per-row Normal normaliser: the reference's -log(var) (compat) or -log(2 pi var) / 2
+  m.ll_add = d->lik != AB_LIK_NORMAL ? 0.0
+             : (double)d->N * (m.compat ? -log(d->obs_var) : -0.5 * log(2.0 * M_PI * d->obs_var));
   return AB_OK;
 }
 

@@ -5,6 +5,8 @@ Model (compiler/augur/test/hlr.rv):
     b ~ Normal(0, v)                (optional)
     theta[k] ~ Normal(0, v)         for k < D
     y[n] ~ Bernoulli(sigmoid(dotprod(theta, x[n]) + b))
+or, with the same priors, y[n] ~ Poisson(exp(dotprod(theta, x[n]) + b)) or
+y[n] ~ Normal(dotprod(theta, x[n]) + b, obs_var) (lik="poisson" / "normal").
 A chain's parameters are one f64 vector [theta[0..D-1], b, v]; schedule
 components (HMC / NUTS / MWG) move blocks of it.  All chains run on the
 device, one thread block per chain (hlr.cu).
@@ -30,7 +32,11 @@ class HlrModelC(C.Structure):
     _fields_ = [("N", C.c_int), ("D", C.c_int), ("ldx", C.c_int), ("has_b", C.c_int),
                 ("vprior", C.c_int), ("compat", C.c_int), ("x_dtype", C.c_int),
                 ("lam", C.c_double), ("a0", C.c_double), ("s0", C.c_double),
-                ("X", C.c_void_p), ("y", C.c_void_p)]
+                ("X", C.c_void_p), ("y", C.c_void_p), ("lik", C.c_int), ("obs_var", C.c_double),
+                ("yr", C.c_void_p)]
+
+
+LIKELIHOODS = {"bernoulli": 0, "poisson": 1, "normal": 2}
 
 
 def block_indices(names, D):
@@ -49,22 +55,32 @@ def block_indices(names, D):
 
 
 class HlrData:
-    """Design matrix and labels resident on the device (f32 or bf16)."""
+    """Design matrix and labels resident on the device (f32 or bf16).
+    lik: "bernoulli" (0/1 labels), "poisson" (counts) or "normal" (real
+    labels, observation variance obs_var)."""
 
     def __init__(self, X, y, has_b=True, vprior="exponential", lam=1.0, a0=1.0, s0=1.0,
-                 compat=True, x_dtype="f32", device="cuda"):
+                 compat=True, x_dtype="f32", device="cuda", lik="bernoulli", obs_var=1.0):
         X = np.asarray(X)
         self.N, self.D = X.shape
         tdt = {"f32": torch.float32, "bf16": torch.bfloat16}[x_dtype]
         self.X = torch.as_tensor(np.ascontiguousarray(X, dtype=np.float32)).to(device=device, dtype=tdt)
-        self.y = torch.as_tensor(np.ascontiguousarray(y, dtype=np.int32)).to(device)
+        self.lik = LIKELIHOODS[lik]
+        self.obs_var = float(obs_var)
+        if self.lik == LIKELIHOODS["normal"]:
+            self.yr = torch.as_tensor(np.ascontiguousarray(y, dtype=np.float32)).to(device)
+            self.y = torch.zeros(self.N, dtype=torch.int32, device=device)
+        else:
+            self.y = torch.as_tensor(np.ascontiguousarray(y, dtype=np.int32)).to(device)
+            self.yr = None
         self.has_b = bool(has_b)
         self.vprior = {"exponential": 0, "invgamma": 1}[vprior]
         self.compat = bool(compat)
         self.x_dtype = {"f32": 0, "bf16": 1}[x_dtype]
         self.lam, self.a0, self.s0 = float(lam), float(a0), float(s0)
         self.c = HlrModelC(self.N, self.D, self.D, int(self.has_b), self.vprior, int(self.compat),
-                           self.x_dtype, self.lam, self.a0, self.s0, self.X.data_ptr(), self.y.data_ptr())
+                           self.x_dtype, self.lam, self.a0, self.s0, self.X.data_ptr(), self.y.data_ptr(),
+                           self.lik, self.obs_var, self.yr.data_ptr() if self.yr is not None else None)
 
 
 def ll_grad(data, pars, idx, stream=None):

@@ -178,8 +178,20 @@ typedef struct ab_hlr_model {
   int x_dtype;          /* AB_F32 or AB_BF16                                  */
   double lam, a0, s0;
   const void* X;        /* device [N][ldx] */
-  const int* y;         /* device [N], 0/1 */
+  const int* y;         /* device [N]: 0/1 (Bernoulli) or counts >= 0 (Poisson) */
+  /* The data factor, with t = theta . x[n] + b (zero-initialised: the
+   * logistic model above).  AB_LIK_POISSON: y[n] ~ Poisson(exp(t))
+   * (augur_poisson_ll, cbits/augur_dist.c:124-130, adjoint through exp);
+   * AB_LIK_NORMAL: yr[n] ~ Normal(t, obs_var) with a fixed variance
+   * (augur_normal_ll, :372-381; compat selects the reference's -log(var)
+   * normaliser).  The reference's modelling language states these as
+   * `data y[n] ~ Poisson(exp(dotprod(theta, x[n]) + b))` and
+   * `data y[n] ~ Normal(dotprod(theta, x[n]) + b, s2)`. */
+  int lik;              /* AB_LIK_BERNOULLI (0), AB_LIK_POISSON, AB_LIK_NORMAL */
+  double obs_var;       /* AB_LIK_NORMAL: observation variance > 0 */
+  const float* yr;      /* AB_LIK_NORMAL: device [N] real labels */
 } ab_hlr_model;
+enum { AB_LIK_BERNOULLI = 0, AB_LIK_POISSON = 1, AB_LIK_NORMAL = 2 };
 
 /* One schedule component: kind 0 = HMC [block] [simlen, eps]
  * (h_augur_mcmc_hmc, cbits/augur_mcmclib.h:389-424), 1 = NUTS [block] [eps]

@@ -174,7 +174,12 @@ void orc_lda_sweeps(int D, int K, int V, const int* doc_off, const int* w,
  * Hierarchical logistic regression (compiler/augur/test/hlr.rv and the
  * InvGamma-variance variant without bias):
  *   v ~ Exponential(lam) | InvGamma(a0, s0);  b ~ Normal(0, v) (optional);
- *   theta[k] ~ Normal(0, v);  y[n] ~ Bernoulli(sigmoid(theta . x[n] + b)).
+ *   theta[k] ~ Normal(0, v);  y[n] ~ Bernoulli(sigmoid(theta . x[n] + b)),
+ * and the same priors with the other generalised-linear likelihoods the
+ * reference's modelling language can state with t = theta . x[n] + b
+ * (lik): 1 y[n] ~ Poisson(exp(t)) (augur_poisson_ll, cbits/augur_dist.c:
+ * 124-130), 2 yr[n] ~ Normal(t, obs_var) with a fixed variance
+ * (augur_normal_ll, :372-381).
  * Parameters are one vector par = [theta[0..D-1], b, v].  A block is a list
  * of indices into par in the schedule's order (HMC [v, b, theta] -> D+1, D,
  * 0..D-1).  `compat` selects the reference's own density formulas
@@ -188,7 +193,10 @@ typedef struct {
   int N, D, has_b, vprior, compat; /* vprior: 0 Exponential(lam), 1 InvGamma(a0, s0) */
   double lam, a0, s0;
   const double* X; /* N x D row-major */
-  const int* y;
+  const int* y;    /* Bernoulli and Poisson labels */
+  int lik;         /* 0 Bernoulli(sigmoid(t)), 1 Poisson(exp(t)), 2 Normal(t, obs_var) */
+  double obs_var;
+  const double* yr; /* Normal labels */
 } orc_hlr;
 
 static double orc_expit(double x) { return 1.0 / (1.0 + exp(-x)); }
@@ -242,6 +250,36 @@ static double orc_bern_dt(const orc_hlr* m, int y, double t) {
   return (double)y - orc_expit(t);
 }
 
+/* Poisson(exp(t)): the reference's y log(rate) - rate - sum_{k <= y} log k
+ * and its adjoint through exp, augur_poisson_dotarg1 (:132-139) x exp(t);
+ * compat = 0: y t - exp(t) - lgamma(y + 1) and y - exp(t). */
+static double orc_pois_ll(const orc_hlr* m, int y, double t) {
+  if (m->compat) {
+    const double rate = exp(t);
+    double acc = 0.0;
+    for (int k = 1; k <= y; k++) acc += log((double)k);
+    return y * log(rate) - rate - acc;
+  }
+  return y * t - exp(t) - lgamma(y + 1.0);
+}
+static double orc_pois_dt(const orc_hlr* m, int y, double t) {
+  const double rate = exp(t);
+  if (m->compat) return (rate > 0.0 ? y / rate - 1.0 : -ORC_LARGE) * rate;
+  return y - rate;
+}
+
+/* Data factor of row n at t and its derivative, by likelihood. */
+static double orc_lik_ll(const orc_hlr* m, int n, double t) {
+  if (m->lik == 1) return orc_pois_ll(m, m->y[n], t);
+  if (m->lik == 2) return orc_normal_ll(m, m->yr[n], t, m->obs_var);
+  return orc_bern_ll(m, m->y[n], t);
+}
+static double orc_lik_dt(const orc_hlr* m, int n, double t) {
+  if (m->lik == 1) return orc_pois_dt(m, m->y[n], t);
+  if (m->lik == 2) return (m->yr[n] - t) / m->obs_var;   /* augur_normal_dotarg1, :388-390 */
+  return orc_bern_dt(m, m->y[n], t);
+}
+
 static int orc_in_block(const int* idx, int P, int lo, int hi) {
   for (int j = 0; j < P; ++j) if (idx[j] >= lo && idx[j] < hi) return 1;
   return 0;
@@ -270,7 +308,7 @@ double orc_hlr_ll(const orc_hlr* m, const double* par, const int* idx, int P) {
       const double* x = m->X + (size_t)n * D;
       double dot = 0.0;
       for (int k = 0; k < D; ++k) dot += par[k] * x[k];
-      s += orc_bern_ll(m, m->y[n], dot + b);
+      s += orc_lik_ll(m, n, dot + b);
     }
     ll += s;
   }
@@ -303,7 +341,7 @@ void orc_hlr_grad(const orc_hlr* m, const double* par, const int* idx, int P, do
       const double* x = m->X + (size_t)n * D;
       double dot = 0.0;
       for (int k = 0; k < D; ++k) dot += par[k] * x[k];
-      double r = orc_bern_dt(m, m->y[n], dot + b);
+      double r = orc_lik_dt(m, n, dot + b);
       if (in_b) full[D] += r;
       if (in_th) for (int k = 0; k < D; ++k) full[k] += r * x[k];
     }

@@ -194,16 +194,30 @@ class Oracle:
 class OrcHlr(C.Structure):
     _fields_ = [("N", C.c_int), ("D", C.c_int), ("has_b", C.c_int), ("vprior", C.c_int),
                 ("compat", C.c_int), ("lam", C.c_double), ("a0", C.c_double), ("s0", C.c_double),
-                ("X", _dp), ("y", _ip)]
+                ("X", _dp), ("y", _ip), ("lik", C.c_int), ("obs_var", C.c_double), ("yr", _dp)]
+
+
+LIKELIHOODS = {"bernoulli": 0, "poisson": 1, "normal": 2}
 
 
 class HlrModel:
     """Data and hyper-parameters of one HLR instance (oracle side).
-    vprior: "exponential" (hlr.rv, rate lam) or "invgamma" (a0, s0)."""
+    vprior: "exponential" (hlr.rv, rate lam) or "invgamma" (a0, s0).
+    lik: "bernoulli" (y ~ Bernoulli(sigmoid(t))), "poisson" (y ~
+    Poisson(exp(t))) or "normal" (y ~ Normal(t, obs_var), y real), with
+    t = theta . x[n] + b."""
 
-    def __init__(self, X, y, has_b=True, vprior="exponential", lam=1.0, a0=1.0, s0=1.0, compat=True):
+    def __init__(self, X, y, has_b=True, vprior="exponential", lam=1.0, a0=1.0, s0=1.0, compat=True,
+                 lik="bernoulli", obs_var=1.0):
         self.X = np.ascontiguousarray(X, dtype=np.float64)
-        self.y = np.ascontiguousarray(y, dtype=np.int32)
+        self.lik = LIKELIHOODS[lik]
+        if self.lik == 2:
+            self.yr = np.ascontiguousarray(y, dtype=np.float64)
+            self.y = np.zeros(len(self.yr), np.int32)
+        else:
+            self.y = np.ascontiguousarray(y, dtype=np.int32)
+            self.yr = np.zeros(len(self.y), np.float64)
+        self.obs_var = float(obs_var)
         self.N, self.D = self.X.shape
         self.has_b, self.compat = int(has_b), int(compat)
         self.vprior = {"exponential": 0, "invgamma": 1}[vprior]
@@ -211,7 +225,7 @@ class HlrModel:
 
     def struct(self):
         return OrcHlr(self.N, self.D, self.has_b, self.vprior, self.compat, self.lam, self.a0, self.s0,
-                      dptr(self.X), iptr(self.y))
+                      dptr(self.X), iptr(self.y), self.lik, self.obs_var, dptr(self.yr))
 
     def flat(self):
         return (self.N, self.D, self.has_b, self.vprior, self.lam, self.a0, self.s0,
@@ -226,6 +240,9 @@ def _hlr_call(o, name, m, restype, extra_types, *extra):
     if o.kind == "ref":
         if not m.compat:
             raise ValueError("the reference build only has the reference's own densities")
+        g = o.fn("glm_set", None)
+        g.argtypes = [C.c_int, C.c_double, _dp]
+        g(m.lik, m.obs_var, dptr(m.yr))
         f.argtypes = _FLAT + extra_types
         return f(*m.flat(), *extra)
     s = m.struct()

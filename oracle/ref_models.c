@@ -174,6 +174,33 @@ typedef struct {
 
 static ref_hlr_t g_hlr;
 
+/* The likelihood of the data factor (the generated code differs only there):
+ * 0 y[n] ~ Bernoulli(sigmoid(t)), 1 y[n] ~ Poisson(exp(t)), 2 yr[n] ~
+ * Normal(t, obs_var) with a fixed variance; t = theta . x[n] + b.  Set before
+ * each ref_hlr_* call (ref_glm_set). */
+static int g_lik = 0;
+static double g_obs_var = 1.0;
+static const double* g_yr = 0;
+
+void ref_glm_set(int lik, double obs_var, const double* yr) {
+  g_lik = lik;
+  g_obs_var = obs_var;
+  g_yr = yr;
+}
+
+/* Data factor of row n at t, and the adjoint of t (the generated chain:
+ * the distribution's dotarg1 times the link's derivative). */
+static double ref_lik_ll(int n, double t) {
+  if (g_lik == 1) return augur_poisson_ll(g_hlr.y[n], augur_exp(t));
+  if (g_lik == 2) return augur_normal_ll(g_yr[n], t, g_obs_var);
+  return augur_bernoulli_ll(g_hlr.y[n], augur_expit(t));
+}
+static double ref_lik_adj(int n, double t) {
+  if (g_lik == 1) return augur_poisson_dotarg1(g_hlr.y[n], augur_exp(t)) * augur_exp(t);
+  if (g_lik == 2) return augur_normal_dotarg1(g_yr[n], t, g_obs_var);
+  return augur_bernoulli_dotarg1(g_hlr.y[n], augur_expit(t)) * augur_expit_grad_0(t);
+}
+
 static int in_blk(int lo, int hi) {
   for (int j = 0; j < g_hlr.P; ++j) if (g_hlr.idx[j] >= lo && g_hlr.idx[j] < hi) return 1;
   return 0;
@@ -208,7 +235,7 @@ static double ref_hlr_ll_fn(AugurAux_t aux, AugurMod_t mod) {
     for (int n = 0; n < g_hlr.N; ++n) {
       AugurVec_t xn = dvec((double*)g_hlr.X + (size_t)n * D, D);
       double t = augur_dotprod(&th, &xn) + b;
-      s += augur_bernoulli_ll(g_hlr.y[n], augur_expit(t));
+      s += ref_lik_ll(n, t);
     }
     ll += s;
   }
@@ -240,9 +267,7 @@ static void ref_hlr_grad_fn(AugurAux_t aux, AugurMod_t mod) {
     for (int n = 0; n < g_hlr.N; ++n) {
       AugurVec_t xn = dvec((double*)g_hlr.X + (size_t)n * D, D);
       double t2 = augur_dotprod(&th, &xn) + b;
-      double t3 = augur_expit(t2);
-      double adj3 = augur_bernoulli_dotarg1(g_hlr.y[n], t3);
-      double adj2 = adj3 * augur_expit_grad_0(t2);
+      double adj2 = ref_lik_adj(n, t2);
       if (in_b) full[D] += adj2 * 1;
       if (in_th) {
         augur_dotprod_grad_0(&vdst, adj2 * 1, &th, &xn);

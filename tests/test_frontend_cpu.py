@@ -49,6 +49,37 @@ def test_unsupported_model_is_refused():
         augurlib.recognise(rv.parse_model(src))
 
 
+def test_glm_regressions_are_recognised():
+    """Poisson and linear regressions on dotprod(theta, x[n]) [+ b] with the
+    hlr.rv priors run on the HLR engine with their own likelihood; a Normal
+    likelihood whose variance is a sampled parameter is refused."""
+    pois = """(K : Int, N : Int, lam : Real, x : Vec (Vec Real)) => {
+      param v ~ Exponential(lam) ;
+      param b ~ Normal(0.0, v) ;
+      param theta[k] ~ Normal(0.0, v) for k <- 0 until K ;
+      data y[n] ~ Poisson( exp(dotprod(theta, x[n]) + b) ) for n <- 0 until N ;
+    }"""
+    fam, info = augurlib.recognise(rv.parse_model(pois))
+    assert fam == "hlr" and info["lik"] == "poisson" and info["b"] == "b"
+    lin = """(K : Int, N : Int, a0 : Real, s0 : Real, s2 : Real, x : Vec (Vec Real)) => {
+      param v ~ InvGamma(a0, s0) ;
+      param theta[k] ~ Normal(0.0, v) for k <- 0 until K ;
+      data y[n] ~ Normal(dotprod(theta, x[n]), s2) for n <- 0 until N ;
+    }"""
+    fam, info = augurlib.recognise(rv.parse_model(lin))
+    assert fam == "hlr" and info["lik"] == "normal" and info["obs_var"].name == "s2" and info["b"] is None
+    sampled_var = """(K : Int, N : Int, a0 : Real, s0 : Real, x : Vec (Vec Real)) => {
+      param v ~ InvGamma(a0, s0) ;
+      param theta[k] ~ Normal(0.0, v) for k <- 0 until K ;
+      data y[n] ~ Normal(dotprod(theta, x[n]), v) for n <- 0 until N ;
+    }"""
+    with pytest.raises(NotImplementedError):
+        augurlib.recognise(rv.parse_model(sampled_var))
+    no_link = pois.replace("Poisson( exp(dotprod(theta, x[n]) + b) )", "Poisson(dotprod(theta, x[n]) + b)")
+    with pytest.raises(NotImplementedError):
+        augurlib.recognise(rv.parse_model(no_link))
+
+
 def test_syntax_errors_are_reported():
     with pytest.raises(rv.RvSyntaxError):
         rv.parse_model("(K : Int) => { param x ~ ; }")

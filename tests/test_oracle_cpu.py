@@ -189,6 +189,55 @@ def test_hlr_gradient_finite_difference(orc):
         assert abs(fd - g[j]) <= 1e-5 * max(1.0, abs(g[j]))
 
 
+def _glm_data(lik, N, D, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((N, D))
+    beta = rng.standard_normal(D) * 0.3
+    t = X @ beta + 0.1
+    if lik == "poisson":
+        y = rng.poisson(np.exp(t)).astype(np.int32)
+    else:
+        y = t + rng.standard_normal(N) * 0.7
+    return X, y, beta
+
+
+@pytest.mark.parametrize("lik", ["poisson", "normal"])
+def test_glm_oracle_vs_reference_live(orc, ref, lik):
+    """Poisson(exp(t)) and Normal(t, obs_var) likelihoods with the HLR priors:
+    the oracle's restatement equals the reference's own cbits densities,
+    adjoints and NUTS / HMC transitions bit for bit."""
+    X, y, beta = _glm_data(lik, 80, 3, 11)
+    m = O.HlrModel(X, y, has_b=True, vprior="invgamma", lik=lik, obs_var=0.49)
+    par = np.concatenate([beta, [0.1], [1.3]])
+    for idx in [[0, 1, 2], [3], [4], [4, 3, 0, 1, 2]]:
+        assert O.hlr_ll(orc, m, par, idx) == O.hlr_ll(ref, m, par, idx)
+        np.testing.assert_array_equal(O.hlr_grad(orc, m, par, idx), O.hlr_grad(ref, m, par, idx))
+    for it in range(4):
+        a, b = par.copy(), par.copy()
+        O.hlr_nuts(orc, m, a, [4, 3, 0, 1, 2], 0.05, 3, it)
+        O.hlr_nuts(ref, m, b, [4, 3, 0, 1, 2], 0.05, 3, it)
+        np.testing.assert_array_equal(a, b)
+        a, b = par.copy(), par.copy()
+        O.hlr_hmc(orc, m, a, [0, 1, 2, 3], 0.2, 0.04, 3, it)
+        O.hlr_hmc(ref, m, b, [0, 1, 2, 3], 0.2, 0.04, 3, it)
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("lik", ["poisson", "normal"])
+def test_glm_gradient_finite_difference(orc, lik):
+    X, y, beta = _glm_data(lik, 200, 4, 12)
+    m = O.HlrModel(X, y, has_b=True, vprior="exponential", compat=False, lik=lik, obs_var=0.5)
+    par = np.concatenate([beta * 0.5, [0.2], [0.8]])
+    idx = [5, 4, 0, 1, 2, 3]
+    g = O.hlr_grad(orc, m, par, idx)
+    h = 1e-6
+    for j, i in enumerate(idx):
+        pp, pm = par.copy(), par.copy()
+        pp[i] += h; pm[i] -= h
+        fd = (O.hlr_ll(orc, m, pp, idx) - O.hlr_ll(orc, m, pm, idx)) / (2 * h)
+        assert abs(fd - g[j]) <= 1e-5 * max(1.0, abs(g[j]))
+
+
 # ---- Gaussian mixtures ---------------------------------------------------------
 def test_mvgmm_golden_reference_example(orc):
     g = np.load(os.path.join(GOLD, "mvgmm_k3_d2.npz"))
