@@ -160,6 +160,9 @@ _SIGS = {
     "ab_gmm_table_doubles": (sz, [i32, i32]),
     "ab_gmm_prep": (i32, [i32, i32, vp, vp, vp, vp]),
     "ab_gmm_disc_z": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_z_scratch_bytes": (sz, [i32, i32, i32]),
+    "ab_gmm_z_queue_offset": (sz, [i32, i32]),
+    "ab_gmm_disc_z_screened": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, u64, u32, u32, vp, vp]),
     "ab_gmm_stats_scratch_bytes": (sz, [i32, i32]),
     "ab_gmm_stats": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
     "ab_gmm_conj_pis": (i32, [i32, vp, vp, vp, u64, u32, u32, vp]),

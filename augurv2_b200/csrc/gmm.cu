@@ -245,6 +245,279 @@ gmm_z_kernel(int N, int d, int K, int shared_cov, const float* __restrict__ Y, c
   z[n] = zk;
 }
 
+// ---- assignment draw screened in binary32 ----------------------------------
+// The same draw as gmm_z_kernel, decided for most points in binary32:
+//   gmm_zs_prep_kernel  per component (once per call): the lower triangle of
+//                       Linv_k and mu_k rounded to binary32, and the constants
+//                       of the error bound below; log(pis_k) + c - hdet_k;
+//   gmm_zs_kernel       one thread per point: t_k = log p_k in binary32 with a
+//                       rigorous bound eps_k on its error against the exact
+//                       value, p_k / p_max = exp(t_k - t_max), the running
+//                       sums, and the reference's draw when u lies outside the
+//                       sums' uncertainty band; other points go to a queue;
+//   gmm_zx_kernel       one warp per queued point: the reference's binary64
+//                       loop (gmm_z_kernel's operations, rows of Linv w on the
+//                       lanes, every sum in its order), so every draw equals
+//                       gmm_z_kernel's bit for bit.
+// Error bound (u = 2^-24; all quantities of component k; L~, w~ the binary32
+// values, w~_j = fl32(y_j - mu_j) with the difference formed in binary64):
+//   |w~_j - w_j| <= u |w~_j| (1 + 2^-28);
+//   row i of Linv w (i + 1 products, fused multiply-adds; zero padding adds
+//   exact zeros): |s~_i - s_i| <= delta_i = u (1 + 4u) (i + 3) A_i,
+//     A_i = sum_j |L~_ij||w~_j| <= R_i W (R_i >= ||L~_i||, W >= ||w~||);
+//   expon = sum_i s_i^2: |e~ - e| <= (d + 1) u e~ + sum_i (2 |s~_i| delta_i + delta_i^2),
+//     with sum_i |s~_i| a_i (a_i = (i + 3) R_i) accumulated beside the rows
+//     and sum_i delta_i^2 <= u^2 (1 + 4u)^2 W^2 S_aa, S_aa = sum_i a_i^2;
+//   t_k = fl(lpc_k - e~ / 2), lpc_k = fl32(log pis_k + c - hdet_k): |t_k - log p_k|
+//     <= eps_k = E_k / 2 + u (|lpc_k| + |t_k|) + 2^-40 (|lpc_k| + e~ + 1) (the last
+//     term covers the reference's own binary64 roundings);
+//   p~_k = exp(t_k - t_max) (binary32 exp, <= 4u); the exact p_k / p_max lies
+//     in [exp(dt - x), exp(dt + x)], x = eps_k + u |dt| + 4u, dt = t_k - t_max,
+//     so |p~_k - p_k / p_max| <= A_k, formed with directed roundings; a
+//     component far from the point has a wide band but a tiny p_k;
+//   band = sum_k A_k + (K + 6) u norm~ + 2^-40 norm~ covers the running sums'
+//     and u * norm's roundings, the comparisons' and the reference's running
+//     quotient sums.
+// A draw is decided (and equals the reference's) when u norm~ + band is below
+// the first running sum that exceeds it minus band, and the previous sum plus
+// band is below u norm~ - band.  Points whose largest log density is
+// outside [-690, 690] (where the reference's binary64 exp could underflow or
+// overflow), any non-finite value, or a call whose components have
+// c - hdet_k > 700, take the exact path.
+constexpr int GMM_ZS_MAXK = 32;
+constexpr int GMM_ZS_THREADS = 128;
+
+// Per component, floats: L~ with row i padded to whole float4s (zeros) at
+// gmm_zs_row(i), a [d], then lpc, S_aa; the stride is whole float4s.
+__host__ __device__ constexpr int gmm_zs_row(int i) { return 4 * (i / 4 + 1) * (2 * (i / 4) + i % 4); }
+__host__ __device__ inline int gmm_zs_stride(int d) { return (gmm_zs_row(d) + d + 2 + 3) / 4 * 4; }
+
+// tab: K float tables of gmm_zs_stride(d), then the means, binary64 [K][d].
+__global__ void __launch_bounds__(64) gmm_zs_prep_kernel(int d, int K, int shared_cov, const double* __restrict__ pis,
+                                                         const double* __restrict__ mu,
+                                                         const double* __restrict__ Linv,
+                                                         const double* __restrict__ hdet, float* __restrict__ tab,
+                                                         int* __restrict__ flag) {
+  __shared__ double red[1][64];
+  const int k = blockIdx.x, kc = shared_cov ? 0 : k;
+  const double* Lk = Linv + (size_t)kc * d * d;
+  const double* mk = mu + (size_t)k * d;
+  float* t = tab + (size_t)k * gmm_zs_stride(d);
+  const int T = gmm_zs_row(d);
+  float* L32 = t;
+  float* a = t + T;
+  float* sc = a + d;
+  for (int i = threadIdx.x; i < d; i += blockDim.x) {
+    double r2 = 0.0;
+    const int row = gmm_zs_row(i), len = (i / 4 + 1) * 4;
+    for (int j = 0; j < len; ++j) {
+      const float l = j <= i ? __double2float_rn(Lk[(size_t)i * d + j]) : 0.0f;
+      L32[row + j] = l;
+      r2 += (double)l * (double)l;
+    }
+    // rounded up, with a relative slack for the binary64 sums' own rounding
+    a[i] = __fmul_ru((float)(i + 3), __double2float_ru(sqrt(r2) * (1.0 + 1e-12)));
+    reinterpret_cast<double*>(tab + (size_t)K * gmm_zs_stride(d))[(size_t)k * d + i] = mk[i];
+  }
+  __syncthreads();
+  double saa = 0.0;
+  for (int i = threadIdx.x; i < d; i += blockDim.x) saa += (double)a[i] * a[i];
+  red[0][threadIdx.x] = saa;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)blockDim.x; ++i) saa += red[0][i];
+    const double c = -0.5 * (double)d * log(2.0 * 3.14159265358979323846264338327950288);
+    const double llc = c - hdet[kc];
+    const double pk = pis[k];
+    sc[0] = pk > 0.0 ? __double2float_rn(log(pk) + llc) : -INFINITY;
+    sc[1] = __double2float_ru(saa * (1.0 + 1e-12));
+    if (!(pk >= 0.0) || !(llc <= 700.0) || !isfinite(llc)) atomicExch(flag, 1);
+  }
+}
+
+template <int DT>
+__global__ void __launch_bounds__(GMM_ZS_THREADS, 5)   // 5 CTAs of 43 KB per SM
+gmm_zs_kernel(int N, int d, int K, const float* __restrict__ Y, const double* __restrict__ mu,
+              const float* __restrict__ tab,
+              const int* __restrict__ flag, int* __restrict__ queue, int* __restrict__ qn, int* __restrict__ z,
+              uint64_t seed, uint32_t iter, uint32_t comp) {
+  extern __shared__ float ts[];   // the K components' tables, then the binary64 means
+  const int stride = gmm_zs_stride(d);
+  {
+    // K * stride is whole float4s, the means 2 K d floats
+    const float4* src = reinterpret_cast<const float4*>(tab);
+    float4* dst = reinterpret_cast<float4*>(ts);
+    const int nf = K * stride + 2 * K * d, n4 = nf / 4;
+    for (int e = threadIdx.x; e < n4; e += blockDim.x) dst[e] = src[e];
+    for (int e = 4 * n4 + threadIdx.x; e < nf; e += blockDim.x) ts[e] = tab[e];
+  }
+  __syncthreads();
+  const double* mus = reinterpret_cast<const double*>(ts + (size_t)K * stride);
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= N) return;
+  const float u32 = 5.9604644775390625e-8f;   // 2^-24
+  bool exact = *flag != 0;
+  float tk[GMM_ZS_MAXK], ek[GMM_ZS_MAXK];
+  float tmax = -INFINITY;
+  if (!exact) {
+    float y[DT];
+#pragma unroll
+    for (int j = 0; j < DT; ++j) y[j] = j < d ? Y[(size_t)n * d + j] : 0.0f;
+    const int T = gmm_zs_row(d);
+    for (int k = 0; k < K; ++k) {
+      const float* L32 = ts + k * stride;
+      const float* a = L32 + T;
+      const double* mk = mus + (size_t)k * d;
+      const float* sc = a + d;
+      const float lpc = sc[0];
+      if (lpc == -INFINITY) {   // weight 0: the term is exactly 0 here and in the reference
+        tk[k] = -INFINITY;
+        ek[k] = 0.0f;
+        continue;
+      }
+      constexpr int DW = (DT + 3) / 4 * 4;   // whole float4s of row entries
+      float w[DW];
+      float W2 = 0.0f;
+#pragma unroll
+      for (int j = 0; j < DW; ++j) {
+        w[j] = (j < DT && j < d) ? __double2float_rn(__dadd_rn((double)y[j < DT ? j : 0], -mk[j])) : 0.0f;
+        W2 = __fmaf_rn(w[j], w[j], W2);
+      }
+      float e = 0.0f, t1 = 0.0f;
+#pragma unroll
+      for (int i = 0; i < DT; ++i) {
+        if (i < d) {
+          // row i in float4s; its padding is zero (exact zero products)
+          const float4* Li = reinterpret_cast<const float4*>(L32 + gmm_zs_row(i));
+          float s = 0.0f;
+#pragma unroll
+          for (int q = 0; q <= i / 4; ++q) {
+            const float4 l = Li[q];
+            s = __fmaf_rn(l.x, w[4 * q], s);
+            s = __fmaf_rn(l.y, w[4 * q + 1], s);
+            s = __fmaf_rn(l.z, w[4 * q + 2], s);
+            s = __fmaf_rn(l.w, w[4 * q + 3], s);
+          }
+          e = __fmaf_rn(s, s, e);
+          t1 = __fmaf_rn(fabsf(s), a[i], t1);
+        }
+      }
+      // W >= ||w~|| (the sum of squares' rounding and the root's covered)
+      const float W = __fsqrt_ru(__fmul_ru(W2, 1.0f + (float)(DT + 2) * u32));
+      const float sd2 = __fmul_ru(__fmul_ru(W, W), sc[1]);
+      const float E = __fmul_ru(__fadd_ru(__fadd_ru(__fmul_ru((float)(d + 1) * u32, e),
+                                                    __fmul_ru(2.0f * u32, __fmul_ru(W, t1))),
+                                          __fmul_ru(u32 * u32 * 1.01f, sd2)),
+                                1.0f + 0x1p-16f);
+      const float t = __fmaf_rn(-0.5f, e, lpc);
+      const float eps = __fadd_ru(__fadd_ru(__fmul_ru(0.5f, E), __fmul_ru(u32, fabsf(lpc) + fabsf(t))),
+                                  __fmul_ru(0x1p-40f, fabsf(lpc) + e + 1.0f));
+      tk[k] = t;
+      ek[k] = eps;
+      if (!(t < INFINITY) || !(eps < INFINITY)) exact = true;   // non-finite
+      tmax = fmaxf(tmax, t);
+    }
+    if (!(tmax >= -690.0f && tmax <= 690.0f)) exact = true;
+  }
+  int zk = -1;
+  if (!exact) {
+    // p~_k and an absolute bound A_k on |p~_k - p_k / p_max| (the exact value
+    // lies in [exp(dt - x), exp(dt + x)], x = eps_k + u |dt| + 4u, binary32
+    // exp within 4u); far components, whose bands are wide, weigh their width
+    // by their tiny size
+    float C[GMM_ZS_MAXK];
+    float acc = 0.0f, err = 0.0f;
+    for (int k = 0; k < K; ++k) {
+      float p = 0.0f;
+      if (tk[k] != -INFINITY) {
+        const float dt = __fsub_rn(tk[k], tmax);
+        p = expf(dt);
+        const float x = __fadd_ru(__fadd_ru(ek[k], __fmul_ru(u32, fabsf(dt))), 4.0f * u32);
+        const float up = __fmul_ru(expf(__fadd_ru(dt, x)), 1.0f + 8.0f * u32);
+        const float dn = __fmul_rd(expf(__fsub_rd(dt, x)), 1.0f - 8.0f * u32);
+        err = __fadd_ru(err, fmaxf(__fsub_ru(up, p), __fsub_ru(p, dn)));
+      }
+      acc = __fadd_rn(acc, p);
+      C[k] = acc;
+    }
+    // band: the terms' errors, the running sums' and u * norm's roundings,
+    // the comparisons' own roundings, the reference's running quotient sums
+    const float Nt = C[K - 1];
+    const float band = __fmul_ru(__fadd_ru(__fadd_ru(err, __fmul_ru((float)(K + 6) * u32, Nt)),
+                                           __fmul_ru(0x1p-40f, Nt)), 1.0f + 0x1p-16f);
+    Stream s = make_stream(seed, (uint32_t)n, iter, TAG_Z | (comp << 8));
+    const double u = s.uniform();
+    const float un = __fmul_rn(__double2float_rn(u), Nt);
+    int i = 0;
+    while (i < K - 1 && !(un < C[i])) ++i;
+    const bool above_prev = i == 0 || __fadd_ru(C[i - 1], band) < __fsub_rd(un, band);
+    const bool below_this = i == K - 1 || __fadd_ru(un, band) < __fsub_rd(C[i], band);
+    if (above_prev && below_this && Nt >= 1.0f && band < INFINITY) zk = i;
+  }
+  if (zk >= 0) {
+    z[n] = zk;
+  } else {
+    const int slot = atomicAdd(qn, 1);
+    queue[slot] = n;
+  }
+}
+
+// The reference's binary64 draw for the queued points, one warp per point:
+// lane i forms row i of Linv (y - mu_k) (rows i + 32 too when d > 32) with
+// gmm_z_kernel's operation order; lane 0 adds the squares in row order and
+// makes the draw.
+__global__ void __launch_bounds__(256)
+gmm_zx_kernel(int d, int K, int shared_cov, const float* __restrict__ Y, const double* __restrict__ pis,
+              const double* __restrict__ mu, const double* __restrict__ Linv, const double* __restrict__ hdet,
+              const int* __restrict__ queue, const int* __restrict__ qn, int* __restrict__ z, uint64_t seed,
+              uint32_t iter, uint32_t comp) {
+  __shared__ double wsh[8][GMM_MAX_D], ssh[8][GMM_MAX_D];
+  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  const int nq = *qn;
+  const double c = __dmul_rn(__dmul_rn(-0.5, (double)d), log(2.0 * 3.14159265358979323846264338327950288));
+  for (int q = blockIdx.x * 8 + wi; q < nq; q += gridDim.x * 8) {
+    const int n = queue[q];
+    double pmf[GMM_MAX_K];
+    for (int k = 0; k < K; ++k) {
+      const int kc = shared_cov ? 0 : k;
+      const double* Lk = Linv + (size_t)kc * d * d;
+      const double* mk = mu + (size_t)k * d;
+      for (int j = lane; j < d; j += 32) wsh[wi][j] = __dadd_rn((double)Y[(size_t)n * d + j], -mk[j]);
+      __syncwarp();
+      for (int i = lane; i < d; i += 32) {
+        double s = 0.0;
+        for (int j = 0; j <= i; ++j) s = __dadd_rn(s, __dmul_rn(Lk[(size_t)i * d + j], wsh[wi][j]));
+        ssh[wi][i] = s;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        double expon = 0.0;
+        for (int i = 0; i < d; ++i) expon = __dadd_rn(expon, __dmul_rn(ssh[wi][i], ssh[wi][i]));
+        const double ll = __dadd_rn(__dadd_rn(c, -hdet[kc]), -__dmul_rn(0.5, expon));
+        double prob = 1.0;
+        prob = __dmul_rn(prob, pis[k]);
+        prob = __dmul_rn(prob, exp(ll));
+        pmf[k] = prob;
+      }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      Stream s = make_stream(seed, (uint32_t)n, iter, TAG_Z | (comp << 8));
+      const double u = s.uniform();
+      double norm = 0.0;
+      for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, pmf[k]);
+      double acc = __ddiv_rn(pmf[0], norm);
+      int zk = K - 1;
+      for (int i = 1; i < K; ++i) {
+        if (u < acc) { zk = i - 1; break; }
+        acc = __dadd_rn(acc, __ddiv_rn(pmf[i], norm));
+      }
+      z[n] = zk;
+    }
+    __syncwarp();
+  }
+}
+
 // ---- conjugate statistics ----------------------------------------------------
 // CTA b accumulates points [b*chunk, (b+1)*chunk): counts, sum of y
 // (want_sum) and the lower triangle of sum (y - mu_z)(y - mu_z)^T
@@ -720,6 +993,51 @@ int launch_gmm_z(int N, int d, int K, int shared, const float* Y, const double* 
   return AB_OK;
 }
 
+// Scratch of the screened draw: the component tables, the exact-path flag
+// and queue length, the queue.
+static inline size_t gmm_al256(size_t x) { return (x + 255) & ~(size_t)255; }
+static inline size_t gmm_zs_smem(int d, int K) {
+  return sizeof(float) * (size_t)K * gmm_zs_stride(d) + sizeof(double) * (size_t)K * d;
+}
+size_t gmm_zs_scratch(int N, int d, int K) { return gmm_al256(gmm_zs_smem(d, K)) + 256 + gmm_al256(sizeof(int) * (size_t)N); }
+bool gmm_zs_fits(int d, int K) { return K <= GMM_ZS_MAXK && d <= 32 && gmm_zs_smem(d, K) <= 100 * 1024; }
+
+template <int DT>
+static int launch_zs_t(int N, int d, int K, const float* Y, const double* mu, const float* tab, const int* flag,
+                       int* queue, int* qn, int* z, uint64_t seed, uint32_t iter, uint32_t comp, cudaStream_t st) {
+  const size_t smem = gmm_zs_smem(d, K);
+  AB_CUDA(cudaFuncSetAttribute(gmm_zs_kernel<DT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  gmm_zs_kernel<DT><<<ceil_div(N, GMM_ZS_THREADS), GMM_ZS_THREADS, smem, st>>>(N, d, K, Y, mu, tab, flag, queue, qn,
+                                                                              z, seed, iter, comp);
+  AB_LAUNCH_CHECK("gmm_zs_kernel");
+  return AB_OK;
+}
+
+int launch_gmm_z_screened(int N, int d, int K, int shared, const float* Y, const double* pis, const double* mu,
+                          const double* Linv, const double* hdet, int* z, uint64_t seed, uint32_t iter,
+                          uint32_t comp, void* scratch, cudaStream_t st) {
+  if (!gmm_zs_fits(d, K)) return launch_gmm_z(N, d, K, shared, Y, pis, mu, Linv, hdet, z, seed, iter, comp, st);
+  char* base = static_cast<char*>(scratch);
+  float* tab = reinterpret_cast<float*>(base);
+  int* ctl = reinterpret_cast<int*>(base + gmm_al256(gmm_zs_smem(d, K)));
+  int* flag = ctl;
+  int* qn = ctl + 1;
+  int* queue = reinterpret_cast<int*>(reinterpret_cast<char*>(ctl) + 256);
+  AB_CUDA(cudaMemsetAsync(ctl, 0, 2 * sizeof(int), st));
+  gmm_zs_prep_kernel<<<K, 64, 0, st>>>(d, K, shared, pis, mu, Linv, hdet, tab, flag);
+  AB_LAUNCH_CHECK("gmm_zs_prep_kernel");
+  int rc;
+  if (d <= 2) rc = launch_zs_t<2>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
+  else if (d <= 4) rc = launch_zs_t<4>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
+  else if (d <= 8) rc = launch_zs_t<8>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
+  else if (d <= 16) rc = launch_zs_t<16>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
+  else rc = launch_zs_t<32>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
+  if (rc) return rc;
+  gmm_zx_kernel<<<296, 256, 0, st>>>(d, K, shared, Y, pis, mu, Linv, hdet, queue, qn, z, seed, iter, comp);
+  AB_LAUNCH_CHECK("gmm_zx_kernel");
+  return AB_OK;
+}
+
 int launch_gmm_prep(int Kc, int d, const double* cov, double* Linv, double* hdet, cudaStream_t st) {
   const size_t smem = sizeof(double) * 2 * (size_t)d * d;
   AB_CUDA(cudaFuncSetAttribute(gmm_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -788,6 +1106,28 @@ extern "C" int ab_gmm_prep(int Kc, int d, const double* cov, double* Linv, doubl
   AB_REQUIRE(Kc > 0 && d > 0 && d <= GMM_MAX_D, AB_ERR_ARG, "ab_gmm_prep: bad sizes");
   AB_REQUIRE(cov && Linv && hdet, AB_ERR_ARG, "ab_gmm_prep: null pointer");
   return launch_gmm_prep(Kc, d, cov, Linv, hdet, as_stream(stream));
+}
+
+extern "C" size_t ab_gmm_z_scratch_bytes(int N, int d, int K) {
+  if (N <= 0 || d <= 0 || K <= 0) return 0;
+  return gmm_zs_scratch(N, d, K);
+}
+
+extern "C" size_t ab_gmm_z_queue_offset(int d, int K) {
+  if (d <= 0 || K <= 0) return 0;
+  return gmm_al256(gmm_zs_smem(d, K)) + sizeof(int);
+}
+
+extern "C" int ab_gmm_disc_z_screened(int N, int d, int K, int shared_cov, const float* Y, const double* pis,
+                                      const double* mu, const double* Linv, const double* hdet, int* z,
+                                      uint64_t seed, uint32_t iter, uint32_t comp, void* scratch, void* stream) {
+  int rc = gmm_check(N, d, K);
+  if (rc) return rc;
+  AB_REQUIRE(Y && pis && mu && Linv && hdet && z && scratch, AB_ERR_ARG, "ab_gmm_disc_z_screened: null pointer");
+  AB_REQUIRE((reinterpret_cast<uintptr_t>(scratch) & 255) == 0, AB_ERR_ARG,
+             "ab_gmm_disc_z_screened: scratch must be 256-byte aligned");
+  return launch_gmm_z_screened(N, d, K, shared_cov, Y, pis, mu, Linv, hdet, z, seed, iter, comp, scratch,
+                               as_stream(stream));
 }
 
 extern "C" int ab_gmm_disc_z(int N, int d, int K, int shared_cov, const float* Y, const double* pis,

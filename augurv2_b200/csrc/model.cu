@@ -178,7 +178,7 @@ struct GmmModel : ab_model {
   double *mu0 = nullptr, *cov0 = nullptr, *pis = nullptr, *cov = nullptr, *alpha = nullptr, *scale0 = nullptr;
   double *mu = nullptr, *Linv = nullptr, *hdet = nullptr, *sum = nullptr, *obs = nullptr, *prop_cov = nullptr;
   double* ll_out = nullptr;
-  unsigned char *stats_scratch = nullptr, *ll_scratch = nullptr;
+  unsigned char *stats_scratch = nullptr, *ll_scratch = nullptr, *z_scratch = nullptr;
 
   int prep_components(cudaStream_t st) {
     return shared ? AB_OK : ab_gmm_prep(K, d, cov, Linv, hdet, st);
@@ -205,7 +205,7 @@ struct GmmModel : ab_model {
         if (!rc) rc = ab_gmm_conj_cov(K, d, df, scale0, cnt, obs, cov, seed, it, 0, st);
         if (!rc) rc = ab_gmm_prep(K, d, cov, Linv, hdet, st);
       }
-      if (!rc) rc = ab_gmm_disc_z(N, d, K, shared, Y, pis, mu, Linv, hdet, z, seed, it, 0, st);
+      if (!rc) rc = ab_gmm_disc_z_screened(N, d, K, shared, Y, pis, mu, Linv, hdet, z, seed, it, 0, z_scratch, st);
       if (rc) return rc;
       iteration += 1;
     }
@@ -451,6 +451,7 @@ extern "C" int ab_init_gmm(const ab_gmm_init* in, ab_model** out) {
   chk(h->alloc(&h->obs, (size_t)K * dd));
   chk(h->alloc(&h->ll_out, 1));
   chk(h->alloc(&h->stats_scratch, ab_gmm_stats_scratch_bytes(d, K)));
+  chk(h->alloc(&h->z_scratch, ab_gmm_z_scratch_bytes(N, d, K)));
   chk(h->alloc(&h->ll_scratch, ab_ll_scratch_bytes()));
   if (rc) return finish_init(h, rc, out);
   {

@@ -65,6 +65,9 @@ class GmmGibbs(Checkpointable):
         self.obs = torch.zeros((K, d, d), dtype=torch.float64, device=dev)
         self.scratch = torch.zeros(int(N.lib().ab_gmm_stats_scratch_bytes(d, K)) // 8 + 1,
                                    dtype=torch.float64, device=dev)
+        # the screened assignment draw's tables and queue (ab_gmm_disc_z_screened)
+        self.zscratch = torch.zeros(int(N.lib().ab_gmm_z_scratch_bytes(self.N, d, K)), dtype=torch.uint8,
+                                    device=dev)
         self.shrinks = torch.zeros(K, dtype=torch.int32, device=dev)
         self.accepts = torch.zeros(K, dtype=torch.int32, device=dev)
         L = N.lib()
@@ -161,9 +164,9 @@ class GmmGibbs(Checkpointable):
                 N.check(L.ab_gmm_conj_cov(K, d, self.df, N.ptr(self.scale0), N.ptr(self.cnt), N.ptr(self.obs),
                                           N.ptr(self.cov), self.seed, it, 0, st), "conj_cov")
                 N.check(L.ab_gmm_prep(K, d, N.ptr(self.cov), N.ptr(self.Linv), N.ptr(self.hdet), st), "prep")
-            N.check(L.ab_gmm_disc_z(self.N, d, K, int(self.shared), N.ptr(self.Y), N.ptr(self.pis), N.ptr(self.mu),
-                                    N.ptr(self.Linv), N.ptr(self.hdet), N.ptr(self.z), self.seed, it, 0, st),
-                    "disc_z")
+            N.check(L.ab_gmm_disc_z_screened(self.N, d, K, int(self.shared), N.ptr(self.Y), N.ptr(self.pis),
+                                             N.ptr(self.mu), N.ptr(self.Linv), N.ptr(self.hdet), N.ptr(self.z),
+                                             self.seed, it, 0, N.ptr(self.zscratch), st), "disc_z")
             self.iteration += 1
 
     def state(self):

@@ -559,27 +559,46 @@ def run_gmm(steps=10, warmup=3, cpu=True):
         b.record()
         torch.cuda.synchronize()
         ms += a.elapsed_time(b)
-    # the assignment kernel alone (its FP64 work is the sweep's bulk)
+    # the assignment draw alone: the sweep's screened launch (prep, binary32
+    # screen, binary64 path for the queued points) and the all-binary64 kernel
     L = Nn.lib()
     zs = s.z.clone()
-    zms = 0.0
-    for i in range(steps):
-        flush.fill_(i & 0xFF)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        Nn.check(L.ab_gmm_disc_z(GMM_N, d, K, 0, Nn.ptr(s.Y), Nn.ptr(s.pis), Nn.ptr(s.mu), Nn.ptr(s.Linv),
-                                 Nn.ptr(s.hdet), Nn.ptr(zs), s.seed, 10_000 + i, 0, Nn.stream_ptr()), "disc_z")
-        b.record()
-        torch.cuda.synchronize()
-        zms += a.elapsed_time(b)
-    zms /= steps
+    times = {}
+    for kind in ("screened", "binary64"):
+        tot = 0.0
+        for i in range(-1, steps):          # i = -1: untimed first launch
+            flush.fill_(i & 0xFF)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            if kind == "screened":
+                Nn.check(L.ab_gmm_disc_z_screened(GMM_N, d, K, 0, Nn.ptr(s.Y), Nn.ptr(s.pis), Nn.ptr(s.mu),
+                                                  Nn.ptr(s.Linv), Nn.ptr(s.hdet), Nn.ptr(zs), s.seed, 10_000 + i, 0,
+                                                  Nn.ptr(s.zscratch), Nn.stream_ptr()), "disc_z_screened")
+            else:
+                Nn.check(L.ab_gmm_disc_z(GMM_N, d, K, 0, Nn.ptr(s.Y), Nn.ptr(s.pis), Nn.ptr(s.mu), Nn.ptr(s.Linv),
+                                         Nn.ptr(s.hdet), Nn.ptr(zs), s.seed, 10_000 + i, 0, Nn.stream_ptr()),
+                         "disc_z")
+            b.record()
+            torch.cuda.synchronize()
+            if i >= 0:
+                tot += a.elapsed_time(b)
+        times[kind] = tot / steps
+    # points the screen left to the binary64 path in the last screened call
+    # (the queue length after the component tables)
+    qoff = int(L.ab_gmm_z_queue_offset(d, K))
     flops_pt = K * (d * d + 3 * d)     # triangular solve (d^2/2 FMAs) + centring and squares, per component
+    zms = times["screened"]
     ach = GMM_N * flops_pt / (zms / 1e3) / 1e12
+    fp32_peak = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal B200 FP32 FMA rate at the measured SM clock
     line = {"metric": "GMM Gibbs points/sec (hmvgmm, K=16 d=32)", "value": GMM_N * steps / (ms / 1e3),
             "unit": "points/s", "ms_per_sweep": ms / steps, "steps": steps, "warmup": warmup,
-            "roofline": {"bound": "fp64", "kernel": "gmm_z_kernel", "achieved": ach, "peak": 37.0,
-                         "unit": "TFLOP/s", "frac": ach / 37.0, "peak_source": "nominal (no measured FP64 peak)",
-                         "launch_ms": zms, "algorithmic_flops_per_point": flops_pt},
+            "roofline": {"bound": "fp32", "kernel": "gmm_zs_kernel (binary32-screened assignment draw)",
+                         "achieved": ach, "peak": fp32_peak, "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                         "peak_source": "nominal (148 SMs x 128 FP32 FMA per clock at 1965 MHz; no measured "
+                                        "FP32 peak)",
+                         "launch_ms": zms, "binary64_kernel_ms": times["binary64"],
+                         "points_to_binary64_path": int(s.zscratch[qoff:qoff + 4].view(torch.int32).item()),
+                         "algorithmic_flops_per_point": flops_pt},
             "config": {"workload": "gmm_hmvgmm_n200000_k16_d32", "N": GMM_N, "K": K, "d": d,
                        "y_dtype": "f32", "l2": "flushed between timed sweeps"}}
     if cpu:

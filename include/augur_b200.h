@@ -249,6 +249,25 @@ int ab_gmm_disc_z(int N, int d, int K, int shared_cov, const float* Y, const dou
                   const double* Linv, const double* hdet, int* z, uint64_t seed, uint32_t iter, uint32_t comp,
                   void* stream);
 
+/* The same draw decided for most points in binary32: log p_k per point and
+ * component with a rigorous bound on its error (the binary32 rounding of
+ * Linv, mu and y - mu, of every product and sum, and the reference's own
+ * binary64 roundings), the running sums of p_k / p_max, and the reference's
+ * draw wherever the uniform lies outside their uncertainty band; the other
+ * points (a few in 10^4), and every point of a call with extreme
+ * log-densities, run the reference's binary64 loop.  Equal to
+ * ab_gmm_disc_z bit for bit.  scratch: ab_gmm_z_scratch_bytes(N, d, K)
+ * bytes, 256-byte aligned (component tables and the queue of points the
+ * screen leaves).  Shapes outside K <= 32, d <= 32 run ab_gmm_disc_z's
+ * kernel. */
+size_t ab_gmm_z_scratch_bytes(int N, int d, int K);
+/* Byte offset in that scratch of an int: how many points of the last call
+ * took the binary64 path (when the screen ran). */
+size_t ab_gmm_z_queue_offset(int d, int K);
+int ab_gmm_disc_z_screened(int N, int d, int K, int shared_cov, const float* Y, const double* pis,
+                           const double* mu, const double* Linv, const double* hdet, int* z, uint64_t seed,
+                           uint32_t iter, uint32_t comp, void* scratch, void* stream);
+
 /* Conjugate statistics of z (CgConj.hs:186-246): counts cnt int32 [K] always;
  * sum f64 [K][d] of y if `sum` is non-NULL; obs f64 [K][d][d] =
  * sum (y - mu[z])(y - mu[z])^T if `obs` is non-NULL (needs mu).  scratch:
