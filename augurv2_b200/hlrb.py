@@ -998,17 +998,39 @@ class NutsGroup:
             s.reset_history()
         self._set_active([True] * len(self.samplers))
 
+    def _rounds_to_first_finish(self, d, ran, min_draws):
+        """Rounds until the first active instance is expected to reach its
+        draw target, from the draws per round its slowest chain made so far
+        in this call (at least 1; None before any instance has drawn)."""
+        best = None
+        for i, a in enumerate(self.active):
+            r = ran(i)
+            if not a or r <= 0 or d[i] <= 0:
+                continue
+            target = min(min_draws, self.samplers[i].hist_cap)
+            est = -(-(target - int(d[i])) * r // int(d[i]))      # ceil
+            best = est if best is None else min(best, est)
+        return None if best is None else max(1, best)
+
     @traced("nuts_group.run")
     def run(self, min_draws, max_rounds, block=25):
         """Rounds until every instance has min_draws draws per chain; returns
-        the rounds each instance ran in this call."""
+        the rounds each instance ran in this call.  The draw counts are read
+        back every `block` rounds, or sooner when an instance is expected to
+        reach its target earlier (so that a large instance does not run up to
+        `block` rounds past its target; each read-back is one host round trip)."""
         start = list(self.rounds)
         ran = lambda i: self.rounds[i] - start[i]
         if self.graph is None:
             self.capture()
         self._set_active([True] * len(self.samplers))
+        d = None
         while any(self.active):
             reps = min(block, min(max_rounds - ran(i) for i, a in enumerate(self.active) if a))
+            if d is not None:
+                est = self._rounds_to_first_finish(d, ran, min_draws)
+                if est is not None:
+                    reps = min(reps, est)
             if reps > 0:
                 self.step(reps)
             d = self.min_draws()
