@@ -255,10 +255,10 @@ gmm_z_kernel(int N, int d, int K, int shared_cov, const float* __restrict__ Y, c
 //                       value, p_k / p_max = exp(t_k - t_max), the running
 //                       sums, and the reference's draw when u lies outside the
 //                       sums' uncertainty band; other points go to a queue;
-//   gmm_zx_kernel       one warp per queued point: the reference's binary64
-//                       loop (gmm_z_kernel's operations, rows of Linv w on the
-//                       lanes, every sum in its order), so every draw equals
-//                       gmm_z_kernel's bit for bit.
+//   gmm_zx_kernel       one CTA per queued point, a warp per component: the
+//                       reference's binary64 loop (gmm_z_kernel's operations,
+//                       rows of Linv w on the lanes, every sum in its order),
+//                       so every draw equals gmm_z_kernel's bit for bit.
 // Error bound (u = 2^-24; all quantities of component k; L~, w~ the binary32
 // values, w~_j = fl32(y_j - mu_j) with the difference formed in binary64):
 //   |w~_j - w_j| <= u |w~_j| (1 + 2^-28);
@@ -462,50 +462,50 @@ gmm_zs_kernel(int N, int d, int K, const float* __restrict__ Y, const double* __
   }
 }
 
-// The reference's binary64 draw for the queued points, one warp per point:
-// lane i forms row i of Linv (y - mu_k) (rows i + 32 too when d > 32) with
-// gmm_z_kernel's operation order; lane 0 adds the squares in row order and
-// makes the draw.
-__global__ void __launch_bounds__(256)
+// The reference's binary64 draw for the queued points, one CTA of K warps
+// per point (K <= 32, d <= 32): warp k takes component k, lane i forms row
+// i of Linv (y - mu_k) with gmm_z_kernel's operation order and lane 0 adds
+// the squares in row order, all components side by side; thread 0 then
+// makes the draw from the K densities.  CTAs take queued points in turn.
+__global__ void __launch_bounds__(GMM_ZS_MAXK * 32)
 gmm_zx_kernel(int d, int K, int shared_cov, const float* __restrict__ Y, const double* __restrict__ pis,
               const double* __restrict__ mu, const double* __restrict__ Linv, const double* __restrict__ hdet,
               const int* __restrict__ queue, const int* __restrict__ qn, int* __restrict__ z, uint64_t seed,
               uint32_t iter, uint32_t comp) {
-  __shared__ double wsh[8][GMM_MAX_D], ssh[8][GMM_MAX_D];
-  const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+  __shared__ double wsh[GMM_ZS_MAXK][32], ssh[GMM_ZS_MAXK][32], pmf[GMM_ZS_MAXK];
+  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
   const int nq = *qn;
   const double c = __dmul_rn(__dmul_rn(-0.5, (double)d), log(2.0 * 3.14159265358979323846264338327950288));
-  for (int q = blockIdx.x * 8 + wi; q < nq; q += gridDim.x * 8) {
+  const int kc = shared_cov ? 0 : k;
+  const double* Lk = Linv + (size_t)kc * d * d;
+  const double* mk = mu + (size_t)k * d;
+  for (int q = blockIdx.x; q < nq; q += gridDim.x) {
     const int n = queue[q];
-    double pmf[GMM_MAX_K];
-    for (int k = 0; k < K; ++k) {
-      const int kc = shared_cov ? 0 : k;
-      const double* Lk = Linv + (size_t)kc * d * d;
-      const double* mk = mu + (size_t)k * d;
-      for (int j = lane; j < d; j += 32) wsh[wi][j] = __dadd_rn((double)Y[(size_t)n * d + j], -mk[j]);
-      __syncwarp();
-      for (int i = lane; i < d; i += 32) {
-        double s = 0.0;
-        for (int j = 0; j <= i; ++j) s = __dadd_rn(s, __dmul_rn(Lk[(size_t)i * d + j], wsh[wi][j]));
-        ssh[wi][i] = s;
-      }
-      __syncwarp();
-      if (lane == 0) {
-        double expon = 0.0;
-        for (int i = 0; i < d; ++i) expon = __dadd_rn(expon, __dmul_rn(ssh[wi][i], ssh[wi][i]));
-        const double ll = __dadd_rn(__dadd_rn(c, -hdet[kc]), -__dmul_rn(0.5, expon));
-        double prob = 1.0;
-        prob = __dmul_rn(prob, pis[k]);
-        prob = __dmul_rn(prob, exp(ll));
-        pmf[k] = prob;
-      }
-      __syncwarp();
+    if (lane < d) wsh[k][lane] = __dadd_rn((double)Y[(size_t)n * d + lane], -mk[lane]);
+    __syncwarp();
+    if (lane < d) {
+      const double* Li = Lk + (size_t)lane * d;
+      double s = 0.0;
+#pragma unroll 4
+      for (int jj = 0; jj <= lane; ++jj) s = __dadd_rn(s, __dmul_rn(Li[jj], wsh[k][jj]));
+      ssh[k][lane] = s;
     }
+    __syncwarp();
     if (lane == 0) {
-      Stream s = make_stream(seed, (uint32_t)n, iter, TAG_Z | (comp << 8));
-      const double u = s.uniform();
+      double expon = 0.0;
+      for (int i = 0; i < d; ++i) expon = __dadd_rn(expon, __dmul_rn(ssh[k][i], ssh[k][i]));
+      const double ll = __dadd_rn(__dadd_rn(c, -hdet[kc]), -__dmul_rn(0.5, expon));
+      double prob = 1.0;
+      prob = __dmul_rn(prob, pis[k]);
+      prob = __dmul_rn(prob, exp(ll));
+      pmf[k] = prob;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Stream st = make_stream(seed, (uint32_t)n, iter, TAG_Z | (comp << 8));
+      const double u = st.uniform();
       double norm = 0.0;
-      for (int k = 0; k < K; ++k) norm = __dadd_rn(norm, pmf[k]);
+      for (int i = 0; i < K; ++i) norm = __dadd_rn(norm, pmf[i]);
       double acc = __ddiv_rn(pmf[0], norm);
       int zk = K - 1;
       for (int i = 1; i < K; ++i) {
@@ -514,7 +514,7 @@ gmm_zx_kernel(int d, int K, int shared_cov, const float* __restrict__ Y, const d
       }
       z[n] = zk;
     }
-    __syncwarp();
+    __syncthreads();
   }
 }
 
@@ -523,32 +523,44 @@ gmm_zx_kernel(int d, int K, int shared_cov, const float* __restrict__ Y, const d
 // (want_sum) and the lower triangle of sum (y - mu_z)(y - mu_z)^T
 // (want_obs; the reference's full-matrix update augur_mat_atm_inc_vtmt is
 // symmetric elementwise).  The chunk is taken in sub-chunks of at most
-// `sub` points: a sub-chunk's rows of Y are copied to shared memory with
-// coalesced loads (all in flight at once), sorted by component with a
-// stable counting sort (warp 0, match_any ranks), and the components are
-// walked one at a time: each thread owns fixed table entries and
-// accumulates them in registers over the component's points in point order,
-// adding the sub-chunk's sum to its partial.  Partials go to scratch
-// [CTA][K][W] and gmm_stats_reduce_kernel adds them in CTA order
-// (deterministic; the reference adds in point order).
-constexpr int GMM_STAT_MAXE = 4;       // table entries per thread (W <= 4 * GMM_THREADS)
+// `sub` points: a sub-chunk's rows of Y are read with coalesced loads (all
+// in flight at once) into shared memory, as binary32 rows when the sums are
+// wanted and, for the scatter, centred once per point in binary64
+// (c_i = y_i - mu_z,i, the value every scatter entry of the point uses);
+// the points are sorted by component with a stable counting sort (warp 0,
+// match_any ranks), and the components are walked one at a time: each
+// thread owns fixed table entries and accumulates them in registers over
+// the component's points in point order (a count is the component's number
+// of points, the same double as adding 1.0 per point), adding the
+// sub-chunk's sum to its partial.  Partials go to scratch [CTA][K][W] and
+// gmm_stats_reduce_kernel adds them in CTA order (deterministic; the
+// reference adds in point order).
+constexpr int GMM_STAT_THREADS = 512;  // at d = 32 no thread owns more than two of the 529 scatter entries
+constexpr int GMM_STAT_MAXE = 4;       // table entries per thread (W <= 4 * GMM_STAT_THREADS)
 constexpr int GMM_STAT_SMEM = 96 * 1024;
 
-__host__ __device__ inline int gmm_stat_sub(int d, int chunk) {
-  const int fit = GMM_STAT_SMEM / (4 * d + 8);
+// bytes of shared memory per point of a sub-chunk: label and rank, the
+// binary32 row (sums), the centred binary64 row (scatter)
+__host__ __device__ inline int gmm_stat_point_bytes(int d, int want_sum, int want_obs) {
+  return 8 + (want_sum ? 4 * d : 0) + (want_obs ? 8 * d : 0);
+}
+
+__host__ __device__ inline int gmm_stat_sub(int d, int chunk, int want_sum, int want_obs) {
+  const int fit = GMM_STAT_SMEM / gmm_stat_point_bytes(d, want_sum, want_obs);
   return chunk < fit ? chunk : fit;
 }
 
-__global__ void __launch_bounds__(GMM_THREADS)
+__global__ void __launch_bounds__(GMM_STAT_THREADS)
 gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __restrict__ z,
                  const double* __restrict__ mu, int want_sum, int want_obs, int chunk,
                  double* __restrict__ part) {
-  extern __shared__ int sidx[];          // zs [sub], perm [sub], ys [sub][d] (float)
+  extern __shared__ double sdbl[];       // cs [sub][d] (double), then zs [sub], perm [sub], ys [sub][d] (float)
   __shared__ int koff[GMM_MAX_K + 1];
-  const int sub = gmm_stat_sub(d, chunk);
-  int* zs = sidx;
-  int* perm = sidx + sub;
-  float* ys = reinterpret_cast<float*>(sidx + 2 * sub);
+  const int sub = gmm_stat_sub(d, chunk, want_sum, want_obs);
+  double* cs = sdbl;
+  int* zs = reinterpret_cast<int*>(cs + (want_obs ? (size_t)sub * d : 0));
+  int* perm = zs + sub;
+  float* ys = reinterpret_cast<float*>(perm + sub);
   const int T = d * (d + 1) / 2;
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
   const int tid = threadIdx.x, lane = tid & 31;
@@ -572,8 +584,17 @@ gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __
       const int k = z[base + p];
       zs[p] = (k >= 0 && k < K) ? k : -1;    // a label outside [0, K) is not counted
     }
-    for (int e = tid; e < m * d; e += blockDim.x) ys[e] = Y[(size_t)base * d + e];
+    if (want_sum)
+      for (int e = tid; e < m * d; e += blockDim.x) ys[e] = Y[(size_t)base * d + e];
     __syncthreads();
+    if (want_obs) {
+      // the centred rows, one binary64 subtraction per coordinate
+      for (int e = tid; e < m * d; e += blockDim.x) {
+        const int p = e / d, i = e - p * d;
+        const int k = zs[p];
+        cs[e] = k >= 0 ? __dadd_rn((double)Y[(size_t)base * d + e], -mu[(size_t)k * d + i]) : 0.0;
+      }
+    }
     if (tid < 32) {
       // stable counting sort of the sub-chunk by component
       for (int k = lane; k <= K; k += 32) koff[k] = 0;
@@ -605,36 +626,26 @@ gmm_stats_kernel(int N, int d, int K, const float* __restrict__ Y, const int* __
     }
     __syncthreads();
     for (int k = 0; k < K; ++k) {
-      double acc[GMM_STAT_MAXE], mi[GMM_STAT_MAXE], mj[GMM_STAT_MAXE];
+      const int p0 = koff[k], p1 = koff[k + 1];
 #pragma unroll
       for (int q = 0; q < GMM_STAT_MAXE; ++q) {
-        acc[q] = 0.0;
-        mi[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ei[q]] : 0.0;
-        mj[q] = (q < ne && ekind[q] == 2) ? mu[(size_t)k * d + ej[q]] : 0.0;
-      }
-      for (int p = koff[k]; p < koff[k + 1]; ++p) {
-        const float* y = ys + perm[p] * d;
-#pragma unroll
-        for (int q = 0; q < GMM_STAT_MAXE; ++q) {
-          if (q < ne) {
-            if (ekind[q] == 0) {
-              acc[q] = __dadd_rn(acc[q], 1.0);
-            } else if (ekind[q] == 1) {
-              acc[q] = __dadd_rn(acc[q], (double)y[ei[q]]);
-            } else {
-              const double di = __dadd_rn((double)y[ei[q]], -mi[q]);
-              const double dj = __dadd_rn((double)y[ej[q]], -mj[q]);
-              acc[q] = __dadd_rn(acc[q], __dmul_rn(di, dj));
-            }
+        if (q >= ne) continue;
+        double acc = 0.0;
+        if (ekind[q] == 0) {
+          acc = (double)(p1 - p0);                 // exactly the sum of p1 - p0 ones
+        } else if (ekind[q] == 1) {
+          const int i = ei[q];
+          for (int p = p0; p < p1; ++p) acc = __dadd_rn(acc, (double)ys[perm[p] * d + i]);
+        } else {
+          const int i = ei[q], j = ej[q];
+#pragma unroll 4
+          for (int p = p0; p < p1; ++p) {
+            const double* c = cs + perm[p] * d;
+            acc = __dadd_rn(acc, __dmul_rn(c[i], c[j]));
           }
         }
-      }
-#pragma unroll
-      for (int q = 0; q < GMM_STAT_MAXE; ++q) {
-        if (q < ne) {
-          double* dst = part + ((size_t)blockIdx.x * K + k) * W + tid + q * blockDim.x;
-          *dst = base == n0 ? acc[q] : __dadd_rn(*dst, acc[q]);
-        }
+        double* dst = part + ((size_t)blockIdx.x * K + k) * W + tid + q * blockDim.x;
+        *dst = base == n0 ? acc : __dadd_rn(*dst, acc);
       }
     }
     __syncthreads();                             // the next sub-chunk reuses shared memory
@@ -1033,7 +1044,7 @@ int launch_gmm_z_screened(int N, int d, int K, int shared, const float* Y, const
   else if (d <= 16) rc = launch_zs_t<16>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
   else rc = launch_zs_t<32>(N, d, K, Y, mu, tab, flag, queue, qn, z, seed, iter, comp, st);
   if (rc) return rc;
-  gmm_zx_kernel<<<296, 256, 0, st>>>(d, K, shared, Y, pis, mu, Linv, hdet, queue, qn, z, seed, iter, comp);
+  gmm_zx_kernel<<<592, 32 * K, 0, st>>>(d, K, shared, Y, pis, mu, Linv, hdet, queue, qn, z, seed, iter, comp);
   AB_LAUNCH_CHECK("gmm_zx_kernel");
   return AB_OK;
 }
@@ -1055,13 +1066,13 @@ int launch_gmm_stats(int N, int d, int K, const float* Y, const int* z, const do
                      int want_obs, int* cnt, double* sum, double* obs, double* part, cudaStream_t st) {
   const int T = d * (d + 1) / 2;
   const int W = 1 + (want_sum ? d : 0) + (want_obs ? T : 0);
-  AB_REQUIRE(W <= GMM_STAT_MAXE * GMM_THREADS, AB_ERR_ARG, "gmm: d too large for the statistics pass");
+  AB_REQUIRE(W <= GMM_STAT_MAXE * GMM_STAT_THREADS, AB_ERR_ARG, "gmm: d too large for the statistics pass");
   const int chunk = (N + GMM_STAT_CTAS - 1) / GMM_STAT_CTAS;
   const int nparts = (N + chunk - 1) / chunk;
-  const int sub = gmm_stat_sub(d, chunk);
-  const size_t smem = (sizeof(int) * 2 + sizeof(float) * (size_t)d) * (size_t)sub;
+  const int sub = gmm_stat_sub(d, chunk, want_sum, want_obs);
+  const size_t smem = (size_t)gmm_stat_point_bytes(d, want_sum, want_obs) * (size_t)sub;
   AB_CUDA(cudaFuncSetAttribute(gmm_stats_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  gmm_stats_kernel<<<nparts, GMM_THREADS, smem, st>>>(N, d, K, Y, z, mu, want_sum, want_obs, chunk, part);
+  gmm_stats_kernel<<<nparts, GMM_STAT_THREADS, smem, st>>>(N, d, K, Y, z, mu, want_sum, want_obs, chunk, part);
   AB_LAUNCH_CHECK("gmm_stats_kernel");
   gmm_stats_reduce_kernel<<<ceil_div((size_t)K * W, 256), 256, 0, st>>>(d, K, want_sum, want_obs, nparts, part,
                                                                         cnt, sum, obs);
