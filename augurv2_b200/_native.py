@@ -168,6 +168,8 @@ _SIGS = {
     "ab_gmm_conj_pis": (i32, [i32, vp, vp, vp, u64, u32, u32, vp]),
     "ab_gmm_conj_mu": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, vp, u64, u32, u32, vp]),
     "ab_gmm_conj_cov": (i32, [i32, i32, i32, vp, vp, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_bartlett": (i32, [i32, i32, i32, vp, vp, u64, u32, u32, vp]),
+    "ab_gmm_conj_cov_chi": (i32, [i32, i32, i32, vp, vp, vp, vp, vp, u64, u32, u32, vp]),
     "ab_gmm_eslice": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, vp, u64, u32, u32, vp, vp]),
     "ab_gmm_mwg": (i32, [i32, i32, i32, i32, vp, vp, vp, vp, vp, vp, i32, i32, i32, vp, u64, u32, u32, vp, vp]),
     # whole-model log densities, predictive log-likelihoods, dethlr's bias

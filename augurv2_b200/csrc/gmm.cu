@@ -27,7 +27,8 @@ constexpr int GMM_MAX_K = 64;
 constexpr int GMM_THREADS = 256;
 constexpr int GMM_STAT_CTAS = 296;
 
-#define GM(A, i, j) (A)[(size_t)(i) * d + (j)]
+// d <= GMM_MAX_D, so a shared-memory matrix index fits 32 bits
+#define GM(A, i, j) (A)[(i) * d + (j)]
 
 // ---- warp-level matrix routines (one full warp, matrices in shared memory)
 
@@ -38,14 +39,17 @@ __device__ void w_chol(double* A, int d) {
   for (int j = 0; j < d; ++j) {
     if (lane == 0) {
       double s = 0.0;
+#pragma unroll 4
       for (int k = 0; k < j; ++k) s = __dadd_rn(s, __dmul_rn(GM(A, j, k), GM(A, j, k)));
       GM(A, j, j) = __dsqrt_rn(__dadd_rn(GM(A, j, j), -s));
     }
     __syncwarp();
+    const double rjj = __ddiv_rn(1.0, GM(A, j, j));   // the reference's 1 / A[j][j], once per column
     for (int i = j + 1 + lane; i < d; i += 32) {
       double s = 0.0;
+#pragma unroll 4
       for (int k = 0; k < j; ++k) s = __dadd_rn(s, __dmul_rn(GM(A, i, k), GM(A, j, k)));
-      GM(A, i, j) = __dmul_rn(__ddiv_rn(1.0, GM(A, j, j)), __dadd_rn(GM(A, i, j), -s));
+      GM(A, i, j) = __dmul_rn(rjj, __dadd_rn(GM(A, i, j), -s));
     }
     __syncwarp();
   }
@@ -64,6 +68,7 @@ __device__ void w_trmi(double* L, double* T, int d) {
   for (int c = lane; c < d; c += 32) {
     for (int m = c; m < d; ++m) {
       double b = (c == m) ? 1.0 : 0.0;
+#pragma unroll 4
       for (int i = c; i < m; ++i) b = __dadd_rn(b, -__dmul_rn(GM(T, m, i), GM(L, i, c)));
       GM(L, m, c) = __ddiv_rn(b, GM(T, m, m));
     }
@@ -89,6 +94,7 @@ __device__ void w_cholinv(double* A, double* T, int d) {
   for (int c = lane; c < d; c += 32) {
     for (int r = c; r < d; ++r) {
       double acc = 0.0;
+#pragma unroll 4
       for (int k = c; k < d; ++k) {
         const double akc = (k < r) ? GM(A, k, c) : GM(T, k, c);
         acc = __dadd_rn(acc, __dmul_rn(GM(T, k, r), akc));
@@ -109,6 +115,7 @@ __device__ void w_trvm(const double* L, double* v, double* tmp, int d) {
   const int lane = threadIdx.x & 31;
   for (int i = lane; i < d; i += 32) {
     double s = 0.0;
+#pragma unroll 4
     for (int j = 0; j <= i; ++j) s = __dadd_rn(s, __dmul_rn(GM(L, i, j), v[j]));
     tmp[i] = s;
   }
@@ -122,6 +129,7 @@ __device__ void w_mvm(double* dst, const double* A, const double* v, int d) {
   const int lane = threadIdx.x & 31;
   for (int i = lane; i < d; i += 32) {
     double s = 0.0;
+#pragma unroll 4
     for (int j = 0; j < d; ++j) s = __dadd_rn(s, __dmul_rn(GM(A, i, j), v[j]));
     dst[i] = s;
   }
@@ -135,6 +143,7 @@ __device__ void w_trtrmm(const double* L1, double* L2, double* tmp, int d) {
   for (int e = lane; e < d * d; e += 32) {
     const int i = e / d, j = e - i * d;
     double s = 0.0;
+#pragma unroll 4
     for (int k = 0; k < i; ++k) s = __dadd_rn(s, __dmul_rn(GM(L1, i, k), GM(L2, k, j)));
     s = __dadd_rn(s, __dmul_rn(GM(L1, i, i), GM(L2, i, j)));
     tmp[e] = s;
@@ -763,12 +772,14 @@ gmm_conj_mu_kernel(int d, int shared_cov, const double* __restrict__ mu0, const 
 // i*n + i + t, t < n - i (n = cnt[k] + df), substream (k, iter, 9|comp<<8).
 // One CTA per (k, i): thread-strided partial sums, then the fixed-order
 // block sum.  That is O(d * cnt[k]) normals per component per sweep (the
-// reference's algorithm), spread over K * d CTAs.  The sums are staged on
-// the diagonal of cov[k], which gmm_conj_cov_kernel then reads and
-// overwrites with the draw.
+// reference's algorithm), spread over K * d CTAs.  Row i's sum of component
+// k goes to chi[k * sk + i * si]: the diagonal of cov[k] (sk = d * d,
+// si = d + 1), which gmm_conj_cov_kernel then reads and overwrites with the
+// draw, or a [K][d] table of its own (sk = d, si = 1) when the draw runs
+// beside the steps that still read cov.
 __global__ void __launch_bounds__(GMM_THREADS)
-gmm_bartlett_chi_kernel(int d, int df, const int* __restrict__ cnt, double* __restrict__ cov, uint64_t seed,
-                        uint32_t iter, uint32_t comp) {
+gmm_bartlett_chi_kernel(int d, int df, const int* __restrict__ cnt, double* __restrict__ chi, int sk, int si,
+                        uint64_t seed, uint32_t iter, uint32_t comp) {
   __shared__ double red[34];
   const int k = blockIdx.x / d, i = blockIdx.x - k * d;
   const int n = cnt[k] + df;
@@ -780,8 +791,8 @@ gmm_bartlett_chi_kernel(int d, int df, const int* __restrict__ cnt, double* __re
     const double zz = s.normal();
     local = __dadd_rn(local, __dmul_rn(zz, zz));
   }
-  const double chi = block_sum_f64(local, red);
-  if (threadIdx.x == 0) cov[(size_t)k * d * d + (size_t)i * d + i] = chi;
+  const double sum = block_sum_f64(local, red);
+  if (threadIdx.x == 0) chi[(size_t)k * sk + (size_t)i * si] = sum;
 }
 
 // augur_invwishart_mvnormal_conj (augur_dist.c:751-757) and
@@ -791,13 +802,13 @@ gmm_bartlett_chi_kernel(int d, int df, const int* __restrict__ cnt, double* __re
 // consumes them (row-major over the lower triangle; each diagonal
 // chi-square of n - i normals follows its row's off-diagonal normals).  The
 // chi-square sums of up to cnt + df squares come from
-// gmm_bartlett_chi_kernel (on cov's diagonal), added in a fixed tree order
+// gmm_bartlett_chi_kernel (chi[k * sk + i * si]), added in a fixed tree order
 // instead of sequentially (a rounding-level difference); the d x d algebra
 // runs on warp 0.
 __global__ void __launch_bounds__(GMM_THREADS)
 gmm_conj_cov_kernel(int d, int df, const double* __restrict__ scale0, const int* __restrict__ cnt,
-                    const double* __restrict__ obs, double* __restrict__ cov, uint64_t seed, uint32_t iter,
-                    uint32_t comp) {
+                    const double* __restrict__ obs, const double* chi, int sk, int si, double* cov, uint64_t seed,
+                    uint32_t iter, uint32_t comp) {
   extern __shared__ double sm[];
   const int k = blockIdx.x, tid = threadIdx.x;
   const int dd = d * d;
@@ -828,7 +839,7 @@ gmm_conj_cov_kernel(int d, int df, const double* __restrict__ scale0, const int*
     } else if (j > i) {
       A[e] = 0.0;
     } else {
-      A[e] = __dsqrt_rn(cov[(size_t)k * dd + e]);
+      A[e] = __dsqrt_rn(chi[(size_t)k * sk + (size_t)i * si]);
     }
   }
   __syncthreads();
@@ -1090,15 +1101,38 @@ int launch_gmm_conj_mu(int K, int d, int shared, const double* mu0, const double
   return AB_OK;
 }
 
-int launch_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
-                        double* cov, uint64_t seed, uint32_t iter, uint32_t comp, cudaStream_t st) {
-  gmm_bartlett_chi_kernel<<<K * d, GMM_THREADS, 0, st>>>(d, df, cnt, cov, seed, iter, comp);
+// The Bartlett chi-square sums into chi (chi == nullptr: cov's diagonal).
+int launch_gmm_bartlett(int K, int d, int df, const int* cnt, double* chi, double* cov, uint64_t seed,
+                        uint32_t iter, uint32_t comp, cudaStream_t st) {
+  if (chi != nullptr)
+    gmm_bartlett_chi_kernel<<<K * d, GMM_THREADS, 0, st>>>(d, df, cnt, chi, d, 1, seed, iter, comp);
+  else
+    gmm_bartlett_chi_kernel<<<K * d, GMM_THREADS, 0, st>>>(d, df, cnt, cov, d * d, d + 1, seed, iter, comp);
   AB_LAUNCH_CHECK("gmm_bartlett_chi_kernel");
+  return AB_OK;
+}
+
+// The inverse-Wishart draw from the chi-square sums in chi (chi == nullptr:
+// cov's diagonal).
+int launch_gmm_conj_cov_from(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
+                             const double* chi, double* cov, uint64_t seed, uint32_t iter, uint32_t comp,
+                             cudaStream_t st) {
   const size_t smem = sizeof(double) * 4 * (size_t)d * d;
   AB_CUDA(cudaFuncSetAttribute(gmm_conj_cov_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  gmm_conj_cov_kernel<<<K, GMM_THREADS, smem, st>>>(d, df, scale0, cnt, obs, cov, seed, iter, comp);
+  if (chi != nullptr)
+    gmm_conj_cov_kernel<<<K, GMM_THREADS, smem, st>>>(d, df, scale0, cnt, obs, chi, d, 1, cov, seed, iter, comp);
+  else
+    gmm_conj_cov_kernel<<<K, GMM_THREADS, smem, st>>>(d, df, scale0, cnt, obs, cov, d * d, d + 1, cov, seed, iter,
+                                                      comp);
   AB_LAUNCH_CHECK("gmm_conj_cov_kernel");
   return AB_OK;
+}
+
+int launch_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
+                        double* cov, uint64_t seed, uint32_t iter, uint32_t comp, cudaStream_t st) {
+  int rc = launch_gmm_bartlett(K, d, df, cnt, nullptr, cov, seed, iter, comp, st);
+  if (rc) return rc;
+  return launch_gmm_conj_cov_from(K, d, df, scale0, cnt, obs, nullptr, cov, seed, iter, comp, st);
 }
 
 size_t gmm_move_smem(int d) {
@@ -1185,6 +1219,23 @@ extern "C" int ab_gmm_conj_cov(int K, int d, int df, const double* scale0, const
   AB_REQUIRE(df > 0 && df < 100000, AB_ERR_ARG, "ab_gmm_conj_cov: bad degrees of freedom");
   AB_REQUIRE(scale0 && cnt && obs && cov, AB_ERR_ARG, "ab_gmm_conj_cov: null pointer");
   return launch_gmm_conj_cov(K, d, df, scale0, cnt, obs, cov, seed, iter, comp, as_stream(stream));
+}
+
+extern "C" int ab_gmm_bartlett(int K, int d, int df, const int* cnt, double* chi, uint64_t seed, uint32_t iter,
+                               uint32_t comp, void* stream) {
+  AB_REQUIRE(K > 0 && K <= GMM_MAX_K && d > 0 && d <= GMM_MAX_D, AB_ERR_ARG, "ab_gmm_bartlett: bad sizes");
+  AB_REQUIRE(df > 0 && df < 100000, AB_ERR_ARG, "ab_gmm_bartlett: bad degrees of freedom");
+  AB_REQUIRE(cnt && chi, AB_ERR_ARG, "ab_gmm_bartlett: null pointer");
+  return launch_gmm_bartlett(K, d, df, cnt, chi, nullptr, seed, iter, comp, as_stream(stream));
+}
+
+extern "C" int ab_gmm_conj_cov_chi(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
+                                   const double* chi, double* cov, uint64_t seed, uint32_t iter, uint32_t comp,
+                                   void* stream) {
+  AB_REQUIRE(K > 0 && K <= GMM_MAX_K && d > 0 && d <= GMM_MAX_D, AB_ERR_ARG, "ab_gmm_conj_cov_chi: bad sizes");
+  AB_REQUIRE(df > 0 && df < 100000, AB_ERR_ARG, "ab_gmm_conj_cov_chi: bad degrees of freedom");
+  AB_REQUIRE(scale0 && cnt && obs && chi && cov, AB_ERR_ARG, "ab_gmm_conj_cov_chi: null pointer");
+  return launch_gmm_conj_cov_from(K, d, df, scale0, cnt, obs, chi, cov, seed, iter, comp, as_stream(stream));
 }
 
 extern "C" int ab_gmm_eslice(int N, int d, int K, int shared_cov, const float* Y, const int* z, const double* mu0,

@@ -63,6 +63,8 @@ class GmmGibbs(Checkpointable):
         self.cnt = torch.zeros(K, dtype=torch.int32, device=dev)
         self.sum = torch.zeros((K, d), dtype=torch.float64, device=dev)
         self.obs = torch.zeros((K, d, d), dtype=torch.float64, device=dev)
+        self.chi = torch.zeros((K, d), dtype=torch.float64, device=dev)     # Bartlett chi-square sums
+        self._side = None
         self.scratch = torch.zeros(int(N.lib().ab_gmm_stats_scratch_bytes(d, K)) // 8 + 1,
                                    dtype=torch.float64, device=dev)
         # the screened assignment draw's tables and queue (ab_gmm_disc_z_screened)
@@ -154,6 +156,19 @@ class GmmGibbs(Checkpointable):
             else:
                 N.check(L.ab_gmm_stats(self.N, d, K, N.ptr(self.Y), N.ptr(self.z), None, N.ptr(self.cnt),
                                        N.ptr(self.sum), None, N.ptr(self.scratch), st), "stats")
+                # the Bartlett chi-square sums need only the counts: they are
+                # drawn on a side stream beside the weights, the means and the
+                # scatter pass (ab_gmm_conj_cov's draw, in two calls)
+                main = stream if stream is not None else torch.cuda.current_stream(self.Y.device)
+                if self._side is None:
+                    self._side = torch.cuda.Stream(self.Y.device)
+                fork = torch.cuda.Event()
+                fork.record(main)
+                self._side.wait_event(fork)
+                N.check(L.ab_gmm_bartlett(K, d, self.df, N.ptr(self.cnt), N.ptr(self.chi), self.seed, it, 0,
+                                          N.stream_ptr(self._side)), "bartlett")
+                join = torch.cuda.Event()
+                join.record(self._side)
                 N.check(L.ab_gmm_conj_pis(K, N.ptr(self.alpha), N.ptr(self.cnt), N.ptr(self.pis), self.seed, it,
                                           0, st), "conj_pis")
                 N.check(L.ab_gmm_conj_mu(K, d, 0, N.ptr(self.mu0), N.ptr(self.cov0), N.ptr(self.cnt),
@@ -161,8 +176,10 @@ class GmmGibbs(Checkpointable):
                         "conj_mu")
                 N.check(L.ab_gmm_stats(self.N, d, K, N.ptr(self.Y), N.ptr(self.z), N.ptr(self.mu),
                                        N.ptr(self.cnt), None, N.ptr(self.obs), N.ptr(self.scratch), st), "stats")
-                N.check(L.ab_gmm_conj_cov(K, d, self.df, N.ptr(self.scale0), N.ptr(self.cnt), N.ptr(self.obs),
-                                          N.ptr(self.cov), self.seed, it, 0, st), "conj_cov")
+                main.wait_event(join)
+                N.check(L.ab_gmm_conj_cov_chi(K, d, self.df, N.ptr(self.scale0), N.ptr(self.cnt),
+                                              N.ptr(self.obs), N.ptr(self.chi), N.ptr(self.cov), self.seed, it, 0,
+                                              st), "conj_cov")
                 N.check(L.ab_gmm_prep(K, d, N.ptr(self.cov), N.ptr(self.Linv), N.ptr(self.hdet), st), "prep")
             N.check(L.ab_gmm_disc_z_screened(self.N, d, K, int(self.shared), N.ptr(self.Y), N.ptr(self.pis),
                                              N.ptr(self.mu), N.ptr(self.Linv), N.ptr(self.hdet), N.ptr(self.z),

@@ -294,6 +294,17 @@ int ab_gmm_conj_mu(int K, int d, int shared_cov, const double* mu0, const double
 int ab_gmm_conj_cov(int K, int d, int df, const double* scale0, const int* cnt, const double* obs, double* cov,
                     uint64_t seed, uint32_t iter, uint32_t comp, void* stream);
 
+/* The same draw in two calls, so that the first can run beside the steps
+ * that still read cov (the conjugate mean draw and the scatter pass):
+ * ab_gmm_bartlett writes the Bartlett chi-square sums (bartlett_decomp's
+ * diagonal before its square root, cbits/augur_dist.c:722-738) into chi
+ * double[K][d]; ab_gmm_conj_cov_chi then makes the draw from them.  Together
+ * they give ab_gmm_conj_cov's result bit for bit. */
+int ab_gmm_bartlett(int K, int d, int df, const int* cnt, double* chi, uint64_t seed, uint32_t iter,
+                    uint32_t comp, void* stream);
+int ab_gmm_conj_cov_chi(int K, int d, int df, const double* scale0, const int* cnt, const double* obs,
+                        const double* chi, double* cov, uint64_t seed, uint32_t iter, uint32_t comp, void* stream);
+
 /* ESlice [mu]: augur_mcmc_eslice (cbits/augur_mcmclib.h:439-485) for every
  * component (one thread block each) over the full conditional of mu[k]
  * (prior table in slot prior_slot); (k, iter, 10|comp<<8).  shrinks int32[K]. */

@@ -67,6 +67,29 @@ def test_stats_and_conj_draws(orc):
     np.testing.assert_allclose(g.cov.cpu().numpy(), O.gmm_conj_cov(orc, om, cnt, obs, 9, 2), rtol=1e-9, atol=1e-12)
 
 
+@pytest.mark.parametrize("K,d", [(16, 32), (3, 5)])
+def test_conj_cov_in_two_calls_equals_one(K, d):
+    """ab_gmm_bartlett + ab_gmm_conj_cov_chi (the sweep's split, the first on
+    a side stream) give ab_gmm_conj_cov's draw bit for bit."""
+    rng = np.random.default_rng(K + d)
+    cnt = torch.as_tensor(rng.integers(0, 5000, size=K).astype(np.int32)).cuda()
+    a = rng.standard_normal((K, d, d))
+    obs = torch.as_tensor(np.einsum("kij,klj->kil", a, a) * 50.0).cuda()
+    scale0 = torch.eye(d, dtype=torch.float64, device="cuda")
+    one = torch.zeros((K, d, d), dtype=torch.float64, device="cuda")
+    two = torch.zeros_like(one)
+    chi = torch.zeros((K, d), dtype=torch.float64, device="cuda")
+    L = N.lib()
+    st = N.stream_ptr()
+    N.check(L.ab_gmm_conj_cov(K, d, d + 2, N.ptr(scale0), N.ptr(cnt), N.ptr(obs), N.ptr(one), 5, 3, 0, st), "cov")
+    N.check(L.ab_gmm_bartlett(K, d, d + 2, N.ptr(cnt), N.ptr(chi), 5, 3, 0, st), "bartlett")
+    N.check(L.ab_gmm_conj_cov_chi(K, d, d + 2, N.ptr(scale0), N.ptr(cnt), N.ptr(obs), N.ptr(chi), N.ptr(two), 5, 3,
+                                  0, st), "cov_chi")
+    torch.cuda.synchronize()
+    assert torch.equal(one, two)
+    assert torch.isfinite(one).all()
+
+
 @pytest.mark.parametrize("N_,K,d", [(300_000, 16, 32), (250_000, 3, 40), (1, 2, 3), (900, 16, 2)])
 def test_stats_sizes(orc, N_, K, d):
     """Statistics at sizes where a CTA's chunk spans several shared-memory
