@@ -34,17 +34,22 @@ constexpr int GMM_STAT_CTAS = 296;
 
 // augur_mat_cholesky (:312-328), column by column; (i, j) uses row i and
 // row j left of j, and the diagonal (j, j) - all final before column j.
+// The diagonal's products A[j][k]^2 are formed on the lanes (k = lane,
+// lane + 32) and every lane adds them in k order from the shuffles, so the
+// sum is the reference's sequence of additions.
 __device__ void w_chol(double* A, int d) {
   const int lane = threadIdx.x & 31;
   for (int j = 0; j < d; ++j) {
-    if (lane == 0) {
-      double s = 0.0;
-#pragma unroll 4
-      for (int k = 0; k < j; ++k) s = __dadd_rn(s, __dmul_rn(GM(A, j, k), GM(A, j, k)));
-      GM(A, j, j) = __dsqrt_rn(__dadd_rn(GM(A, j, j), -s));
-    }
-    __syncwarp();
-    const double rjj = __ddiv_rn(1.0, GM(A, j, j));   // the reference's 1 / A[j][j], once per column
+    const double p0 = lane < j ? __dmul_rn(GM(A, j, lane), GM(A, j, lane)) : 0.0;
+    const double p1 = lane + 32 < j ? __dmul_rn(GM(A, j, lane + 32), GM(A, j, lane + 32)) : 0.0;
+    double sd = 0.0;
+    const int j0 = j < 32 ? j : 32;
+    for (int k = 0; k < j0; ++k) sd = __dadd_rn(sd, __shfl_sync(0xffffffffu, p0, k));
+    for (int k = 32; k < j; ++k) sd = __dadd_rn(sd, __shfl_sync(0xffffffffu, p1, k - 32));
+    const double djj = __dsqrt_rn(__dadd_rn(GM(A, j, j), -sd));
+    __syncwarp();                                     // A[j][j] read by every lane before it is replaced
+    if (lane == 0) GM(A, j, j) = djj;
+    const double rjj = __ddiv_rn(1.0, djj);           // the reference's 1 / A[j][j], once per column
     for (int i = j + 1 + lane; i < d; i += 32) {
       double s = 0.0;
 #pragma unroll 4
@@ -84,23 +89,28 @@ __device__ void w_trmi(double* L, double* T, int d) {
 // augur_mat_cholesky_invert (:363-375): trmi, then for each column c and row
 // r >= c (in order) A[r][c] = sum_{k=c}^{d-1} A[k][r] A[k][c] with the
 // column's earlier rows already replaced, then the lower part mirrored.
-// Columns only read their own progress and later columns, which the
-// reference has not yet touched, so they run in parallel from a copy T.
+// After trmi the factor's upper triangle is zero, so the terms k < r are
+// zero products: starting from +0.0 they leave the sum +0.0, and the entry
+// is the sum over k = r .. d-1 of M[k][r] M[k][c] (M the inverse factor, kept
+// in T), in k order - independent of every other entry (while the entries
+// are finite).  The d(d+1)/2 entries are dealt to the lanes in turn, which
+// balances their d - r terms (column 0 alone used to take d^2 / 2 steps of
+// one lane).
 __device__ void w_cholinv(double* A, double* T, int d) {
   const int lane = threadIdx.x & 31;
   w_trmi(A, T, d);
   for (int e = lane; e < d * d; e += 32) T[e] = A[e];
   __syncwarp();
-  for (int c = lane; c < d; c += 32) {
-    for (int r = c; r < d; ++r) {
-      double acc = 0.0;
+  const int ntri = d * (d + 1) / 2;
+  for (int idx = lane; idx < ntri; idx += 32) {
+    int r = (int)((sqrtf(8.0f * (float)idx + 1.0f) - 1.0f) * 0.5f);
+    while (r * (r + 1) / 2 > idx) --r;
+    while ((r + 1) * (r + 2) / 2 <= idx) ++r;
+    const int c = idx - r * (r + 1) / 2;
+    double acc = 0.0;
 #pragma unroll 4
-      for (int k = c; k < d; ++k) {
-        const double akc = (k < r) ? GM(A, k, c) : GM(T, k, c);
-        acc = __dadd_rn(acc, __dmul_rn(GM(T, k, r), akc));
-      }
-      GM(A, r, c) = acc;
-    }
+    for (int k = r; k < d; ++k) acc = __dadd_rn(acc, __dmul_rn(GM(T, k, r), GM(T, k, c)));
+    GM(A, r, c) = acc;
   }
   __syncwarp();
   for (int e = lane; e < d * d; e += 32) {
